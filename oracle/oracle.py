@@ -1,0 +1,127 @@
+"""CPU oracle loader — test infrastructure, not the product.
+
+ctypes front-end for ``oracle/_build/liboracle.so``, the FP64 C++ restatement
+of the sim-trhepd-rheed surface and bulk solves.  Only ``tests/``, the smoke
+check and ``bench.py``'s CPU-baseline leg may import this module; the product
+path never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "liboracle.so"
+_lib = None
+
+
+def build(quiet: bool = True) -> Path:
+    """Compile the oracle with its Makefile (g++ -fopenmp, scipy's OpenBLAS)."""
+    cmd = ["make", "-C", str(HERE)]
+    out = subprocess.run(cmd, capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        L.oracle_surface_open.restype = ctypes.c_void_p
+        L.oracle_surface_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
+                                          ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        L.oracle_surface_close.argtypes = [ctypes.c_void_p]
+        L.oracle_surface_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_surface_scalars.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        L.oracle_surface_tables.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p]
+        L.oracle_surface_solve.restype = ctypes.c_int
+        L.oracle_surface_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_surface_write.restype = ctypes.c_int
+        L.oracle_surface_write.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.oracle_bulk_run.restype = ctypes.c_int
+        L.oracle_bulk_run.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                      ctypes.c_int]
+        L.oracle_set_threads.argtypes = [ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int | None = None) -> int:
+    n = n or os.cpu_count() or 1
+    lib().oracle_set_threads(int(n))
+    return n
+
+
+class Surface:
+    """One surf.exe problem (bulkP.b + surf.txt + dz2 + int_method), domain 1."""
+
+    def __init__(self, bulkp: str | os.PathLike, surf: str | os.PathLike, dz2: float,
+                 method: int = 5):
+        err = ctypes.create_string_buffer(512)
+        h = lib().oracle_surface_open(str(bulkp).encode(), str(surf).encode(), float(dz2),
+                                      int(method), err, 512)
+        if not h:
+            raise RuntimeError("oracle: " + err.value.decode())
+        self._h = h
+        d = (ctypes.c_int * 10)()
+        lib().oracle_surface_dims(h, d)
+        (self.nb, self.nv, self.nvb, self.ns, self.ncol, self.nrep1, self.nrep2, self.ngr,
+         self.naz, self.ng) = list(d)
+        s = (ctypes.c_double * 9)()
+        lib().oracle_surface_scalars(h, s)
+        self.dz, self.wn, self.ghx, self.ghy, self.gky, self.azi, self.daz, self.gi, self.dg = list(s)
+        self.method = method
+
+    @property
+    def n_angles(self) -> int:
+        return self.nrep1 * self.nrep2
+
+    def tables(self):
+        v = np.empty((self.ncol, self.nv), dtype=np.complex128)
+        vi = np.empty((self.ncol, self.nv), dtype=np.complex128)
+        iv = np.empty((self.nb, self.nb), dtype=np.int32)
+        lib().oracle_surface_tables(self._h, v.ctypes.data, vi.ctypes.data, iv.ctypes.data)
+        return v, vi, iv  # v[c, k] = column c; iv[j, i] = Fortran iv(i+1, j+1)
+
+    def solve(self, first: int = 0, count: int | None = None):
+        count = self.n_angles - first if count is None else count
+        f2 = np.empty((count, self.nb), dtype=np.float64)
+        ang = np.empty(count, dtype=np.float64)
+        ren = np.empty(count, dtype=np.int32)
+        rc = lib().oracle_surface_solve(self._h, first, count, f2.ctypes.data, ang.ctypes.data,
+                                        ren.ctypes.data)
+        if rc:
+            raise RuntimeError(f"oracle solve failed rc={rc}")
+        return f2, ang, ren
+
+    def write(self, path) -> None:
+        rc = lib().oracle_surface_write(self._h, str(path).encode())
+        if rc:
+            raise RuntimeError(f"oracle write failed rc={rc}")
+
+    def close(self):
+        if self._h:
+            lib().oracle_surface_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def bulk_run(bulk_txt, out_path) -> None:
+    err = ctypes.create_string_buffer(512)
+    rc = lib().oracle_bulk_run(str(bulk_txt).encode(), str(out_path).encode(), err, 512)
+    if rc:
+        raise RuntimeError("oracle bulk: " + err.value.decode())

@@ -1,0 +1,2100 @@
+// =============================================================================
+// CPU ORACLE — test infrastructure, not the product.
+//
+// A plain FP64 restatement of the sim-trhepd-rheed multislice path (surface and
+// bulk solve) used to check the CUDA implementation.  Only tests/, the smoke
+// check in __graft_entry__.py and bench.py's CPU-baseline leg may load it.
+//
+// Every routine follows one reference routine, in the same loop order and with
+// the same branch thresholds; the reference file:line is cited on each.  Dense
+// linear algebra goes to the LAPACK/BLAS build that scipy bundles (OpenBLAS
+// 0.3.30, LP64) where the reference calls MKL.  Parity of this restatement is
+// pinned against the reference's own committed outputs (test/test{23,47,521}).
+// =============================================================================
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../trhepd-opt_b200/csrc/scattering_tables.h"
+#include "fortran_io.h"
+#include "lapack.h"
+
+namespace oracle {
+
+static const double kPi = std::atan(1.0) * 4.0;
+static const int kMab = 6;  // surfio.f90:16
+
+// column-major helpers
+struct CMat {
+  int m = 0, n = 0;
+  std::vector<cplx> a;
+  CMat() = default;
+  CMat(int m_, int n_) : m(m_), n(n_), a((size_t)m_ * n_) {}
+  cplx& operator()(int i, int j) { return a[(size_t)j * m + i]; }
+  const cplx& operator()(int i, int j) const { return a[(size_t)j * m + i]; }
+  cplx* col(int j) { return a.data() + (size_t)j * m; }
+  cplx* data() { return a.data(); }
+};
+
+// ---------------------------------------------------------------- asf.f90
+// asfparam: Doyle-Turner coefficients first when iabr==0, else Peng
+// (sim-trhepd-rheed/src/asf.f90:415-431).
+static int asfparam(int iz, int iabr, double* a, double* b) {
+  if (iabr == 0 && iz >= 1 && iz <= 98 && trhepd_tables::kDoyleTurner[iz - 1][0] > 1e-5) {
+    for (int i = 0; i < 4; ++i) {
+      a[i] = trhepd_tables::kDoyleTurner[iz - 1][i];
+      b[i] = trhepd_tables::kDoyleTurner[iz - 1][4 + i];
+    }
+    return 4;
+  }
+  if (iz >= 1 && iz <= 98) {
+    for (int i = 0; i < 4; ++i) {
+      a[i] = trhepd_tables::kPeng[iz - 1][i];
+      b[i] = trhepd_tables::kPeng[iz - 1][4 + i];
+    }
+    return 4;
+  }
+  return 0;
+}
+// asf.f90:437-470
+static double amass(int iz) {
+  return (iz >= 1 && iz <= 110) ? trhepd_tables::kAtomicMass[iz - 1] : 1000.0;
+}
+
+// ---------------------------------------------------------------- element data
+struct Elements {
+  int nelm = 0, nabr = 4, nabi = 1;
+  // a,b,c stored (mab, nelm) column-major like the reference
+  std::vector<double> a, b, c, dth, dtk, dtz, elm, dchg;
+  void resize(int n) {
+    nelm = n;
+    a.assign((size_t)kMab * n, 0.0);
+    b.assign((size_t)kMab * n, 0.0);
+    c.assign((size_t)kMab * n, 0.0);
+    dth.assign(n, 0.0);
+    dtk.assign(n, 0.0);
+    dtz.assign(n, 0.0);
+    elm.assign(n, 0.0);
+    dchg.assign(n, 0.0);
+  }
+  double& A(int j, int i) { return a[(size_t)i * kMab + j]; }
+  double& B(int j, int i) { return b[(size_t)i * kMab + j]; }
+  double& C(int j, int i) { return c[(size_t)i * kMab + j]; }
+};
+
+// asfcrr: energy and Debye-Waller correction of the Gaussian coefficients
+// (sim-trhepd-rheed/src/scpot.f90:11-58).
+static double asfcrr(double be, Elements& E, double tem, double smesh) {
+  const double pi = kPi, c2m = 511.001, ek = .262466;
+  double wn = std::sqrt(1e3 * be * ek * (1.0 + 0.5 * be / c2m));
+  double s = 4.0 * pi / smesh;
+  double rel = (1.0 + be / c2m) * s;
+  double rat = std::sqrt(100.0 / be * (1.0 + 50.0 / c2m) / (1.0 + be * 0.5 / c2m)) * s;
+  double vib = 11407.0 * tem;
+  for (int i = 0; i < E.nelm; ++i) {
+    double dwz;
+    if (tem > 1e-5) {
+      dwz = vib / (E.dtz[i] * E.dtz[i] * E.elm[i]);
+      E.dth[i] = std::sqrt((vib + vib) / E.elm[i]) / (4.0 * pi * E.dth[i]);
+      E.dtk[i] = std::sqrt((vib + vib) / E.elm[i]) / (4.0 * pi * E.dtk[i]);
+    } else if (tem < -1e-5) {
+      dwz = (8.0 * pi * pi) * E.dtz[i] * E.dtz[i];
+    } else {
+      dwz = E.dtz[i];
+      E.dth[i] = std::sqrt(E.dth[i] * 0.5) / (pi + pi);
+      E.dtk[i] = std::sqrt(E.dtk[i] * 0.5) / (pi + pi);
+    }
+    for (int j = 0; j < E.nabr; ++j) {
+      E.C(j, i) = E.B(j, i) / (-16.0 * pi * pi);
+      E.A(j, i) = E.A(j, i) * std::sqrt(4.0 * pi / (E.B(j, i) + dwz)) * rel;
+      E.B(j, i) = -4.0 * pi * pi / (E.B(j, i) + dwz);
+    }
+    if (std::fabs(E.dchg[i]) > 1e-4) E.dchg[i] = E.dchg[i] * 1.88972619 * rel;
+    if (E.nabi >= 2) {
+      for (int j = E.nabr; j < E.nabr + E.nabi; ++j) {
+        E.C(j, i) = E.B(j, i) / (-16.0 * pi * pi);
+        E.A(j, i) = E.A(j, i) * std::sqrt(4.0 * pi / E.B(j, i)) * rat;
+        E.B(j, i) = -4.0 * pi * pi / E.B(j, i);
+      }
+    }
+  }
+  return wn;
+}
+
+// asfcef: asf(k,i,e) = a*exp(c*s_k + sj_k)  (sim-trhepd-rheed/src/scpot.f90:62-95)
+// asf is (nv, mab, nelm) column-major.
+static void asfcef(int nv, const std::vector<int>& igh, const std::vector<int>& igk, double ghx,
+                   double ghy, double gky, Elements& E, std::vector<double>& asf,
+                   std::vector<double>& Ghk) {
+  asf.assign((size_t)nv * kMab * E.nelm, 0.0);
+  Ghk.assign(nv, 0.0);
+  std::vector<double> s(nv), sj(nv);
+  for (int k = 0; k < nv; ++k) {
+    double x = ghx * igh[k], y = ghy * igh[k] + gky * igk[k];
+    s[k] = x * x + y * y;
+  }
+  for (int j = 0; j < E.nelm; ++j) {
+    for (int k = 0; k < nv; ++k) {
+      double x = E.dth[j] * ghx * igh[k];
+      double y = E.dth[j] * ghy * igh[k] + E.dtk[j] * gky * igk[k];
+      sj[k] = -0.5 * (x * x + y * y);
+    }
+    for (int i = 0; i < E.nabr; ++i)
+      for (int k = 0; k < nv; ++k)
+        asf[((size_t)j * kMab + i) * nv + k] = E.A(i, j) * std::exp(E.C(i, j) * s[k] + sj[k]);
+    if (E.nabi >= 2)
+      for (int i = E.nabr; i < E.nabr + E.nabi; ++i)
+        for (int k = 0; k < nv; ++k)
+          asf[((size_t)j * kMab + i) * nv + k] =
+              E.A(i, j) * std::exp(E.C(i, j) * s[k] + sj[k] * 0.5);
+  }
+  for (int k = 0; k < nv; ++k) Ghk[k] = std::sqrt(s[k]);
+  if (E.nabi == 1)
+    for (int j = 0; j < E.nelm; ++j) asf[((size_t)j * kMab + E.nabr) * nv + 0] = E.A(E.nabr, j);
+}
+
+// ---------------------------------------------------------------- strfac.f90
+static double reduce01(double x) { return x - std::floor(x + 1e-4); }  // strfac.f90:80-84
+
+// Plane-group images of one atom, in surface-lattice fractional coordinates
+// (sim-trhepd-rheed/src/strfac.f90:88-527).  Special positions within 2e-4
+// collapse the orbit exactly as the reference does.
+static int plane_group_images(int nsg, double* xs, double* ys) {
+  const double t = 2e-4;
+  double x = xs[0], y = ys[0];
+  auto near = [&](double u, double v) { return std::fabs(u - v) < t; };
+  auto on0h = [&](double u) { return near(u, 0.0) || near(u, 0.5); };
+  auto set = [&](int i, double a, double b) {
+    xs[i] = a;
+    ys[i] = b;
+  };
+  switch (nsg) {
+    case 1:
+      return 1;
+    case 2:  // p211
+      if (on0h(x) && on0h(y)) return 1;
+      set(1, -x, -y);
+      return 2;
+    case 3:  // p1m1
+      if (on0h(y)) return 1;
+      set(1, x, -y);
+      return 2;
+    case 4:  // p1g1
+      set(1, x + 0.5, -y);
+      return 2;
+    case 5:  // c1m1
+      if (on0h(y)) {
+        set(1, x + 0.5, 0.5 - y);
+        return 2;
+      }
+      set(1, x + 0.5, 0.5 - y);
+      set(2, x, -y);
+      set(3, x + 0.5, 0.5 + y);
+      return 4;
+    case 6:  // p2mm
+      if (on0h(x) && on0h(y)) return 1;
+      if (on0h(x)) {
+        set(1, x, -y);
+        return 2;
+      }
+      if (on0h(y)) {
+        set(1, -x, y);
+        return 2;
+      }
+      set(1, x, -y);
+      set(2, -x, y);
+      set(3, -x, -y);
+      return 4;
+    case 7:  // p2mg
+      if (on0h(x) && on0h(y)) {
+        set(1, x, 0.5 - y);
+        return 2;
+      }
+      if (near(y, 0.25) || near(y, 0.75)) {
+        set(1, -x, -y);
+        return 2;
+      }
+      set(1, x, 0.5 - y);
+      set(2, -x, -y);
+      set(3, -x, 0.5 + y);
+      return 4;
+    case 8:  // p2gg
+      if (on0h(x) && on0h(y)) {
+        set(1, 0.5 - x, 0.5 + y);
+        return 2;
+      }
+      set(1, 0.5 - x, 0.5 + y);
+      set(2, 0.5 + x, 0.5 - y);
+      set(3, -x, -y);
+      return 4;
+    case 9:  // c2mm
+      if (on0h(x) && on0h(y)) {
+        set(1, 0.5 - x, 0.5 + y);
+        return 2;
+      }
+      if ((near(x, 0.25) || near(x, 0.75)) && (near(y, 0.25) || near(y, 0.75))) {
+        set(1, x, -y);
+        set(2, -x, y);
+        set(3, -x, -y);
+        return 4;
+      }
+      if (on0h(x)) {
+        set(1, x, -y);
+        set(2, 0.5 - x, 0.5 + y);
+        set(3, 0.5 - x, 0.5 - y);
+        return 4;
+      }
+      if (on0h(y)) {
+        set(1, -x, y);
+        set(2, 0.5 + x, 0.5 - y);
+        set(3, 0.5 - x, 0.5 - y);
+        return 4;
+      }
+      set(1, x, -y);
+      set(2, -x, y);
+      set(3, -x, -y);
+      set(4, 0.5 + x, 0.5 + y);
+      set(5, 0.5 + x, 0.5 - y);
+      set(6, 0.5 - x, 0.5 + y);
+      set(7, 0.5 - x, 0.5 - y);
+      return 8;
+    case 10:  // p4
+      if ((near(x, 0) && near(y, 0)) || (near(x, 0.5) && near(y, 0.5))) return 1;
+      if ((near(x, 0.5) && near(y, 0)) || (near(x, 0) && near(y, 0.5))) {
+        set(1, y, -x);
+        return 2;
+      }
+      set(1, -y, x);
+      set(2, -x, -y);
+      set(3, y, -x);
+      return 4;
+    case 11:  // p4mm
+      if ((near(x, 0) && near(y, 0)) || (near(x, 0.5) && near(y, 0.5))) return 1;
+      if ((near(x, 0.5) && near(y, 0)) || (near(x, 0) && near(y, 0.5))) {
+        set(1, y, x);
+        return 2;
+      }
+      if (near(y - x, 0) || near(x + y - 1.0, 0) || on0h(x) || on0h(y)) {
+        set(1, -y, x);
+        set(2, -x, -y);
+        set(3, y, -x);
+        return 4;
+      }
+      set(1, y, x);
+      set(2, -y, x);
+      set(3, -x, y);
+      set(4, -x, -y);
+      set(5, -y, -x);
+      set(6, y, -x);
+      set(7, x, -y);
+      return 8;
+    case 12:  // p4gm
+      if ((near(x, 0) && near(y, 0)) || (near(x, 0.5) && near(y, 0.5))) {
+        set(1, 0.5 - y, 0.5 - x);
+        return 2;
+      }
+      if ((near(x, 0.5) && near(y, 0)) || (near(x, 0) && near(y, 0.5))) {
+        set(1, y, -x);
+        return 2;
+      }
+      if (near(y - x + 0.5, 0) || near(y - x - 0.5, 0) || near(x + y - 0.5, 0) ||
+          near(x + y - 1.5, 0)) {
+        set(1, -y, x);
+        set(2, -x, -y);
+        set(3, y, -x);
+        return 4;
+      }
+      set(1, -y, x);
+      set(2, -x, -y);
+      set(3, y, -x);
+      set(4, 0.5 - y, 0.5 - x);
+      set(5, 0.5 + x, 0.5 - y);
+      set(6, 0.5 + y, 0.5 + x);
+      set(7, 0.5 - x, 0.5 + y);
+      return 8;
+    case 13:  // p3
+      if ((near(x, 0) && near(y, 0)) || (near(x, 1.0 / 3.0) && near(y, 2.0 / 3.0)) ||
+          (near(x, 2.0 / 3.0) && near(y, 1.0 / 3.0)))
+        return 1;
+      set(1, -y, x - y);
+      set(2, y - x, -x);
+      return 3;
+    case 14:  // p3m1
+      if ((near(x, 0) && near(y, 0)) || (near(x, 1.0 / 3.0) && near(y, 2.0 / 3.0)) ||
+          (near(x, 2.0 / 3.0) && near(y, 1.0 / 3.0)))
+        return 1;
+      if (near(x + x - y, 0) || near(y + y - x, 0) || near(x + x - y - 1.0, 0) ||
+          near(y + y - x - 1.0, 0) || near(x + y - 1.0, 0)) {
+        set(1, -y, x - y);
+        set(2, y - x, -x);
+        return 3;
+      }
+      set(1, x, x - y);
+      set(2, -y, x - y);
+      set(3, y - x, y);
+      set(4, y - x, -x);
+      set(5, -y, -x);
+      return 6;
+    case 15:  // p31m
+      if (near(x, 0) && near(y, 0)) return 1;
+      if ((near(x, 1.0 / 3.0) && near(y, 2.0 / 3.0)) || (near(x, 2.0 / 3.0) && near(y, 1.0 / 3.0))) {
+        set(1, y, x);
+        return 2;
+      }
+      if (near(x, 0) || near(y, 0) || near(x - y, 0)) {
+        set(1, -y, x - y);
+        set(2, y - x, -x);
+        return 3;
+      }
+      set(1, y, x);
+      set(2, -y, x - y);
+      set(3, -x, y - x);
+      set(4, y - x, -x);
+      set(5, x - y, -y);
+      return 6;
+    case 16:  // p6
+      if (near(x, 0) && near(y, 0)) return 1;
+      if ((near(x, 1.0 / 3.0) && near(y, 2.0 / 3.0)) || (near(x, 2.0 / 3.0) && near(y, 1.0 / 3.0))) {
+        set(1, y, x);
+        return 2;
+      }
+      if ((near(x, 0.5) && near(y, 0)) || (near(x, 0) && near(y, 0.5)) ||
+          (near(x, 0.5) && near(y, 0.5))) {
+        set(1, -y, x - y);
+        set(2, y - x, -x);
+        return 3;
+      }
+      set(1, x - y, x);
+      set(2, -y, x - y);
+      set(3, -x, -y);
+      set(4, y - x, -x);
+      set(5, y, y - x);
+      return 6;
+    case 17:  // p6mm
+      if (near(x, 0) && near(y, 0)) return 1;
+      if ((near(x, 1.0 / 3.0) && near(y, 2.0 / 3.0)) || (near(x, 2.0 / 3.0) && near(y, 1.0 / 3.0))) {
+        set(1, y, x);
+        return 2;
+      }
+      if ((near(x, 0.5) && near(y, 0)) || (near(x, 0) && near(y, 0.5)) ||
+          (near(x, 0.5) && near(y, 0.5))) {
+        set(1, -y, x - y);
+        set(2, y - x, -x);
+        return 3;
+      }
+      if (near(x, 0) || near(y, 0) || near(x - y, 0)) {
+        set(1, -y, x - y);
+        set(2, y - x, -x);
+        set(3, -x, -y);
+        set(4, y, y - x);
+        set(5, x - y, x);
+        return 6;
+      }
+      set(1, x, x - y);
+      set(2, x - y, x);
+      set(3, y, x);
+      set(4, -y, x - y);
+      set(5, y - x, y);
+      set(6, -x, -y);
+      set(7, -x, y - x);
+      set(8, y - x, -x);
+      set(9, -y, -x);
+      set(10, y, y - x);
+      set(11, x - y, -y);
+      return 12;
+    default:
+      throw std::runtime_error("plane group must be one of 1..17");
+  }
+}
+
+// strfac (sim-trhepd-rheed/src/strfac.f90:5-76)
+static void strfac(int nsg, int nv, int ma, int mb, int na, int nb, const double* gh,
+                   const double* gk, double x, double y, double dx, double dy, cplx* st) {
+  double xs[12], ys[12], xb[12], yb[12];
+  double s = (double)(ma * nb - mb * na);
+  xs[0] = reduce01((nb * x - na * y) / s);
+  ys[0] = reduce01((ma * y - mb * x) / s);
+  int ndeg = plane_group_images(nsg, xs, ys);
+  for (int i = 0; i < ndeg; ++i) {
+    xs[i] = reduce01(xs[i]);
+    ys[i] = reduce01(ys[i]);
+    xb[i] = ma * xs[i] + na * ys[i];
+    yb[i] = mb * xs[i] + nb * ys[i];
+  }
+  for (int m = 0; m < nv; ++m) {
+    cplx acc(0.0, 0.0);
+    for (int i = 0; i < ndeg; ++i) {
+      double gr = gh[m] * (dx + xb[i]) + gk[m] * (dy + yb[i]);
+      acc += cplx(std::cos(gr), std::sin(gr));
+    }
+    st[m] = acc;
+  }
+}
+
+// scpot_stf (scpot.f90:100-110): st(nv, natm)
+static void scpot_stf(int natm, int nv, int nsg, int ma, int mb, int na, int nb,
+                      const std::vector<double>& gh, const std::vector<double>& gk,
+                      const double* x, const double* y, double dx, double dy,
+                      std::vector<cplx>& st) {
+  st.assign((size_t)nv * natm, cplx(0, 0));
+  for (int j = 0; j < natm; ++j)
+    strfac(nsg, nv, ma, mb, na, nb, gh.data(), gk.data(), x[j], y[j], dx, dy,
+           st.data() + (size_t)j * nv);
+}
+
+// scpot: Fourier components of the potential at depth zi
+// (sim-trhepd-rheed/src/scpot.f90:115-193).  mv = leading dim of asf, nv = count.
+static void scpot(int mv, int nv, cplx* v, cplx* vi, int natm, const int* ielm, const double* z,
+                  double zi, const Elements& E, const std::vector<double>& asf,
+                  double rmesh, const std::vector<double>& Ghk, const double* ocr,
+                  const cplx* st) {
+  const double uf = -70.0;
+  const int nabr = E.nabr, nabi = E.nabi;
+  std::vector<double> tv(nv), tvi(nv);
+  auto ASF = [&](int k, int i, int e) { return asf[((size_t)e * kMab + i) * mv + k]; };
+  auto Bc = [&](int i, int e) { return E.b[(size_t)e * kMab + i]; };
+  for (int j = 0; j < natm; ++j) {
+    double ocrmesh = rmesh * ocr[j];
+    int ie = ielm[j] - 1;
+    double z1 = zi - z[j];
+    double z2 = z1 * z1;
+    if (std::fabs(E.dchg[ie]) > 1e-4) {
+      z1 = -std::fabs(z1);
+      tv[0] = ocrmesh * z1 * E.dchg[ie];
+      for (int k = 1; k < nv; ++k) {
+        double ex = Ghk[k] * z1;
+        if (ex > uf)
+          tv[k] = std::exp(ex) * ocrmesh / Ghk[k] * E.dchg[ie];
+        else
+          tv[k] = 0.0;
+      }
+    } else {
+      std::fill(tv.begin(), tv.end(), 0.0);
+    }
+    std::fill(tvi.begin(), tvi.end(), 0.0);
+    if (nabi >= 2) {
+      for (int i = nabr; i < nabr + nabi; ++i) {
+        double ex = Bc(i, ie) * z2;
+        if (ex > uf) {
+          ex = std::exp(ex) * ocrmesh;
+          for (int k = 0; k < nv; ++k) tvi[k] = ASF(k, i, ie) * ex;
+        }
+      }
+    }
+    for (int i = 0; i < nabr; ++i) {
+      double ex = Bc(i, ie) * z2;
+      if (ex > uf) {
+        ex = std::exp(ex) * ocrmesh;
+        if (nabi == 1) {
+          double sap = ASF(0, nabr, ie);
+          for (int k = 0; k < nv; ++k) {
+            double aex = ASF(k, i, ie) * ex;
+            tv[k] = tv[k] + aex;
+            tvi[k] = tvi[k] + std::fabs(sap * aex);
+          }
+        } else {
+          for (int k = 0; k < nv; ++k) tv[k] = tv[k] + ASF(k, i, ie) * ex;
+        }
+      }
+    }
+    const cplx* stj = st + (size_t)j * nv;
+    for (int k = 0; k < nv; ++k) {
+      cplx ct = stj[k];
+      v[k] = v[k] + tv[k] * ct;
+      vi[k] = vi[k] + cplx(0.0, tvi[k]) * ct;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- beam maps
+// srfghk (sim-trhepd-rheed/src/surfsub.f90:9-41): iv(nb,nb) column-major, 1-based
+// entries for l>k; igh/igk grow from the bulk list.
+static int srfghk(int nvm, int nvb, std::vector<int>& igh, std::vector<int>& igk, int nb,
+                  const int* ih, const int* ik, std::vector<int>& iv) {
+  int nv = nvb;
+  igh.resize(std::max<size_t>(igh.size(), (size_t)nvm));
+  igk.resize(std::max<size_t>(igk.size(), (size_t)nvm));
+  iv.assign((size_t)nb * nb, 0);
+  for (int k = 0; k < nb - 1; ++k)
+    for (int l = k + 1; l < nb; ++l) {
+      int ih0 = ih[l] - ih[k], ik0 = ik[l] - ik[k];
+      int found = 0;
+      for (int m = 1; m < nv; ++m)
+        if (ih0 == igh[m] && ik0 == igk[m]) {
+          iv[(size_t)k * nb + l] = m + 1;
+          found = 1;
+          break;
+        }
+      if (!found) {
+        nv = nv + 1;
+        if (nv > nvm) throw std::runtime_error("srfghk: nv > nvm");
+        igh[nv - 1] = ih0;
+        igk[nv - 1] = ik0;
+        iv[(size_t)k * nb + l] = nv;
+      }
+    }
+  return nv;
+}
+
+// scanrg (sim-trhepd-rheed/src/bulksub.f90:9-42)
+static void scanrg(double& azi, double azf, double& daz, int& naz, double& gi, double gf,
+                   double& dg, int& ng) {
+  const int nazm = 200, ngm = 200;
+  const double rad = std::atan(1.0) / 45.0;
+  if (std::fabs(daz) < 1e-4)
+    naz = 1;
+  else {
+    naz = (int)((azf - azi) / daz + 0.1) + 1;
+    if (naz < 1) naz = 1;
+    else if (naz > nazm) naz = nazm;
+  }
+  azi = azi * rad;
+  daz = daz * rad;
+  if (std::fabs(dg) < 1e-4)
+    ng = 1;
+  else {
+    ng = (int)((gf - gi) / dg + .1) + 1;
+    if (ng < 1) ng = 1;
+    else if (ng > ngm) ng = ngm;
+  }
+  gi = gi * rad;
+  dg = dg * rad;
+}
+
+// blkibg (sim-trhepd-rheed/src/bulksub.f90:46-92): groups of beams coupled in the bulk
+static void blkibg(int nb, int* ih, int* ik, int nh, int nk, std::vector<int>& iord, int& ngr,
+                   std::vector<int>& nbg) {
+  iord.resize(nb);
+  nbg.assign(nb, 0);
+  for (int i = 0; i < nb; ++i) iord[i] = i + 1;
+  if (nh == 1 && nk == 1) {
+    ngr = 1;
+    nbg[0] = nb;
+    return;
+  }
+  int j = 1;  // 1-based like the reference
+  ngr = 0;
+  while (true) {
+    int i = j;
+    j = i + 1;
+    int ih0 = ih[i - 1], ik0 = ik[i - 1];
+    ngr = ngr + 1;
+    for (int k = i + 1; k <= nb; ++k) {
+      if ((ih[k - 1] - ih0) % nh == 0 && (ik[k - 1] - ik0) % nk == 0) {
+        if (k > j) {
+          int l = ih[k - 1], n = ik[k - 1], m = iord[k - 1];
+          for (int jj = k; jj >= j + 1; --jj) {
+            ih[jj - 1] = ih[jj - 2];
+            ik[jj - 1] = ik[jj - 2];
+            iord[jj - 1] = iord[jj - 2];
+          }
+          ih[j - 1] = l;
+          ik[j - 1] = n;
+          iord[j - 1] = m;
+        }
+        j = j + 1;
+      }
+    }
+    nbg[ngr - 1] = j - i;
+    if (j > nb) return;
+  }
+}
+
+// blkghk (sim-trhepd-rheed/src/bulksub.f90:96-135): iv(nbgm, nb), 1-based entries
+static int blkghk(int ngr, const std::vector<int>& nbg, int nvm, std::vector<int>& igh,
+                  std::vector<int>& igk, int nbgm, int nb, const int* ih, const int* ik,
+                  std::vector<int>& iv) {
+  igh.assign(nvm, 0);
+  igk.assign(nvm, 0);
+  iv.assign((size_t)nbgm * nb, 0);
+  igh[0] = 0;
+  igk[0] = 0;
+  int nv = 1, ibas = 0;
+  for (int igr = 0; igr < ngr; ++igr) {
+    int iend = ibas + nbg[igr];
+    for (int k = 1 + ibas; k <= iend - 1; ++k)
+      for (int l = k + 1; l <= iend; ++l) {
+        int ih0 = ih[l - 1] - ih[k - 1], ik0 = ik[l - 1] - ik[k - 1];
+        int found = 0;
+        for (int m = 2; m <= nv; ++m)
+          if (ih0 == igh[m - 1] && ik0 == igk[m - 1]) {
+            iv[(size_t)(k - 1) * nbgm + (l - ibas - 1)] = m;
+            found = 1;
+            break;
+          }
+        if (!found) {
+          nv = nv + 1;
+          if (nv > nvm) throw std::runtime_error("blkghk: nv > nvm");
+          igh[nv - 1] = ih0;
+          igk[nv - 1] = ik0;
+          iv[(size_t)(k - 1) * nbgm + (l - ibas - 1)] = nv;
+        }
+      }
+    ibas = iend;
+  }
+  return nv;
+}
+
+// ---------------------------------------------------------------- matcomp.f90
+// matAbdivB: [A|B] -> B <- A\B by zgetrf on n x 2n then ztrsm (matcomp.f90:53-69)
+static void matAbdivB(int n, cplx* t1, int lda, std::vector<int>& piv) {
+  piv.resize(n);
+  zgetrf(n, 2 * n, t1, lda, piv.data());
+  ztrsm('L', 'U', 'N', 'N', n, n, cplx(1, 0), t1, lda, t1 + (size_t)n * lda, lda);
+}
+
+// matAdivB: A*inv(B) with B in A(:, n+1:2n) (matcomp.f90:22-51)
+static void matAdivB(int n, cplx* A, int lda, std::vector<int>& piv) {
+  auto at = [&](int i, int j) -> cplx& { return A[(size_t)j * lda + i]; };
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      cplx t = at(i, j);
+      at(i, j) = at(j, i + n);
+      at(j, i + n) = t;
+    }
+  matAbdivB(n, A, lda, piv);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) at(i, j) = at(j, i + n);
+}
+
+// invstransh (matcomp.f90:140-172)
+static void invstransh(int n, CMat& t1, const CMat& f, const cplx* g, std::vector<int>& piv) {
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      if (i == j) {
+        t1(i, j) = 1.0 + std::conj(f(j, j));
+        t1(i, n + j) = 1.0 - std::conj(f(j, j));
+      } else {
+        t1(i, j) = std::conj(f(j, i));
+        t1(i, n + j) = -std::conj(f(j, i));
+      }
+    }
+  matAbdivB(n, t1.data(), n, piv);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) t1(i, n + j) = cplx(0, 1) * t1(i, n + j) * std::conj(g[i]);
+}
+
+// stransh (matcomp.f90:174-196)
+static void stransh(int n, CMat& t1, const cplx* g, std::vector<int>& piv) {
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      if (i == j) {
+        t1(i, j) = std::conj(g[i]) + cplx(0, -1) * t1(i, j + n);
+        t1(i, j + n) = std::conj(g[i]) + cplx(0, 1) * t1(i, j + n);
+      } else {
+        t1(i, j) = cplx(0, -1) * t1(i, j + n);
+        t1(i, j + n) = cplx(0, 1) * t1(i, j + n);
+      }
+    }
+  matAbdivB(n, t1.data(), n, piv);
+}
+
+// vvi2mate: stage matrix M = -conj(V) - diag(conj(g^2)) (matcomp.f90:253-279)
+static void vvi2mate(int n, int nv, const cplx* v, const cplx* vi, const int* iv, const cplx* g,
+                     CMat& t) {
+  std::vector<cplx> v0(nv), v1(nv);
+  for (int k = 0; k < nv; ++k) {
+    v0[k] = -std::conj(v[k] + vi[k]);
+    v1[k] = -v[k] + vi[k];
+  }
+  for (int j = 0; j < n; ++j) {
+    for (int i = 0; i < j; ++i) t(i, j) = v0[iv[(size_t)i * n + j] - 1];
+    t(j, j) = v0[0] - std::conj(g[j] * g[j]);
+    for (int i = j + 1; i < n; ++i) t(i, j) = v1[iv[(size_t)j * n + i] - 1];
+  }
+}
+
+// cond_est: Gershgorin ratio of the first n columns (matcomp.f90:498-528)
+static double cond_est(int n, const cplx* A) {
+  double mn = std::abs(A[0]), mx = mn;
+  for (int j = 0; j < n; ++j) {
+    double t = 0.0;
+    for (int i = 0; i < n; ++i)
+      if (i != j) {
+        cplx a = A[(size_t)j * n + i];
+        t = t + std::sqrt(a.real() * a.real() + a.imag() * a.imag());
+      }
+    double d = std::abs(A[(size_t)j * n + j]);
+    mn = std::min(mn, d - t);
+    mx = std::max(mx, d + t);
+  }
+  return (mn < 0.0) ? 1e100 : mx / mn;
+}
+
+// hyperbolic_exp4r (matcomp.f90:388-405)
+static void hyperbolic_exp4r(double h, int n, const CMat& a, CMat& q, CMat& r) {
+  zgemm('N', 'N', n, n, n, 1.0, a.a.data(), n, a.a.data(), n, 0.0, r.data(), n);
+  double h3 = h * h * h, h5 = h3 * h * h;
+  for (size_t k = 0; k < (size_t)n * n; ++k) q.a[k] = (h3 / 6) * a.a[k] + (h5 / 120) * r.a[k];
+  for (int i = 0; i < n; ++i) q(i, i) = q(i, i) + h;
+  for (size_t k = 0; k < (size_t)n * n; ++k) r.a[k] = (h / 2) * a.a[k] - (h3 / 24) * r.a[k];
+}
+
+// hyperbolic_exp6r (matcomp.f90:407-428)
+static void hyperbolic_exp6r(double h, int n, const CMat& a, CMat& q, CMat& r) {
+  const double cq0 = 1.0 / 6, cq1 = 1.0 / 120, cq2 = 1.0 / 5040, cr0 = 0.5, cr1 = -1.0 / 24,
+               cr2 = 1.0 / 240;
+  CMat t(n, n);
+  zgemm('N', 'N', n, n, n, 1.0, a.a.data(), n, a.a.data(), n, 0.0, r.data(), n);
+  zgemm('N', 'N', n, n, n, 1.0, r.a.data(), n, a.a.data(), n, 0.0, t.data(), n);
+  double h3 = h * h * h, h5 = h3 * h * h, h7 = h5 * h * h;
+  for (size_t k = 0; k < (size_t)n * n; ++k)
+    q.a[k] = (h3 * cq0) * a.a[k] + (h5 * cq1) * r.a[k] + (h7 * cq2) * t.a[k];
+  for (int i = 0; i < n; ++i) q(i, i) = q(i, i) + h;
+  for (size_t k = 0; k < (size_t)n * n; ++k)
+    r.a[k] = (h * cr0) * a.a[k] + (h3 * cr1) * r.a[k] + (h5 * cr2) * t.a[k];
+}
+
+// ---------------------------------------------------------------- integrators
+// Blanes-Moan symplectic RKN coefficient tables (surf_prkn.f90:11-52); the
+// published coefficients are reproduced exactly because the integrator is
+// defined by them.
+static const double kRkn46[13] = {
+    0.0829844064174052,  0.245298957184271,  0.396309801498368, 0.604872665711080,
+    -0.0390563049223486, -0.350171622895351, 0.1195241940131508, -0.350171622895351,
+    -0.0390563049223486, 0.604872665711080,  0.396309801498368,  0.245298957184271,
+    0.0829844064174052};
+static const double kRkn611[23] = {
+    0.0414649985182624,  0.123229775946271,  0.198128671918067,  0.290553797799558,
+    -0.0400061921041533, -0.127049212625417, 0.0752539843015807, -0.246331761062075,
+    -0.0115113874206879, 0.357208872795928,  0.2366699247869311, 0.20477705429147,
+    0.2366699247869311,  0.357208872795928,  -0.0115113874206879, -0.246331761062075,
+    0.0752539843015807,  -0.127049212625417, -0.0400061921041533, 0.290553797799558,
+    0.198128671918067,   0.123229775946271,  0.0414649985182624};
+
+struct IntStats {
+  int renorm = 0;   // cond_est-triggered renormalisations (excludes the final one)
+  int gemms = 0;    // N^3 complex products issued
+};
+
+// hp_int_spa: symplectic RKN in [X^H, Y^H] form (surf_prkn.f90:278-330)
+static void hp_int_spa(double dz, int ns, int nb, int nv, CMat& f, const cplx* g, const int* iv,
+                       const cplx* v, const cplx* vi, int s, const double* bab, IntStats& st) {
+  CMat t1(nb, 2 * nb), psave(nb, nb), m(nb, nb);
+  std::vector<int> piv;
+  invstransh(nb, t1, f, g, piv);
+  bool x_is_id = true;
+  cplx* Q = t1.col(0);
+  cplx* P = t1.col(nb);
+  const size_t nn = (size_t)nb * nb;
+  auto col = [&](int c, const cplx* base) { return base + (size_t)c * nv; };
+  for (int l = 1; l <= ns; ++l) {
+    for (int k = 1; k <= s; ++k) {
+      double cb = bab[2 * k - 2], ca = bab[2 * k - 1];
+      if (k > 1 || l == 1) vvi2mate(nb, nv, col(s * (l - 1) + k - 1, v), col(s * (l - 1) + k - 1, vi), iv, g, m);
+      if (k == 1 && !x_is_id && l > 1) {
+        for (size_t e = 0; e < nn; ++e) P[e] = P[e] + psave.a[e];  // hp_pinth_usesave
+      } else {  // hp_pinth
+        if (x_is_id) {
+          for (size_t e = 0; e < nn; ++e) P[e] = P[e] + (cb * dz) * m.a[e];
+        } else {
+          zgemm('N', 'N', nb, nb, nb, cplx(1, 0) * (cb * dz), Q, nb, m.data(), nb, 1.0, P, nb);
+          st.gemms++;
+        }
+      }
+      // hp_qinth
+      if (x_is_id) {
+        for (size_t e = 0; e < nn; ++e) Q[e] = (ca * dz) * P[e];
+        for (int i = 0; i < nb; ++i) Q[(size_t)i * nb + i] = Q[(size_t)i * nb + i] + 1.0;
+      } else {
+        for (size_t e = 0; e < nn; ++e) Q[e] = Q[e] + (ca * dz) * P[e];
+      }
+      x_is_id = false;
+    }
+    vvi2mate(nb, nv, col(s * l, v), col(s * l, vi), iv, g, m);
+    // hp_pinth_save
+    zgemm('N', 'N', nb, nb, nb, cplx(1, 0) * (bab[0] * dz), Q, nb, m.data(), nb, 0.0,
+          psave.data(), nb);
+    st.gemms++;
+    for (size_t e = 0; e < nn; ++e) P[e] = P[e] + psave.a[e];
+    double d = cond_est(nb, Q);
+    if (d > 1e3 || l == ns) {
+      if (l != ns) st.renorm++;
+      matAbdivB(nb, t1.data(), nb, piv);
+      x_is_id = true;
+    } else {
+      x_is_id = false;
+    }
+  }
+  stransh(nb, t1, g, piv);
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) f(i, j) = std::conj(t1(j, nb + i));
+}
+
+// hp_int_spa1d: the scalar (nb == 1) RKN-6 path (surf_prkn.f90:485-524)
+static void hp_int_spa1d(double dz, int ns, cplx& f, cplx g, const cplx* v, const cplx* vi, int s,
+                         const double* bab) {
+  cplx q = 1.0;
+  cplx p = cplx(0, 1) * (1.0 - std::conj(f)) / (1.0 + std::conj(f)) * std::conj(g);
+  for (int l = 1; l <= ns; ++l) {
+    for (int k = 1; k <= s; ++k) {
+      double cb = (l != 1 && k == 1) ? 2 * bab[0] : bab[2 * k - 2];
+      double ca = bab[2 * k - 1];
+      int c = s * (l - 1) + k - 1;
+      cplx m = -std::conj(v[c] + vi[c]) - std::conj(g * g);
+      p = p + cb * dz * m * q;
+      q = q + ca * dz * p;
+    }
+    p = p / q;
+    q = 1.0;
+  }
+  int c = ns * s;
+  cplx m = -std::conj(v[c] + vi[c]) - std::conj(g * g);
+  p = p + bab[0] * dz * m * q;
+  f = (std::conj(g) + cplx(0, 1) * p) / (std::conj(g) + cplx(0, -1) * p);
+}
+
+// lf_int_spa: Stormer-Verlet (surf_magnus.f90:46-110)
+static void lf_int_spa(double dz, int ns, int nb, int nv, CMat& f, const cplx* g, const int* iv,
+                       const cplx* v, const cplx* vi, IntStats& st) {
+  CMat t1(nb, 2 * nb), m(nb, nb);
+  std::vector<int> piv;
+  invstransh(nb, t1, f, g, piv);
+  cplx* Q = t1.col(0);
+  cplx* P = t1.col(nb);
+  const size_t nn = (size_t)nb * nb;
+  for (size_t e = 0; e < nn; ++e) Q[e] = (dz / 2) * P[e];
+  for (int i = 0; i < nb; ++i) Q[(size_t)i * nb + i] = Q[(size_t)i * nb + i] + 1.0;
+  bool x_is_id = false;
+  for (int l = 1; l <= ns; ++l) {
+    vvi2mate(nb, nv, v + (size_t)(l - 1) * nv, vi + (size_t)(l - 1) * nv, iv, g, m);
+    if (x_is_id) {
+      for (size_t e = 0; e < nn; ++e) P[e] = P[e] + dz * m.a[e];
+    } else {
+      zgemm('N', 'N', nb, nb, nb, cplx(1, 0) * dz, Q, nb, m.data(), nb, 1.0, P, nb);
+      st.gemms++;
+    }
+    double dz2 = (l == ns) ? dz / 2 : dz;
+    if (x_is_id) {
+      for (size_t e = 0; e < nn; ++e) Q[e] = dz2 * P[e];
+      for (int i = 0; i < nb; ++i) Q[(size_t)i * nb + i] = Q[(size_t)i * nb + i] + 1.0;
+    } else {
+      for (size_t e = 0; e < nn; ++e) Q[e] = Q[e] + dz2 * P[e];
+    }
+    double d = cond_est(nb, Q);
+    if (d > 1e3 || l == ns) {
+      if (l != ns) st.renorm++;
+      matAbdivB(nb, t1.data(), nb, piv);
+      x_is_id = true;
+    } else {
+      x_is_id = false;
+    }
+  }
+  stransh(nb, t1, g, piv);
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) f(i, j) = std::conj(t1(j, nb + i));
+}
+
+// m2_int_spa: second-order Magnus (surf_magnus.f90:114-178)
+static void m2_int_spa(double dz, int ns, int nb, int nv, CMat& f, const cplx* g, const int* iv,
+                       const cplx* v, const cplx* vi, IntStats& st) {
+  CMat t1(nb, 2 * nb), m(nb, nb), r(nb, nb), rp(nb, nb), q(nb, nb);
+  std::vector<int> piv;
+  invstransh(nb, t1, f, g, piv);
+  cplx* Q = t1.col(0);
+  cplx* P = t1.col(nb);
+  const size_t nn = (size_t)nb * nb;
+  bool x_is_id = true;
+  for (int l = 1; l <= ns; ++l) {
+    vvi2mate(nb, nv, v + (size_t)(l - 1) * nv, vi + (size_t)(l - 1) * nv, iv, g, m);
+    hyperbolic_exp4r(dz, nb, m, q, r);
+    if (x_is_id) {
+      for (size_t e = 0; e < nn; ++e) P[e] = P[e] + r.a[e] + rp.a[e];
+    } else {
+      for (size_t e = 0; e < nn; ++e) rp.a[e] = rp.a[e] + r.a[e];
+      zgemm('N', 'N', nb, nb, nb, 1.0, Q, nb, rp.data(), nb, 1.0, P, nb);
+    }
+    rp.a = r.a;
+    if (x_is_id) {
+      zgemm('N', 'N', nb, nb, nb, 1.0, P, nb, q.data(), nb, 0.0, Q, nb);
+      for (int i = 0; i < nb; ++i) Q[(size_t)i * nb + i] = Q[(size_t)i * nb + i] + 1.0;
+    } else {
+      zgemm('N', 'N', nb, nb, nb, 1.0, P, nb, q.data(), nb, 1.0, Q, nb);
+    }
+    double d = cond_est(nb, Q);
+    if (d > 1e3 || l == ns) {
+      if (l != ns) st.renorm++;
+      matAbdivB(nb, t1.data(), nb, piv);
+      x_is_id = true;
+    } else {
+      x_is_id = false;
+    }
+  }
+  for (size_t e = 0; e < nn; ++e) P[e] = P[e] + rp.a[e];
+  stransh(nb, t1, g, piv);
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) f(i, j) = std::conj(t1(j, nb + i));
+}
+
+// m4_int_spa: fourth-order Magnus (surf_magnus.f90:180-251)
+static void m4_int_spa(double dz, int ns, int nb, int nv, CMat& f, const cplx* g, const int* iv,
+                       const cplx* v, const cplx* vi, IntStats& st) {
+  const double c0 = std::sqrt(15.0) / 36, c1 = 5.0 / 36;
+  CMat t1(nb, 2 * nb), m1(nb, nb), m2(nb, nb), m3(nb, nb), rp(nb, nb), r(nb, nb), q(nb, nb);
+  std::vector<int> piv;
+  invstransh(nb, t1, f, g, piv);
+  cplx* Q = t1.col(0);
+  cplx* P = t1.col(nb);
+  const size_t nn = (size_t)nb * nb;
+  bool x_is_id = true;
+  for (int l = 1; l <= ns; ++l) {
+    vvi2mate(nb, nv, v + (size_t)(3 * l - 3) * nv, vi + (size_t)(3 * l - 3) * nv, iv, g, m1);
+    vvi2mate(nb, nv, v + (size_t)(3 * l - 2) * nv, vi + (size_t)(3 * l - 2) * nv, iv, g, m2);
+    vvi2mate(nb, nv, v + (size_t)(3 * l - 1) * nv, vi + (size_t)(3 * l - 1) * nv, iv, g, m3);
+    for (size_t e = 0; e < nn; ++e) {
+      cplx rr = m3.a[e] - m1.a[e];
+      m3.a[e] = m1.a[e] - 2.0 * m2.a[e] + m3.a[e];
+      m1.a[e] = rr;
+    }
+    hyperbolic_exp4r(dz, nb, m2, q, r);
+    for (size_t e = 0; e < nn; ++e) rp.a[e] = rp.a[e] + r.a[e] + dz * (-c0 * m1.a[e] + c1 * m3.a[e]);
+    if (x_is_id) {
+      for (size_t e = 0; e < nn; ++e) P[e] = P[e] + rp.a[e];
+    } else {
+      zgemm('N', 'N', nb, nb, nb, 1.0, Q, nb, rp.data(), nb, 1.0, P, nb);
+    }
+    if (x_is_id) {
+      zgemm('N', 'N', nb, nb, nb, 1.0, P, nb, q.data(), nb, 0.0, Q, nb);
+      for (int i = 0; i < nb; ++i) Q[(size_t)i * nb + i] = Q[(size_t)i * nb + i] + 1.0;
+    } else {
+      zgemm('N', 'N', nb, nb, nb, 1.0, P, nb, q.data(), nb, 1.0, Q, nb);
+    }
+    for (size_t e = 0; e < nn; ++e) rp.a[e] = r.a[e] + dz * (c0 * m1.a[e] + c1 * m3.a[e]);
+    double d = cond_est(nb, Q);
+    if (d > 1e3 || l == ns) {
+      if (l != ns) st.renorm++;
+      matAbdivB(nb, t1.data(), nb, piv);
+      x_is_id = true;
+    } else {
+      x_is_id = false;
+    }
+  }
+  for (size_t e = 0; e < nn; ++e) P[e] = P[e] + rp.a[e];
+  stransh(nb, t1, g, piv);
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) f(i, j) = std::conj(t1(j, nb + i));
+}
+
+// m6_int_spa: sixth-order Magnus (surf_magnus.f90:253-339)
+static void m6_int_spa(double dz, int ns, int nb, int nv, CMat& f, const cplx* g, const int* iv,
+                       const cplx* v, const cplx* vi, IntStats& st) {
+  const double c0 = std::sqrt(15.0) / 180, c1 = 1.0 / 18, c2 = 1.0 / 12960;
+  const double d0 = 4.0 / (3.0 * std::sqrt(15.0)), d1 = 1.0 / 6;
+  CMat t1(nb, 2 * nb), m1(nb, nb), m2(nb, nb), m3(nb, nb), tt(nb, nb), rp(nb, nb), r(nb, nb),
+      q(nb, nb);
+  std::vector<int> piv;
+  invstransh(nb, t1, f, g, piv);
+  cplx* Q = t1.col(0);
+  cplx* P = t1.col(nb);
+  const size_t nn = (size_t)nb * nb;
+  bool x_is_id = true;
+  for (int l = 1; l <= ns; ++l) {
+    vvi2mate(nb, nv, v + (size_t)(3 * l - 3) * nv, vi + (size_t)(3 * l - 3) * nv, iv, g, m1);
+    vvi2mate(nb, nv, v + (size_t)(3 * l - 2) * nv, vi + (size_t)(3 * l - 2) * nv, iv, g, m2);
+    vvi2mate(nb, nv, v + (size_t)(3 * l - 1) * nv, vi + (size_t)(3 * l - 1) * nv, iv, g, m3);
+    for (size_t e = 0; e < nn; ++e) {
+      r.a[e] = m3.a[e] - m1.a[e];
+      q.a[e] = m1.a[e] - 2.0 * m2.a[e] + m3.a[e];
+      m1.a[e] = r.a[e];
+      m2.a[e] = m2.a[e] + d1 * q.a[e];
+    }
+    zgemm('N', 'N', nb, nb, nb, cplx(1, 0) * c2 * (dz * dz * dz), m1.data(), nb, m1.data(), nb,
+          0.0, m3.data(), nb);
+    for (size_t e = 0; e < nn; ++e) m3.a[e] = m3.a[e] + c1 * dz * q.a[e];
+    for (size_t e = 0; e < nn; ++e) tt.a[e] = m2.a[e] - d0 * m1.a[e];
+    hyperbolic_exp6r(dz / 2, nb, tt, q, r);
+    for (size_t e = 0; e < nn; ++e) rp.a[e] = rp.a[e] + r.a[e] - (c0 * dz) * m1.a[e] + m3.a[e];
+    if (x_is_id) {
+      for (size_t e = 0; e < nn; ++e) P[e] = P[e] + rp.a[e];
+    } else {
+      zgemm('N', 'N', nb, nb, nb, 1.0, Q, nb, rp.data(), nb, 1.0, P, nb);
+    }
+    if (x_is_id) {
+      zgemm('N', 'N', nb, nb, nb, 1.0, P, nb, q.data(), nb, 0.0, Q, nb);
+      for (int i = 0; i < nb; ++i) Q[(size_t)i * nb + i] = Q[(size_t)i * nb + i] + 1.0;
+    } else {
+      zgemm('N', 'N', nb, nb, nb, 1.0, P, nb, q.data(), nb, 1.0, Q, nb);
+    }
+    rp.a = r.a;
+    for (size_t e = 0; e < nn; ++e) tt.a[e] = m2.a[e] + d0 * m1.a[e];
+    hyperbolic_exp6r(dz / 2, nb, tt, q, r);
+    for (size_t e = 0; e < nn; ++e) rp.a[e] = rp.a[e] + r.a[e];
+    zgemm('N', 'N', nb, nb, nb, 1.0, Q, nb, rp.data(), nb, 1.0, P, nb);
+    zgemm('N', 'N', nb, nb, nb, 1.0, P, nb, q.data(), nb, 1.0, Q, nb);
+    for (size_t e = 0; e < nn; ++e) rp.a[e] = r.a[e] + (dz * c0) * m1.a[e] + m3.a[e];
+    double d = cond_est(nb, Q);
+    if (d > 1e3 || l == ns) {
+      if (l != ns) st.renorm++;
+      matAbdivB(nb, t1.data(), nb, piv);
+      x_is_id = true;
+    } else {
+      x_is_id = false;
+    }
+  }
+  for (size_t e = 0; e < nn; ++e) P[e] = P[e] + rp.a[e];
+  stransh(nb, t1, g, piv);
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) f(i, j) = std::conj(t1(j, nb + i));
+}
+
+// rk4_int: classical RK4 in [X^H, Y^H] form (surf_rk.f90:27-91)
+static void rk4_int(double dz, int ns, int nb, int nv, CMat& f, const cplx* g, const int* iv,
+                    const cplx* v, const cplx* vi, IntStats& st) {
+  CMat t1(nb, 2 * nb), t2(nb, 2 * nb), k1(nb, 2 * nb), k2(nb, 2 * nb), k3(nb, 2 * nb),
+      k4(nb, 2 * nb), m0(nb, nb), m1(nb, nb), m2(nb, nb);
+  std::vector<int> piv;
+  invstransh(nb, t1, f, g, piv);
+  const size_t nn = (size_t)nb * nb, n2 = 2 * nn;
+  auto setid = [&](CMat& t) {
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) t(i, j) = (i == j) ? 1.0 : 0.0;
+  };
+  setid(t1);
+  bool x_is_id = true;
+  vvi2mate(nb, nv, v, vi, iv, g, m2);
+  for (int l = 1; l <= ns; ++l) {
+    m0.a = m2.a;
+    vvi2mate(nb, nv, v + (size_t)(2 * l - 1) * nv, vi + (size_t)(2 * l - 1) * nv, iv, g, m1);
+    vvi2mate(nb, nv, v + (size_t)(2 * l) * nv, vi + (size_t)(2 * l) * nv, iv, g, m2);
+    std::copy(t1.col(nb), t1.col(nb) + nn, k1.col(0));
+    if (x_is_id)
+      std::copy(m0.a.begin(), m0.a.end(), k1.col(nb));
+    else
+      zgemm('N', 'N', nb, nb, nb, 1.0, t1.col(0), nb, m0.data(), nb, 0.0, k1.col(nb), nb);
+    for (size_t e = 0; e < n2; ++e) t2.a[e] = t1.a[e] + 0.5 * dz * k1.a[e];
+    std::copy(t2.col(nb), t2.col(nb) + nn, k2.col(0));
+    zgemm('N', 'N', nb, nb, nb, 1.0, t2.col(0), nb, m1.data(), nb, 0.0, k2.col(nb), nb);
+    for (size_t e = 0; e < n2; ++e) t2.a[e] = t1.a[e] + 0.5 * dz * k2.a[e];
+    std::copy(t2.col(nb), t2.col(nb) + nn, k3.col(0));
+    zgemm('N', 'N', nb, nb, nb, 1.0, t2.col(0), nb, m1.data(), nb, 0.0, k3.col(nb), nb);
+    for (size_t e = 0; e < n2; ++e) t2.a[e] = t1.a[e] + dz * k3.a[e];
+    std::copy(t2.col(nb), t2.col(nb) + nn, k4.col(0));
+    zgemm('N', 'N', nb, nb, nb, 1.0, t2.col(0), nb, m2.data(), nb, 0.0, k4.col(nb), nb);
+    for (size_t e = 0; e < n2; ++e)
+      t1.a[e] = t1.a[e] + (dz / 6) * (k1.a[e] + 2.0 * k2.a[e] + 2.0 * k3.a[e] + k4.a[e]);
+    double d = cond_est(nb, t1.col(0));
+    if (d > 1e3 || l == ns) {
+      if (l != ns) st.renorm++;
+      matAbdivB(nb, t1.data(), nb, piv);
+      setid(t1);
+      x_is_id = true;
+    } else {
+      x_is_id = false;
+    }
+  }
+  stransh(nb, t1, g, piv);
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) f(i, j) = std::conj(t1(j, nb + i));
+}
+
+// ---------------------------------------------------------------- surface model
+// mod_scpot3 + surfio state (sim-trhepd-rheed/src/surfio.f90:18-58, 60-381)
+struct SurfModel {
+  // header of bulkP.b
+  int ndom = 1, inegpos = 1, isym = 0, nh = 1, nk = 1, iabr = 0, iabp = 1, iabe = 0, idiag = 3;
+  std::vector<int> nbd;
+  std::vector<double> rdom, wdom;
+  std::vector<int> ih, ik;
+  double be = 10, azi = 0, daz = 0, gi = 0, dg = 0, tem = 0, dz = 0, epsb = 1e-10;
+  int naz = 1, ng = 1, ml = 100;
+  int nsgb = 1, mp = 0;
+  double aa = 0, bb = 0, gam = 0, cc = 0, dxb = 0, dyb = 0, zoffset = 0;
+  int nelmb = 0, natmb = 0;
+  // surface
+  int nelms = 0, natms = 0, nsgs = 1, msa = 1, msb = 0, nsa = 0, nsb = 1;
+  double dthick = 0, dxs = 0, dys = 0;
+  Elements E;
+  std::vector<int> ielm;
+  std::vector<double> ocr, x, y, z;
+  int ns = 0;
+  double dzs = 0;  // surface slice thickness after surfio's rounding
+  double wn = 0, ghx = 0, ghy = 0, gky = 0, smesh = 1;
+  // per domain (only the first is used by the solve entry points)
+  struct Domain {
+    std::vector<int> iord, nbg, igh, igk, iv;
+    int ngr = 0, nvb = 0, nv = 0;
+    std::vector<double> asf, Ghk, gh, gk;
+    std::vector<cplx> st0, st1, st2;
+    std::vector<cplx> fbulk;  // all t4 records in file order, packed
+    std::vector<size_t> rec_off;
+  };
+  std::vector<Domain> dom;
+
+  // comp_scpot (surfio.f90:29-41)
+  void comp_scpot(const Domain& D, double zi, cplx* v, cplx* vi) const {
+    const int nv = D.nv, nvb = D.nvb;
+    std::fill(v, v + nv, cplx(0, 0));
+    std::fill(vi, vi + nv, cplx(0, 0));
+    scpot(nv, nv, v, vi, natms, ielm.data() + natmb, z.data() + natmb, zi - cc, E, D.asf, 1.0,
+          D.Ghk, ocr.data() + natmb, D.st0.data());
+    scpot(nv, nvb, v, vi, natmb, ielm.data(), z.data(), zi, E, D.asf, smesh, D.Ghk, ocr.data(),
+          D.st1.data());
+    scpot(nv, nvb, v, vi, natmb, ielm.data(), z.data(), zi + cc, E, D.asf, smesh, D.Ghk,
+          ocr.data(), D.st2.data());
+  }
+};
+
+// surfio input half: bulkP.b header + surf.txt (surfio.f90:97-210, 261-267, 291-326)
+static void load_surface(const std::string& bulkp, const std::string& surf, double dz2,
+                         SurfModel& S) {
+  RecordReader R(bulkp);
+  R.next();
+  S.ndom = R.get<int32_t>();
+  R.next();
+  S.inegpos = R.get<int32_t>();
+  S.isym = R.get<int32_t>();
+  S.nh = R.get<int32_t>();
+  S.nk = R.get<int32_t>();
+  S.iabr = R.get<int32_t>();
+  S.iabp = R.get<int32_t>();
+  S.iabe = R.get<int32_t>();
+  int nabr = R.get<int32_t>();
+  int nabi = R.get<int32_t>();
+  S.idiag = R.get<int32_t>();
+  S.nbd.resize(S.ndom);
+  S.rdom.resize(S.ndom);
+  S.wdom.assign(S.ndom, 1.0);
+  R.next();
+  int nbt = 0;
+  for (int i = 0; i < S.ndom; ++i) {
+    S.nbd[i] = R.get<int32_t>();
+    S.rdom[i] = R.get<double>();
+    nbt += S.nbd[i];
+  }
+  R.next();
+  S.ih.resize(nbt);
+  S.ik.resize(nbt);
+  for (int j = 0; j < nbt; ++j) {
+    S.ih[j] = R.get<int32_t>();
+    S.ik[j] = R.get<int32_t>();
+  }
+  R.next();
+  S.be = R.get<double>();
+  S.azi = R.get<double>();
+  S.daz = R.get<double>();
+  S.naz = R.get<int32_t>();
+  S.gi = R.get<double>();
+  S.dg = R.get<double>();
+  S.ng = R.get<int32_t>();
+  R.next();
+  S.tem = R.get<double>();
+  S.dz = R.get<double>();
+  S.ml = R.get<int32_t>();
+  S.epsb = R.get<double>();
+  R.next();
+  S.nsgb = R.get<int32_t>();
+  S.mp = R.get<int32_t>();
+  S.aa = R.get<double>();
+  S.bb = R.get<double>();
+  S.gam = R.get<double>();
+  S.cc = R.get<double>();
+  S.dxb = R.get<double>();
+  S.dyb = R.get<double>();
+  S.zoffset = R.get<double>();
+  R.next();
+  S.nelmb = R.get<int32_t>();
+  S.natmb = R.get<int32_t>();
+
+  ListReader T(surf);
+  S.nelms = T.ints(1)[0];
+  int nelm = S.nelmb + S.nelms;
+  S.E.resize(nelm);
+  S.E.nabr = nabr;
+  S.E.nabi = nabi;
+  for (int i = 0; i < S.nelmb; ++i) {
+    R.next();
+    for (int j = 0; j < nabr + nabi; ++j) S.E.A(j, i) = R.get<double>();
+    for (int j = 0; j < nabr + nabi; ++j) S.E.B(j, i) = R.get<double>();
+    R.next();
+    S.E.dth[i] = R.get<double>();
+    S.E.dtk[i] = R.get<double>();
+    S.E.dtz[i] = R.get<double>();
+    S.E.elm[i] = R.get<double>();
+    S.E.dchg[i] = R.get<double>();
+  }
+  for (int i = S.nelmb; i < nelm; ++i) {
+    auto l1 = T.read(3);
+    int iz = std::stoi(l1[0]);
+    double da1 = ListReader::to_real(l1[1]), sap = ListReader::to_real(l1[2]);
+    S.E.dchg[i] = 0.0;
+    S.E.elm[i] = amass(iz);
+    double a4[4], b4[4];
+    int nr = asfparam(iz, S.iabr, a4, b4);
+    if (nr <= 0) throw std::runtime_error("surf.txt: unknown element");
+    S.E.nabr = nr;
+    for (int j = 0; j < 4; ++j) {
+      S.E.A(j, i) = a4[j];
+      S.E.B(j, i) = b4[j];
+    }
+    S.E.A(0, i) = S.E.A(0, i) - da1;
+    if (S.inegpos > 0)
+      for (int j = 0; j < S.E.nabr; ++j) S.E.A(j, i) = -S.E.A(j, i);
+    S.E.nabi = 1;
+    S.E.A(S.E.nabr, i) = sap;
+    S.E.B(S.E.nabr, i) = 0.0;
+    auto d3 = T.reals(3);
+    S.E.dth[i] = std::fabs(d3[0]);
+    S.E.dtk[i] = std::fabs(d3[1]);
+    S.E.dtz[i] = std::fabs(d3[2]);
+  }
+  {
+    auto t = T.read(8);
+    S.nsgs = std::stoi(t[0]);
+    S.msa = std::stoi(t[1]);
+    S.msb = std::stoi(t[2]);
+    S.nsa = std::stoi(t[3]);
+    S.nsb = std::stoi(t[4]);
+    S.dthick = ListReader::to_real(t[5]);
+    S.dxs = ListReader::to_real(t[6]);
+    S.dys = ListReader::to_real(t[7]);
+  }
+  S.natms = T.ints(1)[0];
+  int natm = S.natmb + S.natms;
+  S.ielm.resize(natm);
+  S.ocr.resize(natm);
+  S.x.resize(natm);
+  S.y.resize(natm);
+  S.z.resize(natm);
+  for (int i = 0; i < S.natmb; ++i) {
+    R.next();
+    S.ielm[i] = R.get<int32_t>();
+    S.ocr[i] = R.get<double>();
+    S.x[i] = R.get<double>();
+    S.y[i] = R.get<double>();
+    S.z[i] = R.get<double>();
+  }
+  for (int i = S.natmb; i < natm; ++i) {
+    auto t = T.read(5);
+    S.ielm[i] = std::stoi(t[0]);
+    S.ocr[i] = ListReader::to_real(t[1]);
+    S.x[i] = ListReader::to_real(t[2]);
+    S.y[i] = ListReader::to_real(t[3]);
+    S.z[i] = ListReader::to_real(t[4]);
+    if (S.ielm[i] >= -S.nelmb && S.ielm[i] <= -1)
+      S.ielm[i] = -S.ielm[i];
+    else if (S.ielm[i] >= 1 && S.ielm[i] <= S.nelms)
+      S.ielm[i] = S.ielm[i] + S.nelmb;
+    else
+      throw std::runtime_error("surf.txt: bad element index");
+    S.z[i] = S.z[i] + S.zoffset;
+  }
+  if (S.ndom > 1) {
+    auto w = T.reals(S.ndom);
+    S.wdom = w;
+  }
+  // surface slices (surfio.f90:198-210)
+  if (S.nsgs < 1) {
+    S.ns = 0;
+    S.dzs = S.dz;
+  } else {
+    double zz = 0.0;
+    for (int i = S.natmb; i < natm; ++i)
+      if (S.z[i] > zz) zz = S.z[i];
+    int ns2 = (int)((zz + S.dthick + S.cc) / S.dz) + 1;
+    S.ns = (int)std::lround((S.dz * ns2) / dz2);
+    S.dzs = (S.dz * ns2) / S.ns;
+  }
+  const double pi = kPi;
+  S.smesh = std::fabs((double)(S.msa * S.nsb - S.msb * S.nsa));
+  S.wn = asfcrr(S.be, S.E, S.tem, S.aa * S.bb * std::sin(S.gam) * S.smesh);
+  S.ghx = (pi + pi) / (S.aa * S.nh);
+  S.ghy = -(pi + pi) / (S.aa * std::tan(S.gam) * S.nh);
+  S.gky = (pi + pi) / (S.bb * std::sin(S.gam) * S.nk);
+
+  // per domain: beam tables, form factors, structure factors, bulk records
+  int ibt = 0;
+  S.dom.resize(S.ndom);
+  for (int idom = 0; idom < S.ndom; ++idom) {
+    auto& D = S.dom[idom];
+    int nb = S.nbd[idom];
+    R.next();
+    D.iord.resize(nb);
+    for (int i = 0; i < nb; ++i) D.iord[i] = R.get<int32_t>();
+    R.next();
+    D.ngr = R.get<int32_t>();
+    D.nvb = R.get<int32_t>();
+    int nvm = 1 + nb * (nb - 1) / 2;
+    if (D.nvb > nvm) throw std::runtime_error("bulk file: nvb > nvm");
+    R.next();
+    D.nbg.resize(D.ngr);
+    for (int i = 0; i < D.ngr; ++i) D.nbg[i] = R.get<int32_t>();
+    R.next();
+    D.igh.assign(nvm, 0);
+    D.igk.assign(nvm, 0);
+    for (int i = 0; i < D.nvb; ++i) {
+      D.igh[i] = R.get<int32_t>();
+      D.igk[i] = R.get<int32_t>();
+    }
+    D.nv = srfghk(nvm, D.nvb, D.igh, D.igk, nb, S.ih.data() + ibt, S.ik.data() + ibt, D.iv);
+    asfcef(D.nv, D.igh, D.igk, S.ghx, S.ghy, S.gky, S.E, D.asf, D.Ghk);
+    D.gh.resize(D.nv);
+    D.gk.resize(D.nv);
+    for (int i = 0; i < D.nv; ++i) {
+      D.gh[i] = (-(pi + pi) / S.nh) * (double)D.igh[i];
+      D.gk[i] = (-(pi + pi) / S.nk) * (double)D.igk[i];
+    }
+    scpot_stf(S.natms, D.nv, S.nsgs, S.msa, S.msb, S.nsa, S.nsb, D.gh, D.gk,
+              S.x.data() + S.natmb, S.y.data() + S.natmb, S.dxs + S.dxb, S.dys + S.dyb, D.st0);
+    scpot_stf(S.natmb, D.nvb, S.nsgb, 1, 0, 0, 1, D.gh, D.gk, S.x.data(), S.y.data(), S.dxb,
+              S.dyb, D.st1);
+    scpot_stf(S.natmb, D.nvb, S.nsgb, 1, 0, 0, 1, D.gh, D.gk, S.x.data(), S.y.data(), 0.0, 0.0,
+              D.st2);
+    // bulk reflection records: nrep1*nrep2 angles, each ngr blocks (surflf.f90:65-72)
+    int nrep = S.naz * S.ng;
+    size_t per = 0;
+    for (int l = 0; l < D.ngr; ++l) per += (size_t)D.nbg[l] * D.nbg[l];
+    D.fbulk.resize(per * nrep);
+    D.rec_off.resize(nrep);
+    for (int r = 0; r < nrep; ++r) {
+      D.rec_off[r] = per * r;
+      size_t o = per * r;
+      for (int l = 0; l < D.ngr; ++l) {
+        R.next();
+        for (size_t e = 0; e < (size_t)D.nbg[l] * D.nbg[l]; ++e) {
+          double re = R.get<double>(), im = R.get<double>();
+          D.fbulk[o++] = cplx(re, im);
+        }
+      }
+    }
+    ibt += nb;
+  }
+}
+
+// Stage depth tables of each integrator (surf_prkn.f90:174-197, surf_magnus.f90:4-42,
+// surf_rk.f90:4-25).  Returns the column count.
+static int build_potential(const SurfModel& S, const SurfModel::Domain& D, int method,
+                           std::vector<cplx>& v, std::vector<cplx>& vi) {
+  const int nv = D.nv, ns = S.ns;
+  const double dz = S.dzs;
+  std::vector<double> depth;
+  switch (method) {
+    case 1:
+    case 4:
+      for (int l = 1; l <= ns; ++l) depth.push_back(dz * (l - 0.5));
+      break;
+    case 2:
+    case 3: {
+      const double c0 = (5.0 - std::sqrt(15.0)) / 10, c1 = 0.5, c2 = (5.0 + std::sqrt(15.0)) / 10;
+      for (int l = 1; l <= ns; ++l) {
+        depth.push_back(dz * ((l - 1) + c0));
+        depth.push_back(dz * ((l - 1) + c1));
+        depth.push_back(dz * ((l - 1) + c2));
+      }
+      break;
+    }
+    case 5:
+    case 6: {
+      int s = (method == 5) ? 6 : 11;
+      const double* bab = (method == 5) ? kRkn46 : kRkn611;
+      for (int l = 1; l <= ns; ++l) {
+        double iz = dz * (l - 1);
+        for (int k = 1; k <= s; ++k) {
+          depth.push_back(iz);
+          iz = iz + dz * bab[2 * k - 1];
+        }
+      }
+      depth.push_back(dz * ns);
+      break;
+    }
+    case 7:
+      for (int l = 1; l <= ns; ++l) {
+        double iz = dz * (l - 1);
+        depth.push_back(iz);
+        depth.push_back(iz + 0.5 * dz);
+      }
+      depth.push_back(dz * ns);
+      break;
+    default:
+      throw std::runtime_error("int_method must be 1..7");
+  }
+  int ncol = (int)depth.size();
+  v.assign((size_t)nv * ncol, cplx(0, 0));
+  vi.assign((size_t)nv * ncol, cplx(0, 0));
+#pragma omp parallel for schedule(dynamic)
+  for (int c = 0; c < ncol; ++c)
+    S.comp_scpot(D, depth[c], v.data() + (size_t)c * nv, vi.data() + (size_t)c * nv);
+  return ncol;
+}
+
+// one (azimuth, angle) surface solve: gamma, bulk f permutation, integrator,
+// intensities (surflf.f90:79-151)
+static void solve_one(const SurfModel& S, const SurfModel::Domain& D, int nb, const int* ih,
+                      const int* ik, int method, const cplx* v, const cplx* vi, double ga,
+                      double az, const cplx* rec, double* f2, IntStats& st) {
+  double cga = std::cos(ga), sga = std::sin(ga), caz = std::cos(az), saz = std::sin(az);
+  double wn = S.wn;
+  double wnsga2 = wn * sga * sga, wnx = wn * cga * caz, wny = wn * cga * saz;
+  std::vector<cplx> gma(nb);
+  for (int i = 0; i < nb; ++i) {
+    double wgx = S.ghx * ih[i] + wnx;
+    double wgy = S.ghy * ih[i] + S.gky * ik[i] + wny;
+    double s = wn * wn - wgx * wgx - wgy * wgy;
+    gma[i] = (s >= 0.0) ? cplx(std::sqrt(s), 0.0) : cplx(0.0, std::sqrt(-s));
+  }
+  CMat f(nb, nb);
+  {
+    int ib1 = 0;
+    size_t o = 0;
+    for (int l = 0; l < D.ngr; ++l) {
+      int n = D.nbg[l];
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) f(D.iord[ib1 + i] - 1, D.iord[ib1 + j] - 1) = rec[o++];
+      ib1 += n;
+    }
+  }
+  const int nv = D.nv;
+  const int* iv = D.iv.data();
+  switch (method) {
+    case 1:
+      m2_int_spa(S.dzs, S.ns, nb, nv, f, gma.data(), iv, v, vi, st);
+      break;
+    case 2:
+      m4_int_spa(S.dzs, S.ns, nb, nv, f, gma.data(), iv, v, vi, st);
+      break;
+    case 3:
+      m6_int_spa(S.dzs, S.ns, nb, nv, f, gma.data(), iv, v, vi, st);
+      break;
+    case 4:
+      lf_int_spa(S.dzs, S.ns, nb, nv, f, gma.data(), iv, v, vi, st);
+      break;
+    case 5:
+      hp_int_spa(S.dzs, S.ns, nb, nv, f, gma.data(), iv, v, vi, 6, kRkn46, st);
+      break;
+    case 6:
+      if (nb == 1)
+        hp_int_spa1d(S.dzs, S.ns, f(0, 0), gma[0], v, vi, 11, kRkn611);
+      else
+        hp_int_spa(S.dzs, S.ns, nb, nv, f, gma.data(), iv, v, vi, 11, kRkn611, st);
+      break;
+    case 7:
+      rk4_int(S.dzs, S.ns, nb, nv, f, gma.data(), iv, v, vi, st);
+      break;
+  }
+  int nb0 = 0;
+  for (int i = 0; i < nb; ++i)
+    if (ih[i] == 0 && ik[i] == 0) nb0 = i;
+  for (int i = 0; i < nb; ++i) {
+    double s = gma[i].real();
+    if (s > 1e-10) {
+      cplx a = f(i, nb0);
+      f2[i] = (a * std::conj(a)).real() * wnsga2 / s;
+    } else {
+      f2[i] = 0.0;
+    }
+  }
+}
+
+// Angle schedule of srfref (surflf.f90:43-92): the longer scan is the inner loop.
+struct AngleSchedule {
+  int nrep1, nrep2;
+  bool ng_outer;  // ng > naz
+};
+static AngleSchedule schedule(const SurfModel& S) {
+  AngleSchedule a;
+  a.ng_outer = S.ng > S.naz;
+  a.nrep1 = a.ng_outer ? S.naz : S.ng;
+  a.nrep2 = a.ng_outer ? S.ng : S.naz;
+  return a;
+}
+
+static void write_header(FILE* o, const SurfModel& S) {
+  const double deg = 180.0 / kPi;
+  if (S.ndom == 1) {
+    std::fprintf(o, "#azimuths,g-angles,beams\n");
+    std::fprintf(o, "%4d%4d%4d\n", S.naz, S.ng, S.nbd[0]);
+    std::fprintf(o, "#ih,ik\n");
+    int cnt = 0;
+    for (int j = 0; j < S.nbd[0]; ++j) {
+      std::fprintf(o, "%4d", S.ih[j]);
+      if (++cnt % 400 == 0) std::fprintf(o, "\n");
+      std::fprintf(o, "%4d", S.ik[j]);
+      if (++cnt % 400 == 0 && j + 1 < S.nbd[0]) std::fprintf(o, "\n");
+    }
+    if (cnt % 400 != 0 || cnt == 0) std::fprintf(o, "\n");
+  } else {
+    std::fprintf(o, "#azimuths,g-angles,domains,nh,nk,gam\n");
+    std::fprintf(o, "%4d%4d%4d%4d%4d%10.3f\n", S.naz, S.ng, S.ndom, S.nh, S.nk, S.gam * deg);
+    std::fprintf(o, "#beams,domain angle,domain weight\n");
+    for (int i = 0; i < S.ndom; ++i)
+      std::fprintf(o, "%4d%10.3f%s\n", S.nbd[i], S.rdom[i] * deg, fortran_E(S.wdom[i], 12, 3).c_str());
+    std::fprintf(o, "#ih,ik\n");
+    int ibt = 0;
+    for (int i = 0; i < S.ndom; ++i) {
+      int cnt = 0;
+      for (int j = ibt; j < ibt + S.nbd[i]; ++j) {
+        std::fprintf(o, "%4d", S.ih[j]);
+        if (++cnt % 400 == 0) std::fprintf(o, "\n");
+        std::fprintf(o, "%4d", S.ik[j]);
+        if (++cnt % 400 == 0 && j + 1 < ibt + S.nbd[i]) std::fprintf(o, "\n");
+      }
+      if (cnt % 400 != 0) std::fprintf(o, "\n");
+      ibt += S.nbd[i];
+    }
+  }
+}
+
+// '(E12.4,200(",",E23.15))' with format reversion (surflf.f90:162)
+static void write_row(FILE* o, double angle, const double* f2, int nb) {
+  std::string line = fortran_E(angle, 12, 4);
+  for (int i = 0; i < nb; ++i) {
+    if (i > 0 && i % 200 == 0) {
+      std::fputs(line.c_str(), o);
+      std::fputs("\n", o);
+      line.clear();
+    }
+    line += ",";
+    line += fortran_E(f2[i], 23, 15);
+  }
+  line += ",";
+  std::fputs(line.c_str(), o);
+  std::fputs("\n", o);
+}
+
+// ---------------------------------------------------------------- bulk path
+// gcmi3: a <- a * inv(b) on the leading n x n blocks (gcmi.f90:5-15)
+static void gcmi3(int n1, int n, cplx* a, cplx* b) {
+  std::vector<int> p(n);
+  zgetrf(n, n, b, n1, p.data());
+  std::vector<cplx> t((size_t)n * n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) t[(size_t)j * n + i] = a[(size_t)i * n1 + j];
+  zgetrs('T', n, n, b, n1, p.data(), t.data(), n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) a[(size_t)j * n1 + i] = t[(size_t)i * n + j];
+}
+
+// trmat: transfer matrix of one bulk slice from the eigendecomposition of the
+// slice Hamiltonian (trmatg.f90:6-59).  t1,t2,t3 are (ld x ld) column-major with
+// ld >= 2nb; iv points at the group's first column of the (nbm, nb) beam map.
+static void trmat(int nbm, int nb, const cplx* gma, const cplx* v, const cplx* vi, const int* iv,
+                  double dz, cplx* t1, cplx* t2, cplx* t3, int ld) {
+  auto T1 = [&](int i, int j) -> cplx& { return t1[(size_t)j * ld + i]; };
+  auto T2 = [&](int i, int j) -> cplx& { return t2[(size_t)j * ld + i]; };
+  auto T3 = [&](int i, int j) -> cplx& { return t3[(size_t)j * ld + i]; };
+  if (nb == 1) {
+    T2(1, 0) = v[0] + vi[0] + gma[0] * gma[0];
+    T2(0, 0) = cplx(1.0, 0.0);
+  } else {
+    for (int i = 0; i < nb; ++i) {
+      T1(i, i) = v[0] + vi[0] + gma[i] * gma[i];
+      for (int j = i + 1; j < nb; ++j) {
+        int k = iv[(size_t)i * nbm + j] - 1;
+        T1(j, i) = v[k] + vi[k];
+        T1(i, j) = std::conj(v[k] - vi[k]);
+      }
+    }
+    int n = nb, lda = ld, ldv = ld, info = 0, one = 1;
+    char jl = 'N', jr = 'V';
+    std::vector<double> rwork(2 * nb);
+    std::vector<cplx> w(nb), work((size_t)std::max(ld * ld, 4 * nb));
+    int lwork = (int)work.size();
+    cplx dummy;
+    scipy_zgeev_(&jl, &jr, &n, t1, &lda, w.data(), &dummy, &one, t2, &ldv, work.data(), &lwork,
+                 rwork.data(), &info, 1, 1);
+    if (info != 0) std::fprintf(stderr, " zgeev failed %d\n", info);
+    for (int j = 0; j < nb; ++j) T2(nb + j, nb - 1) = w[j];
+  }
+  for (int j = 0; j < nb; ++j) {
+    int j2 = j + nb;
+    cplx x2 = std::sqrt(T2(j2, nb - 1));
+    cplx ph = std::exp(cplx(0.0, dz) * x2);
+    cplx ph2 = cplx(1.0, 0.0) / ph;
+    for (int i = 0; i < nb; ++i) {
+      int i2 = i + nb;
+      cplx x1 = gma[i], x3 = T2(i, j);
+      cplx tau = (x1 + x2) * x3, rou = (x1 - x2) * x3;
+      T1(i, j) = tau * ph;
+      T1(i, j2) = rou * ph2;
+      T1(i2, j) = rou * ph;
+      T1(i2, j2) = tau * ph2;
+      T3(i, j) = tau;
+      T3(i, j2) = rou;
+      T3(i2, j) = rou;
+      T3(i2, j2) = tau;
+    }
+  }
+  gcmi3(ld, nb + nb, t1, t3);
+}
+
+// blkref for one (angle, group): slices chained into the unit-layer transfer
+// matrix, phase shift, then the layer iteration with its convergence exit
+// (bulk.f90:51-123).  Returns t4 (nbf x nbf) and the layer count used.
+static int blkref_group(int nbgm, int nbf, const int* ihg, const int* ikg, const int* ivg,
+                        int ns, const cplx* v, const cplx* vi, int nv, double dz, double epsb,
+                        int nh, int nk, int ml, double dx, double dy, double wn, double ghx,
+                        double ghy, double gky, double wnx, double wny, cplx* t4out) {
+  const double pi2 = std::atan(1.0) * 8.0;
+  const int n2 = nbf + nbf, ld = n2;
+  std::vector<cplx> gma(nbf);
+  for (int i = 0; i < nbf; ++i) {
+    double wgx = ghx * ihg[i] + wnx;
+    double wgy = ghy * ihg[i] + gky * ikg[i] + wny;
+    double s = wn * wn - wgx * wgx - wgy * wgy;
+    gma[i] = (s >= 0.0) ? cplx(std::sqrt(s), 0.0) : cplx(0.0, std::sqrt(-s));
+  }
+  std::vector<cplx> t1((size_t)ld * ld), t2((size_t)ld * ld), t3((size_t)ld * ld),
+      t4((size_t)ld * ld);
+  for (int l = 1; l <= ns; ++l) {
+    std::fill(t1.begin(), t1.end(), cplx(0, 0));
+    std::fill(t2.begin(), t2.end(), cplx(0, 0));
+    trmat(nbgm, nbf, gma.data(), v + (size_t)(l - 1) * nv, vi + (size_t)(l - 1) * nv, ivg, dz,
+          t1.data(), t2.data(), t3.data(), ld);
+    if (ns == 1) {
+      t3 = t1;
+    } else if (l == 1) {
+      t4 = t1;
+    } else {
+      zgemm('N', 'N', n2, n2, n2, 1.0, t1.data(), ld, t4.data(), ld, 0.0, t3.data(), ld);
+      if (l < ns) t4 = t3;
+    }
+  }
+  auto T3 = [&](int i, int j) -> cplx& { return t3[(size_t)j * ld + i]; };
+  auto T4 = [&](int i, int j) -> cplx& { return t4[(size_t)j * ld + i]; };
+  if (std::fabs(dx) > 1e-4 || std::fabs(dy) > 1e-4) {
+    double pih = dx * pi2 / nh, pik = dy * pi2 / nk;
+    for (int j = 0; j < nbf; ++j) {
+      double s = pih * ihg[j] + pik * ikg[j];
+      cplx ph(std::cos(s), std::sin(s));
+      for (int i = 0; i < n2; ++i) {
+        T3(i, j) = T3(i, j) * ph;
+        T3(i, j + nbf) = T3(i, j + nbf) * ph;
+      }
+    }
+  }
+  std::vector<double> r20(nbf, 0.0);
+  std::vector<cplx> a((size_t)ld * ld), b((size_t)ld * ld);
+  auto A = [&](int i, int j) -> cplx& { return a[(size_t)j * ld + i]; };
+  auto Bm = [&](int i, int j) -> cplx& { return b[(size_t)j * ld + i]; };
+  int l;
+  for (l = 1; l <= ml; ++l) {
+    for (int j = 0; j < nbf; ++j)
+      for (int i = 0; i < nbf; ++i) {
+        A(i, j) = T3(i, nbf + j);
+        Bm(i, j) = T3(nbf + i, nbf + j);
+      }
+    if (l > 1) {
+      zgemm('N', 'N', nbf, nbf, nbf, 1.0, t3.data(), ld, t4.data(), ld, 1.0, a.data(), ld);
+      zgemm('N', 'N', nbf, nbf, nbf, 1.0, t3.data() + nbf, ld, t4.data(), ld, 1.0, b.data(), ld);
+    }
+    gcmi3(ld, nbf, a.data(), b.data());
+    for (int j = 0; j < nbf; ++j)
+      for (int i = 0; i < nbf; ++i) T4(i, j) = A(i, j);
+    if (l == 20) {
+      for (int i = 0; i < nbf; ++i) r20[i] = (T4(i, i) * std::conj(T4(i, i))).real();
+    } else if (l > 20) {
+      double rmax = 0.0;
+      for (int i = 0; i < nbf; ++i) {
+        double r2 = (T4(i, i) * std::conj(T4(i, i))).real();
+        double rat = std::fabs(r2 - r20[i]);
+        if (rat > rmax) rmax = rat;
+        r20[i] = r2;
+      }
+      if (rmax < epsb) break;
+    }
+  }
+  for (int j = 0; j < nbf; ++j)
+    for (int i = 0; i < nbf; ++i) t4out[(size_t)j * nbf + i] = T4(i, j);
+  return std::min(l, ml);
+}
+
+// bulk.exe (bulkm.f90:207-256 + bulkio.f90:10-223 + blkref): bulk.txt -> bulkP.b,
+// positron mode (bulkm.f90:222-225).
+static void bulk_run(const std::string& bulk_txt, const std::string& out_path) {
+  ListReader T(bulk_txt);
+  const int inegpos = 1, idiag = 3, isym = 0, iabr = 0, iabp = 1, iabe = 0;
+  auto h3 = T.ints(3);
+  int nh = h3[0], nk = h3[1], ndom = h3[2];
+  if (nh < 1 || nk < 1 || ndom < 1) throw std::runtime_error("bulk.txt: bad NH/NK/NDOM");
+  auto nbv = T.ints(ndom);
+  int nbt = 0;
+  for (int v : nbv) {
+    if (v < 1) throw std::runtime_error("bulk.txt: NB < 1");
+    nbt += v;
+  }
+  auto rdom = T.reals(ndom);
+  std::vector<int> ih(nbt), ik(nbt);
+  int ibt = 0;
+  for (int d = 0; d < ndom; ++d) {
+    auto t = T.ints(2 * nbv[d]);
+    for (int j = 0; j < nbv[d]; ++j) {
+      ih[ibt + j] = t[2 * j];
+      ik[ibt + j] = t[2 * j + 1];
+    }
+    ibt += nbv[d];
+  }
+  auto sc = T.reals(7);
+  double be = sc[0], azi = sc[1], azf = sc[2], daz = sc[3], gi = sc[4], gf = sc[5], dg = sc[6];
+  auto t2 = T.read(2);
+  double dz = ListReader::to_real(t2[0]);
+  int ml = std::stoi(t2[1]);
+  double tem = 0.0, epsb = 1e-10;
+  if (ml < 1 || ml > 1000) ml = 1000;
+  int nelm = T.ints(1)[0];
+  if (nelm < 1) throw std::runtime_error("bulk.txt: NELM < 1");
+  Elements E;
+  E.resize(nelm);
+  int nabr = 4, nabi = 1;
+  std::vector<double> raw_a((size_t)kMab * nelm), raw_b((size_t)kMab * nelm);
+  for (int i = 0; i < nelm; ++i) {
+    auto t = T.read(3);
+    int iz = std::stoi(t[0]);
+    double da1 = ListReader::to_real(t[1]), sap = ListReader::to_real(t[2]);
+    E.dchg[i] = 0.0;
+    E.elm[i] = amass(iz);
+    double a4[4], b4[4];
+    nabr = asfparam(iz, iabr, a4, b4);
+    if (nabr <= 0) throw std::runtime_error("bulk.txt: unknown element");
+    for (int j = 0; j < 4; ++j) {
+      E.A(j, i) = a4[j];
+      E.B(j, i) = b4[j];
+    }
+    E.A(0, i) = E.A(0, i) - da1;
+    if (inegpos > 0)
+      for (int j = 0; j < nabr; ++j) E.A(j, i) = -E.A(j, i);
+    nabi = 1;
+    E.A(nabr, i) = sap;
+    E.B(nabr, i) = 0.0;
+    auto d = T.reals(3);
+    E.dth[i] = std::fabs(d[0]);
+    E.dtk[i] = std::fabs(d[1]);
+    E.dtz[i] = std::fabs(d[2]);
+  }
+  E.nabr = nabr;
+  E.nabi = nabi;
+  auto st7 = T.read(7);
+  int nsg = std::stoi(st7[0]);
+  double aa = ListReader::to_real(st7[1]), bb = ListReader::to_real(st7[2]);
+  double gam = ListReader::to_real(st7[3]), cc = ListReader::to_real(st7[4]);
+  double dx = ListReader::to_real(st7[5]), dy = ListReader::to_real(st7[6]);
+  int mp = 0;
+  int natm = T.ints(1)[0];
+  if (natm < 1) throw std::runtime_error("bulk.txt: NATM < 1");
+  std::vector<int> ielm(natm);
+  std::vector<double> ocr(natm), x(natm), y(natm), z(natm);
+  double zmin = 1e10, zmax = -1e10;
+  for (int i = 0; i < natm; ++i) {
+    auto t = T.read(5);
+    ielm[i] = std::stoi(t[0]);
+    ocr[i] = ListReader::to_real(t[1]);
+    x[i] = ListReader::to_real(t[2]);
+    y[i] = ListReader::to_real(t[3]);
+    z[i] = ListReader::to_real(t[4]);
+    if (ielm[i] < 1 || ielm[i] > nelm) throw std::runtime_error("bulk.txt: bad IELM");
+    if (z[i] < zmin) zmin = z[i];
+    if (z[i] > zmax) zmax = z[i];
+  }
+  double zoffset = 0.5 * (cc - zmax - zmin);
+  for (auto& zz : z) zz = zz + zoffset;
+  int naz, ng;
+  scanrg(azi, azf, daz, naz, gi, gf, dg, ng);
+  const double pi = kPi, rad = pi / 180.0;
+  for (auto& r : rdom) r = r * rad;
+  gam = gam * rad;
+  int ns = (int)(cc / dz) + 1;
+  dz = cc / ns;
+  if (ns < 2) throw std::runtime_error("bulk.txt: fewer than 2 slices");
+
+  RecordWriter W(out_path);
+  W.put<int32_t>(ndom);
+  W.end_record();
+  for (int v : {inegpos, isym, nh, nk, iabr, iabp, iabe, nabr, nabi, idiag}) W.put<int32_t>(v);
+  W.end_record();
+  for (int i = 0; i < ndom; ++i) {
+    W.put<int32_t>(nbv[i]);
+    W.put<double>(rdom[i]);
+  }
+  W.end_record();
+  for (int i = 0; i < nbt; ++i) {
+    W.put<int32_t>(ih[i]);
+    W.put<int32_t>(ik[i]);
+  }
+  W.end_record();
+  W.put<double>(be);
+  W.put<double>(azi);
+  W.put<double>(daz);
+  W.put<int32_t>(naz);
+  W.put<double>(gi);
+  W.put<double>(dg);
+  W.put<int32_t>(ng);
+  W.end_record();
+  W.put<double>(tem);
+  W.put<double>(dz);
+  W.put<int32_t>(ml);
+  W.put<double>(epsb);
+  W.end_record();
+  W.put<int32_t>(nsg);
+  W.put<int32_t>(mp);
+  for (double v : {aa, bb, gam, cc, dx, dy, zoffset}) W.put<double>(v);
+  W.end_record();
+  W.put<int32_t>(nelm);
+  W.put<int32_t>(natm);
+  W.end_record();
+  for (int i = 0; i < nelm; ++i) {
+    for (int j = 0; j < nabr + nabi; ++j) W.put<double>(E.A(j, i));
+    for (int j = 0; j < nabr + nabi; ++j) W.put<double>(E.B(j, i));
+    W.end_record();
+    for (double v : {E.dth[i], E.dtk[i], E.dtz[i], E.elm[i], E.dchg[i]}) W.put<double>(v);
+    W.end_record();
+  }
+  for (int i = 0; i < natm; ++i) {
+    W.put<int32_t>(ielm[i]);
+    for (double v : {ocr[i], x[i], y[i], z[i]}) W.put<double>(v);
+    W.end_record();
+  }
+  double wn = asfcrr(be, E, tem, aa * bb * std::sin(gam));
+  double ghx = (pi + pi) / (aa * nh);
+  double ghy = -(pi + pi) / (aa * std::tan(gam) * nh);
+  double gky = (pi + pi) / (bb * std::sin(gam) * nk);
+  ibt = 0;
+  for (int idom = 0; idom < ndom; ++idom) {
+    int nb = nbv[idom];
+    int* ihd = ih.data() + ibt;
+    int* ikd = ik.data() + ibt;
+    std::vector<int> iord, nbg;
+    int ngr = 0;
+    blkibg(nb, ihd, ikd, nh, nk, iord, ngr, nbg);
+    int nbgm = 0, nvm = 1, j = 0;
+    for (int i = 0; i < ngr; ++i) {
+      nbgm = std::max(nbgm, nbg[i]);
+      nvm = nvm + nbg[i] * (nbg[i] - 1) / 2;
+      j += nbg[i];
+    }
+    if (j != nb) throw std::runtime_error("grouping error");
+    std::vector<int> igh, igk, iv;
+    int nv = blkghk(ngr, nbg, nvm, igh, igk, nbgm, nb, ihd, ikd, iv);
+    std::vector<double> asf, Ghk;
+    asfcef(nv, igh, igk, ghx, ghy, gky, E, asf, Ghk);
+    for (int i = 0; i < nb; ++i) W.put<int32_t>(iord[i]);
+    W.end_record();
+    W.put<int32_t>(ngr);
+    W.put<int32_t>(nv);
+    W.end_record();
+    for (int i = 0; i < ngr; ++i) W.put<int32_t>(nbg[i]);
+    W.end_record();
+    for (int i = 0; i < nv; ++i) {
+      W.put<int32_t>(igh[i]);
+      W.put<int32_t>(igk[i]);
+    }
+    W.end_record();
+    std::vector<double> gh(nv), gk(nv);
+    for (int i = 0; i < nv; ++i) {
+      gh[i] = (-(pi + pi) / nh) * (double)igh[i];
+      gk[i] = (-(pi + pi) / nk) * (double)igk[i];
+    }
+    std::vector<cplx> s1, s2, s3;
+    scpot_stf(natm, nv, nsg, 1, 0, 0, 1, gh, gk, x.data(), y.data(), 0.0, 0.0, s1);
+    scpot_stf(natm, nv, nsg, 1, 0, 0, 1, gh, gk, x.data(), y.data(), -dx, -dy, s2);
+    scpot_stf(natm, nv, nsg, 1, 0, 0, 1, gh, gk, x.data(), y.data(), dx, dy, s3);
+    std::vector<cplx> v((size_t)nv * ns), vi((size_t)nv * ns);
+    for (int i = 1; i <= ns; ++i) {
+      double zi = dz * (i - 0.5);
+      cplx* vv = v.data() + (size_t)(i - 1) * nv;
+      cplx* vvi = vi.data() + (size_t)(i - 1) * nv;
+      scpot(nv, nv, vv, vvi, natm, ielm.data(), z.data(), zi, E, asf, 1.0, Ghk, ocr.data(),
+            s1.data());
+      scpot(nv, nv, vv, vvi, natm, ielm.data(), z.data(), zi + cc, E, asf, 1.0, Ghk, ocr.data(),
+            s2.data());
+      scpot(nv, nv, vv, vvi, natm, ielm.data(), z.data(), zi - cc, E, asf, 1.0, Ghk, ocr.data(),
+            s3.data());
+    }
+    // blkref angle loop (bulk.f90:24-126); the work of every (angle, group) is
+    // independent, so it is computed in parallel and written in file order.
+    double azr = azi + rdom[idom];
+    int nrep1 = (ng > naz) ? naz : ng, nrep2 = (ng > naz) ? ng : naz;
+    int total = nrep1 * nrep2;
+    std::vector<int> gofs(ngr + 1, 0);
+    for (int g = 0; g < ngr; ++g) gofs[g + 1] = gofs[g] + nbg[g];
+    std::vector<std::vector<cplx>> out((size_t)total * ngr);
+#pragma omp parallel for schedule(dynamic) collapse(2)
+    for (int t = 0; t < total; ++t)
+      for (int g = 0; g < ngr; ++g) {
+        int irep1 = t / nrep2, irep2 = t % nrep2;
+        double az, cga;
+        if (ng > naz) {
+          az = azr + irep1 * daz;
+          cga = std::cos(gi + irep2 * dg);
+        } else {
+          cga = std::cos(gi + irep1 * dg);
+          az = azr + irep2 * daz;
+        }
+        double wnx = wn * cga * std::cos(az), wny = wn * cga * std::sin(az);
+        int nbf = nbg[g], ibas = gofs[g];
+        auto& o = out[(size_t)t * ngr + g];
+        o.resize((size_t)nbf * nbf);
+        blkref_group(nbgm, nbf, ihd + ibas, ikd + ibas, iv.data() + (size_t)ibas * nbgm, ns,
+                     v.data(), vi.data(), nv, dz, epsb, nh, nk, ml, dx, dy, wn, ghx, ghy, gky, wnx,
+                     wny, o.data());
+      }
+    for (auto& o : out) {
+      for (const cplx& c : o) {
+        W.put<double>(c.real());
+        W.put<double>(c.imag());
+      }
+      W.end_record();
+    }
+    ibt += nb;
+  }
+}
+
+}  // namespace oracle
+
+// =============================================================================
+// C ABI for the test harness
+// =============================================================================
+using namespace oracle;
+
+struct OracleSurface {
+  SurfModel S;
+  int method = 5;
+  int ncol = 0;
+  std::vector<cplx> v, vi;
+};
+
+extern "C" {
+
+void oracle_set_threads(int n) {
+  if (n > 0) omp_set_num_threads(n);
+  scipy_openblas_set_num_threads(1);
+}
+
+// Load bulkP.b + surf.txt, build the stage potential table for `method`.
+// Returns an opaque handle or NULL; err (if given) receives a message.
+void* oracle_surface_open(const char* bulkp, const char* surf, double dz2, int method, char* err,
+                          int errlen) {
+  try {
+    auto* h = new OracleSurface();
+    h->method = method;
+    load_surface(bulkp, surf, dz2, h->S);
+    h->ncol = build_potential(h->S, h->S.dom[0], method, h->v, h->vi);
+    return h;
+  } catch (const std::exception& e) {
+    if (err && errlen > 0) std::snprintf(err, errlen, "%s", e.what());
+    return nullptr;
+  }
+}
+
+void oracle_surface_close(void* h) { delete static_cast<OracleSurface*>(h); }
+
+// Problem dimensions: out[0..9] = nb, nv, nvb, ns, ncol, nrep1, nrep2, ngr, naz, ng
+void oracle_surface_dims(void* hh, int* out) {
+  auto* h = static_cast<OracleSurface*>(hh);
+  auto& S = h->S;
+  auto& D = S.dom[0];
+  auto a = schedule(S);
+  out[0] = S.nbd[0];
+  out[1] = D.nv;
+  out[2] = D.nvb;
+  out[3] = S.ns;
+  out[4] = h->ncol;
+  out[5] = a.nrep1;
+  out[6] = a.nrep2;
+  out[7] = D.ngr;
+  out[8] = S.naz;
+  out[9] = S.ng;
+}
+
+// Scalars: out[0..7] = dz(surface), wn, ghx, ghy, gky, azi, daz, gi ; out[8] = dg
+void oracle_surface_scalars(void* hh, double* out) {
+  auto& S = static_cast<OracleSurface*>(hh)->S;
+  out[0] = S.dzs;
+  out[1] = S.wn;
+  out[2] = S.ghx;
+  out[3] = S.ghy;
+  out[4] = S.gky;
+  out[5] = S.azi;
+  out[6] = S.daz;
+  out[7] = S.gi;
+  out[8] = S.dg;
+}
+
+// Potential table (nv x ncol each, column-major complex128) and beam map iv (nb x nb, 1-based).
+void oracle_surface_tables(void* hh, double* v_out, double* vi_out, int* iv_out) {
+  auto* h = static_cast<OracleSurface*>(hh);
+  if (v_out) std::memcpy(v_out, h->v.data(), h->v.size() * sizeof(cplx));
+  if (vi_out) std::memcpy(vi_out, h->vi.data(), h->vi.size() * sizeof(cplx));
+  if (iv_out) {
+    auto& D = h->S.dom[0];
+    std::memcpy(iv_out, D.iv.data(), D.iv.size() * sizeof(int));
+  }
+}
+
+// Solve angles [first, first+count) of the flattened (irep1, irep2) schedule.
+// f2 receives nb doubles per angle; angle_out the printed angle (deg);
+// renorm_out per-angle renormalisation counts.  Returns 0 on success.
+int oracle_surface_solve(void* hh, int first, int count, double* f2, double* angle_out,
+                         int* renorm_out) {
+  auto* h = static_cast<OracleSurface*>(hh);
+  auto& S = h->S;
+  auto& D = S.dom[0];
+  auto a = schedule(S);
+  int nb = S.nbd[0];
+  int total = a.nrep1 * a.nrep2;
+  if (first < 0 || count < 0 || first + count > total) return -1;
+#pragma omp parallel for schedule(dynamic)
+  for (int t = first; t < first + count; ++t) {
+    int irep1 = t / a.nrep2, irep2 = t % a.nrep2;
+    double ga, az;
+    if (a.ng_outer) {
+      az = S.azi + irep1 * S.daz;
+      ga = S.gi + irep2 * S.dg;
+    } else {
+      ga = S.gi + irep1 * S.dg;
+      az = S.azi + irep2 * S.daz;
+    }
+    IntStats st;
+    solve_one(S, D, nb, S.ih.data(), S.ik.data(), h->method, h->v.data(), h->vi.data(), ga, az,
+              D.fbulk.data() + D.rec_off[t], f2 + (size_t)(t - first) * nb, st);
+    if (angle_out) {
+      double ang = a.ng_outer ? ga : az;
+      angle_out[t - first] = ang * 180.0 / 3.141592654;
+    }
+    if (renorm_out) renorm_out[t - first] = st.renorm;
+  }
+  return 0;
+}
+
+// bulk.exe equivalent: bulk.txt -> bulkP.b.  Returns 0 on success.
+int oracle_bulk_run(const char* bulk_txt, const char* out_path, char* err, int errlen) {
+  try {
+    scipy_openblas_set_num_threads(1);
+    bulk_run(bulk_txt, out_path);
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && errlen > 0) std::snprintf(err, errlen, "%s", e.what());
+    return -1;
+  }
+}
+
+// Full surf.exe equivalent for domain 1: writes the rocking-curve file.
+int oracle_surface_write(void* hh, const char* out_path) {
+  auto* h = static_cast<OracleSurface*>(hh);
+  auto& S = h->S;
+  auto a = schedule(S);
+  int nb = S.nbd[0];
+  int total = a.nrep1 * a.nrep2;
+  std::vector<double> f2((size_t)total * nb), ang(total);
+  int rc = oracle_surface_solve(hh, 0, total, f2.data(), ang.data(), nullptr);
+  if (rc) return rc;
+  FILE* o = std::fopen(out_path, "w");
+  if (!o) return -2;
+  write_header(o, S);
+  for (int r1 = 0; r1 < a.nrep1; ++r1) {
+    for (int r2 = 0; r2 < a.nrep2; ++r2) {
+      int t = r1 * a.nrep2 + r2;
+      write_row(o, ang[t], f2.data() + (size_t)t * nb, nb);
+    }
+    std::fprintf(o, "\n");
+  }
+  std::fclose(o);
+  return 0;
+}
+
+}  // extern "C"
