@@ -1,0 +1,159 @@
+/*
+ * trhepd_b200.h — C ABI of the B200 multislice surface solve.
+ *
+ * Drop-in boundary for the per-glancing-angle multislice path of
+ * sim-trhepd-rheed (Fortran).  Each entry point replaces one reference routine;
+ * the reference interface it stands in for is cited beside it.  Conventions
+ * follow the Fortran side: column-major arrays, 1-based beam/element indices,
+ * complex(8) passed as interleaved (re, im) doubles, int32 integers.  All host
+ * memory stays caller-owned; device memory belongs to the context.
+ *
+ * Every function returns TRHEPD_OK (0) or a nonzero status; the message of the
+ * last failure is available from trhepd_last_error().  A context is not
+ * thread-safe and issues its work on one CUDA stream.
+ */
+#ifndef TRHEPD_B200_H
+#define TRHEPD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum trhepd_status {
+  TRHEPD_OK = 0,
+  TRHEPD_EINVAL = 1,      /* bad argument (sizes, indices, method) */
+  TRHEPD_ECUDA = 2,       /* CUDA runtime error */
+  TRHEPD_ENONFINITE = 3,  /* NaN/Inf or an exactly zero pivot met on the device */
+  TRHEPD_ETIMEOUT = 4,    /* a bounded device wait gave up */
+  TRHEPD_ENOMEM = 5,      /* device allocation failed or over the memory budget */
+  TRHEPD_EIO = 6          /* input file missing or malformed */
+};
+
+/* precision forms of the surface solve */
+enum trhepd_precision {
+  TRHEPD_FP64 = 0,        /* all-FP64 (DMMA) */
+  TRHEPD_SPLIT_BF16 = 1   /* stage products from BF16 slices on tcgen05, FP64 elsewhere */
+};
+
+/* options (trhepd_set_option) */
+enum trhepd_option {
+  TRHEPD_OPT_RENORM_POLICY = 1, /* 0: Gershgorin test > 1e3 per angle and slice (reference)
+                                   1: growth bound, uniform schedule (see DESIGN) */
+  TRHEPD_OPT_RENORM_TAU = 2,    /* growth bound ln(cond) between renormalisations (policy 1) */
+  TRHEPD_OPT_SPLIT_SLICES = 3   /* BF16 slices per operand in the split form (3..5) */
+};
+
+typedef struct trhepd_context trhepd_context;
+
+int trhepd_create(int device, trhepd_context** ctx);
+void trhepd_destroy(trhepd_context* ctx);
+const char* trhepd_last_error(const trhepd_context* ctx);
+int trhepd_set_option(trhepd_context* ctx, int option, double value);
+/* counters of the last solve: out[0] renormalisations, out[1] stage products,
+   out[2] device milliseconds of the solve, out[3] stage columns */
+int trhepd_last_stats(const trhepd_context* ctx, double* out, int n);
+
+/*
+ * Structure state of the potential, mirroring module mod_scpot3
+ * (sim-trhepd-rheed/src/surfio.f90:18-27).  Bulk atoms come first in ielm/z/ocr.
+ */
+typedef struct trhepd_pot_state {
+  int nv, nvb, natms, natmb, nelm, nabr, nabi;
+  const int32_t* ielm;  /* natmb+natms, 1-based element index */
+  double cc, smesh;
+  const double* z;      /* natmb+natms (zoffset applied) */
+  const double* dchg;   /* nelm */
+  const double* Ghk;    /* nv */
+  const double* ocr;    /* natmb+natms */
+  const double* b;      /* (6, nelm) */
+  const double* asf;    /* (nv, 6, nelm) */
+  const double* st0;    /* complex (nv, natms) */
+  const double* st1;    /* complex (nvb, natmb) */
+  const double* st2;    /* complex (nvb, natmb) */
+} trhepd_pot_state;
+
+/*
+ * Structure factors of `natm` atoms for `nv` Fourier components on the GPU.
+ * Replaces scpot_stf / strfac (sim-trhepd-rheed/src/scpot.f90:100-110,
+ * strfac.f90:5-76).  img: per atom 12 (x, y) image pairs in 1x1-lattice units
+ * (from trhepd_plane_group_images), nimg: image counts.  st: complex (nv, natm).
+ */
+int trhepd_structure_factors(trhepd_context* ctx, int nv, const double* gh, const double* gk,
+                             int natm, const double* img, const int32_t* nimg, double dx,
+                             double dy, double* st);
+
+/* Plane-group orbit of one atom (strfac.f90:15-64, the 17 groups at :88-527). */
+int trhepd_plane_group_images(int nsg, int ma, int mb, int na, int nb, double x, double y,
+                              double* out_xy, int* count);
+
+/*
+ * Stage potential tables of an integrator: v, vi complex (nv, ncol) with
+ * ncol = s*ns+1 for int_method 5/6 (s = 6 / 11).  Replaces hp_int_init4/6
+ * (sim-trhepd-rheed/src/surf_prkn.f90:174-197) and comp_scpot (surfio.f90:29-41).
+ */
+int trhepd_potential_table(trhepd_context* ctx, const trhepd_pot_state* pot, int int_method,
+                           int ns, double dz, double* v, double* vi, int* ncol);
+
+/*
+ * Surface solve of every (azimuth, glancing angle) of one domain in one batch.
+ * Replaces srfref (sim-trhepd-rheed/src/surflf.f90:7-171) including its
+ * integrator call (hp_int4 / hp_int6, surf_prkn.f90:123-141) and the intensity
+ * formula (surflf.f90:142-151).  Arguments keep srfref's names and meaning;
+ * t1_records holds the bulk reflection records srfref reads from unit 1
+ * (surflf.f90:65-72): nrep1*nrep2 angles, each ngr blocks of nbg(l)^2 complex
+ * values in file order.  f2 receives (nb, nrep1*nrep2) intensities,
+ * angle_deg the printed angle of each row.
+ */
+int trhepd_srfref(trhepd_context* ctx, const trhepd_pot_state* pot, int nb, int ns,
+                  const int32_t* iv, double dz, int ngr, const int32_t* nbg, const int32_t* iord,
+                  const int32_t* ih, const int32_t* ik, double wn, double ghx, double ghy,
+                  double gky, double azi, double daz, int naz, double gi, double dg, int ng,
+                  int int_method, const double* t1_records, int precision, double* f2,
+                  double* angle_deg);
+
+/*
+ * C++ equivalent of surfio for the first domain (sim-trhepd-rheed/src/
+ * surfio.f90:60-381): parses bulkP.b + surf.txt, applies the slicing rule for
+ * dz2, forms the mod_scpot3 state (structure factors summed on the GPU) and the
+ * srfref arguments.  The handle owns every array the two views point into.
+ */
+typedef struct trhepd_surface_inputs trhepd_surface_inputs;
+
+typedef struct trhepd_srfref_args {
+  int nb, ns;
+  const int32_t* iv;      /* (nb, nb) */
+  double dz;
+  int ngr;
+  const int32_t *nbg, *iord, *ih, *ik;
+  double wn, ghx, ghy, gky, azi, daz;
+  int naz;
+  double gi, dg;
+  int ng, int_method;
+  const double* t1_records;
+  int nrep1, nrep2;       /* angle schedule sizes (surflf.f90:43-49) */
+} trhepd_srfref_args;
+
+int trhepd_surf_load(trhepd_context* ctx, const char* bulkp, const char* surf, double dz2,
+                     int int_method, trhepd_surface_inputs** out);
+void trhepd_surf_free(trhepd_surface_inputs* in);
+int trhepd_surf_views(const trhepd_surface_inputs* in, trhepd_pot_state* pot,
+                      trhepd_srfref_args* args);
+
+/*
+ * surf.exe for the first domain (surfm.f90:6-97 + surfio.f90:60-381): reads
+ * bulkP.b and surf.txt, slices the surface for dz2, solves on the GPU and, if
+ * out_path is not NULL, writes the rocking-curve file in the reference format.
+ * f2 (optional) receives (nb, nangles); dims (optional) receives
+ * {nb, nangles, ns, nv}.
+ */
+int trhepd_surf_run(trhepd_context* ctx, const char* bulkp, const char* surf, double dz2,
+                    int int_method, int precision, const char* out_path, double* f2,
+                    int max_f2, int* dims);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRHEPD_B200_H */

@@ -770,10 +770,122 @@ static const double kRkn611[23] = {
     0.0752539843015807,  -0.127049212625417, -0.0400061921041533, 0.290553797799558,
     0.198128671918067,   0.123229775946271,  0.0414649985182624};
 
+// Test knob: 0 = the reference's Gershgorin policy (default); k > 0 = renormalise
+// every k slices regardless of the estimate (used to study how the result depends
+// on where renormalisation happens).
+static int g_renorm_every = 0;
+
+// Test knob: emulate the split-precision stage product.  0 = off (default,
+// plain zgemm).  S > 0: the potential part of Q*M is formed from S fixed-point
+// slices of Q (per-row power-of-two scale) and of the shared potential matrix
+// (per-column scale), keeping slice pairs with s+t <= S+1; each pair's sums are
+// exact (integers far below 2^53); the diagonal energy term stays FP64.
+static int g_split_slices = 0;
+static int g_split_diag = 0;  // 1: whole diagonal of M kept exact (not only the energy term)
+
+static void split_slices(const cplx* X, int rows, int cols, int ldr, bool by_row, int S,
+                         std::vector<double>& scale, std::vector<std::vector<double>>& sl) {
+  // X column-major (ldr); slices of the real 2-vector view, integer valued
+  int nvec = by_row ? rows : cols;
+  scale.assign(nvec, 0.0);
+  for (int j = 0; j < cols; ++j)
+    for (int i = 0; i < rows; ++i) {
+      const cplx& x = X[(size_t)j * ldr + i];
+      double m = std::max(std::fabs(x.real()), std::fabs(x.imag()));
+      int v = by_row ? i : j;
+      scale[v] = std::max(scale[v], m);
+    }
+  for (auto& sc : scale) {
+    int e = 0;
+    if (sc > 0) std::frexp(sc, &e);  // sc < 2^e
+    sc = std::ldexp(1.0, e);
+  }
+  sl.assign(S, std::vector<double>((size_t)2 * rows * cols));
+  for (int j = 0; j < cols; ++j)
+    for (int i = 0; i < rows; ++i) {
+      const cplx& x = X[(size_t)j * ldr + i];
+      double sc = scale[by_row ? i : j];
+      for (int part = 0; part < 2; ++part) {
+        double r = (part ? x.imag() : x.real()) / sc * 128.0;  // |r| <= 128
+        for (int t = 0; t < S; ++t) {
+          double d = std::nearbyint(r);
+          sl[t][((size_t)j * rows + i) * 2 + part] = d;
+          r = (r - d) * 256.0;
+        }
+      }
+    }
+}
+
+// P += c * (Q*V) with Q (n x n) and V (n x n) in the split scheme.
+static void split_gemm_acc(int n, double c, const cplx* Q, const cplx* V, cplx* P, int S) {
+  std::vector<double> qs, vs;
+  std::vector<std::vector<double>> qsl, vsl;
+  split_slices(Q, n, n, n, true, S, qs, qsl);
+  split_slices(V, n, n, n, false, S, vs, vsl);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      double accr = 0, acci = 0;
+      for (int g = S - 1; g >= 0; --g) {  // groups s+t-2 = g, lowest weight first
+        double gr = 0, gi = 0;
+        for (int a = 0; a <= g; ++a) {
+          int b = g - a;
+          const auto& A = qsl[a];
+          const auto& B = vsl[b];
+          double sr = 0, si = 0;
+          for (int k = 0; k < n; ++k) {
+            double ar = A[((size_t)k * n + i) * 2], ai = A[((size_t)k * n + i) * 2 + 1];
+            double br = B[((size_t)j * n + k) * 2], bi = B[((size_t)j * n + k) * 2 + 1];
+            sr += ar * br - ai * bi;
+            si += ar * bi + ai * br;
+          }
+          gr += sr;
+          gi += si;
+        }
+        double w = std::ldexp(1.0, -14 - 8 * g);
+        accr += gr * w;
+        acci += gi * w;
+      }
+      double sc = qs[i] * vs[j];
+      P[(size_t)j * n + i] += c * cplx(accr * sc, acci * sc);
+    }
+}
+
 struct IntStats {
   int renorm = 0;   // cond_est-triggered renormalisations (excludes the final one)
   int gemms = 0;    // N^3 complex products issued
 };
+
+// P = beta*P + c*Q*M (zgemm, or the emulated split product when enabled)
+static void stage_product(int nb, double c, const cplx* Q, const CMat& m, const cplx* g, cplx* P,
+                          double beta) {
+  if (g_split_slices <= 0) {
+    zgemm('N', 'N', nb, nb, nb, cplx(1, 0) * c, Q, nb, m.a.data(), nb, beta, P, nb);
+    return;
+  }
+  // M = Vs + diag(-conj(g^2)): potential part through the split product, diagonal exact
+  CMat Vs = m;
+  std::vector<cplx> d(nb);
+  for (int j = 0; j < nb; ++j) {
+    d[j] = (g_split_diag ? m(j, j) : -std::conj(g[j] * g[j]));
+    Vs(j, j) = Vs(j, j) - d[j];
+  }
+  if (beta == 0.0) std::fill(P, P + (size_t)nb * nb, cplx(0, 0));
+  if (g_split_diag >= 2) {
+    // Q = Qoff + diag(q): Qoff*Vs through the split product, diag(q)*Vs exact
+    std::vector<cplx> Qo(Q, Q + (size_t)nb * nb), q(nb);
+    for (int i = 0; i < nb; ++i) {
+      q[i] = Qo[(size_t)i * nb + i];
+      Qo[(size_t)i * nb + i] = 0.0;
+    }
+    split_gemm_acc(nb, c, Qo.data(), Vs.a.data(), P, g_split_slices);
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) P[(size_t)j * nb + i] += c * (q[i] * Vs(i, j));
+  } else {
+    split_gemm_acc(nb, c, Q, Vs.a.data(), P, g_split_slices);
+  }
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) P[(size_t)j * nb + i] += c * (Q[(size_t)j * nb + i] * d[j]);
+}
 
 // hp_int_spa: symplectic RKN in [X^H, Y^H] form (surf_prkn.f90:278-330)
 static void hp_int_spa(double dz, int ns, int nb, int nv, CMat& f, const cplx* g, const int* iv,
@@ -796,7 +908,7 @@ static void hp_int_spa(double dz, int ns, int nb, int nv, CMat& f, const cplx* g
         if (x_is_id) {
           for (size_t e = 0; e < nn; ++e) P[e] = P[e] + (cb * dz) * m.a[e];
         } else {
-          zgemm('N', 'N', nb, nb, nb, cplx(1, 0) * (cb * dz), Q, nb, m.data(), nb, 1.0, P, nb);
+          stage_product(nb, cb * dz, Q, m, g, P, 1.0);
           st.gemms++;
         }
       }
@@ -811,12 +923,12 @@ static void hp_int_spa(double dz, int ns, int nb, int nv, CMat& f, const cplx* g
     }
     vvi2mate(nb, nv, col(s * l, v), col(s * l, vi), iv, g, m);
     // hp_pinth_save
-    zgemm('N', 'N', nb, nb, nb, cplx(1, 0) * (bab[0] * dz), Q, nb, m.data(), nb, 0.0,
-          psave.data(), nb);
+    stage_product(nb, bab[0] * dz, Q, m, g, psave.data(), 0.0);
     st.gemms++;
     for (size_t e = 0; e < nn; ++e) P[e] = P[e] + psave.a[e];
     double d = cond_est(nb, Q);
-    if (d > 1e3 || l == ns) {
+    bool renorm = g_renorm_every > 0 ? (l % g_renorm_every == 0) : (d > 1e3);
+    if (renorm || l == ns) {
       if (l != ns) st.renorm++;
       matAbdivB(nb, t1.data(), nb, piv);
       x_is_id = true;
@@ -1959,6 +2071,26 @@ struct OracleSurface {
 };
 
 extern "C" {
+
+void oracle_set_renorm_every(int k) { g_renorm_every = k; }
+
+// Plane-group images in 1x1-lattice units (strfac.f90:15-64); returns the count.
+int oracle_plane_group_images(int nsg, int ma, int mb, int na, int nb, double x, double y,
+                              double* out_xy) {
+  double xs[12], ys[12];
+  double s = (double)(ma * nb - mb * na);
+  xs[0] = reduce01((nb * x - na * y) / s);
+  ys[0] = reduce01((ma * y - mb * x) / s);
+  int ndeg = plane_group_images(nsg, xs, ys);
+  for (int i = 0; i < ndeg; ++i) {
+    double u = reduce01(xs[i]), v = reduce01(ys[i]);
+    out_xy[2 * i] = ma * u + na * v;
+    out_xy[2 * i + 1] = mb * u + nb * v;
+  }
+  return ndeg;
+}
+void oracle_set_split_slices(int s) { g_split_slices = s; }
+void oracle_set_split_diag(int d) { g_split_diag = d; }
 
 void oracle_set_threads(int n) {
   if (n > 0) omp_set_num_threads(n);

@@ -1,0 +1,53 @@
+"""Extract the reference's own regression data into small fixtures.
+
+Reads the reference checkout (path given as argv[1], default /root/reference)
+and writes, per test case (test23 / test47 / test521):
+
+* ``<case>/bulkP.b``, ``<case>/surf.txt``, ``<case>/bulk.txt`` — the inputs the
+  reference's regression runs used (test/<case>/);
+* ``<case>/perf-<method>-<dz>.npz`` — angles and intensities of the committed
+  outputs test/<case>/test-results/perf-<method>-<dz>.txt (E23.15, 15 digits),
+  for the integrators and slice thicknesses listed below.
+
+Run once in a container that has the reference; the fixtures travel with the
+repository and nothing at test time reads the reference.
+"""
+from __future__ import annotations
+
+import shutil
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+SEL = {
+    "test23": [(m, dz) for m in (4, 5, 6, 7) for dz in ("0.68", "0.1", "0.022")],
+    "test47": [(m, dz) for m in (5, 6) for dz in ("0.68", "0.22")] + [(7, "0.22")],
+    "test521": [(5, "0.68"), (6, "0.68"), (5, "0.33"), (6, "0.33")],
+}
+
+
+def parse_s(path):
+    sys.path.insert(0, str(HERE.parents[1] / "trhepd-opt_b200"))
+    from formats import read_rocking_curves
+    return read_rocking_curves(path)
+
+
+def main(ref: Path):
+    for case, sel in SEL.items():
+        src = ref / "test" / case
+        dst = HERE / case
+        dst.mkdir(parents=True, exist_ok=True)
+        for f in ("bulkP.b", "surf.txt", "bulk.txt"):
+            shutil.copyfile(src / f, dst / f)
+        for m, dz in sel:
+            p = src / "test-results" / f"perf-{m}-{dz}.txt"
+            ang, f2, hdr = parse_s(p)
+            np.savez_compressed(dst / f"perf-{m}-{dz}.npz", angle=ang, f2=f2,
+                                beams=hdr["beams"], naz=hdr["naz"], ng=hdr["ng"])
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))

@@ -1,0 +1,738 @@
+// FP64 kernels of the multislice surface solve (sm_100a).
+//
+//   K2 structure factors        strfac      sim-trhepd-rheed/src/strfac.f90:65-75
+//   K3 stage potential table    scpot x3    scpot.f90:115-193, surfio.f90:29-41
+//   K4 stage-matrix gather      vvi2mate    matcomp.f90:253-279
+//   K5 stage GEMM + RKN update  hp_pinth/hp_qinth  surf_prkn.f90:222-276
+//   K7 Gershgorin estimate      cond_est    matcomp.f90:498-528
+//   K8 renormalisation Q^-1 P   matAbdivB   matcomp.f90:53-69
+//   boundary transforms         invstransh/stransh  matcomp.f90:140-196
+//   intensities                 surflf.f90:142-151
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "kernels.h"
+
+namespace trhepd {
+
+// ============================================================ K2 structure factors
+// One thread per (k, atom); the <= 12 plane-group images are summed in registers.
+__global__ void k_structure_factor(const double* __restrict__ gh, const double* __restrict__ gk,
+                                   int nv, const double* __restrict__ img,
+                                   const int* __restrict__ nimg, int natm, double dx, double dy,
+                                   cd* __restrict__ st) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (k >= nv || j >= natm) return;
+  double sr = 0.0, si = 0.0;
+  int n = nimg[j];
+  for (int m = 0; m < n; ++m) {
+    double xb = img[(j * 12 + m) * 2], yb = img[(j * 12 + m) * 2 + 1];
+    double gr = gh[k] * (dx + xb) + gk[k] * (dy + yb);
+    double s, c;
+    sincos(gr, &s, &c);
+    sr += c;
+    si += s;
+  }
+  st[(size_t)j * nv + k] = cd{sr, si};
+}
+
+void launch_structure_factor(const double* gh, const double* gk, int nv, const double* img,
+                             const int* nimg, int natm, double dx, double dy, cd* st,
+                             cudaStream_t stream) {
+  if (natm <= 0 || nv <= 0) return;
+  dim3 grid(ceil_div(nv, 128), natm);
+  k_structure_factor<<<grid, 128, 0, stream>>>(gh, gk, nv, img, nimg, natm, dx, dy, st);
+}
+
+// ============================================================ K3 potential table
+// Block per stage depth; the depth-dependent Gaussian factors exp(b (z - z_j)^2) of
+// every (atom, Gaussian) are formed once in shared memory, then each thread sums
+// the atoms for its Fourier components (coalesced over k).
+constexpr int kMaxPotAtoms = 512;
+constexpr int kMaxGauss = 6;
+
+__global__ void k_potential_table(PotInputs in, const double* __restrict__ depth,
+                                  TableEntry* __restrict__ table) {
+  const int c = blockIdx.x;
+  const double zc = depth[c];
+  const double uf = -70.0;
+  __shared__ double sE[kMaxPotAtoms * kMaxGauss];
+  __shared__ double sZ1[kMaxPotAtoms];  // z1 = zi - z_j (needed by the ion term)
+  __shared__ int sElem[kMaxPotAtoms];
+  const int nabr = in.nabr, mab = in.mab, nv = in.nv;
+  // flatten atoms of the three parts
+  int base[4];
+  base[0] = 0;
+  for (int p = 0; p < 3; ++p) base[p + 1] = base[p] + in.part[p].natm;
+  const int ntot = base[3];
+  for (int t = threadIdx.x; t < ntot; t += blockDim.x) {
+    int p = (t >= base[1]) + (t >= base[2]);
+    int j = t - base[p];
+    const PotPart& P = in.part[p];
+    double zi = zc + P.zshift;
+    double ocrmesh = P.rmesh * P.ocr[j];
+    int ie = P.ielm[j];
+    double z1 = zi - P.z[j];
+    double z2 = z1 * z1;
+    sZ1[t] = z1;
+    sElem[t] = ie;
+    for (int i = 0; i < nabr; ++i) {
+      double ex = in.b[ie * mab + i] * z2;
+      sE[t * kMaxGauss + i] = (ex > uf) ? exp(ex) * ocrmesh : 0.0;
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) {
+    double vr = 0.0, vim = 0.0, wr = 0.0, wim = 0.0;  // v and vi accumulated separately
+    double vir = 0.0, vii = 0.0;
+    for (int p = 0; p < 3; ++p) {
+      const PotPart& P = in.part[p];
+      if (k >= P.nk) continue;
+      for (int j = 0; j < P.natm; ++j) {
+        int t = base[p] + j;
+        int ie = sElem[t];
+        double ocrmesh = P.rmesh * P.ocr[j];
+        double tv = 0.0;
+        if (fabs(in.dchg[ie]) > 1e-4) {  // ionic term (scpot.f90:139-150)
+          double z1 = -fabs(sZ1[t]);
+          if (k == 0) {
+            tv = ocrmesh * z1 * in.dchg[ie];
+          } else {
+            double ex = in.ghk[k] * z1;
+            tv = (ex > uf) ? exp(ex) * ocrmesh / in.ghk[k] * in.dchg[ie] : 0.0;
+          }
+        }
+        double tvi = 0.0;
+        const double* asf_e = in.asf + (size_t)ie * mab * nv;
+        if (in.nabi == 1) {
+          double sap = asf_e[(size_t)nabr * nv + 0];
+          for (int i = 0; i < nabr; ++i) {
+            double e = sE[t * kMaxGauss + i];
+            if (e != 0.0 || true) {
+              double aex = asf_e[(size_t)i * nv + k] * e;
+              tv = tv + aex;
+              tvi = tvi + fabs(sap * aex);
+            }
+          }
+        } else {
+          for (int i = 0; i < nabr; ++i) tv = tv + asf_e[(size_t)i * nv + k] * sE[t * kMaxGauss + i];
+        }
+        cd ct = P.st[(size_t)j * P.nk + k];
+        vr = vr + tv * ct.x;
+        vim = vim + tv * ct.y;
+        // vi += (0, tvi) * ct
+        vir = vir + (0.0 * ct.x - tvi * ct.y);
+        vii = vii + (0.0 * ct.y + tvi * ct.x);
+      }
+    }
+    (void)wr;
+    (void)wim;
+    TableEntry e;
+    e.u = cd{vr + vir, vim + vii};
+    e.w = cd{vr - vir, vim - vii};
+    table[(size_t)c * nv + k] = e;
+  }
+}
+
+void launch_potential_table(const PotInputs& in, const double* depth, int ncol, TableEntry* table,
+                            cudaStream_t st) {
+  if (ncol <= 0) return;
+  k_potential_table<<<ncol, 256, 0, st>>>(in, depth, table);
+}
+
+// ============================================================ K4 gather
+__global__ void k_gather_stage(const TableEntry* __restrict__ tc, const int* __restrict__ pair,
+                               int n, int kpad, int ld, int drop_diag, cd* __restrict__ V) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = blockIdx.y;
+  if (j >= ld || k >= kpad) return;
+  cd v = cd{0.0, 0.0};
+  if (k < n && j < n) {
+    if (k < j) {
+      v = -conj(tc[pair[k * n + j]].u);
+    } else if (k > j) {
+      v = -tc[pair[k * n + j]].w;
+    } else if (!drop_diag) {
+      v = -conj(tc[0].u);
+    }
+  }
+  V[(size_t)k * ld + j] = v;
+}
+
+void launch_gather_stage(const TableEntry* table_col, const int* pair, int n, int kpad, int ld,
+                         bool drop_diag, cd* V, cudaStream_t st) {
+  dim3 grid(ceil_div(ld, 128), kpad);
+  k_gather_stage<<<grid, 128, 0, st>>>(table_col, pair, n, kpad, ld, drop_diag ? 1 : 0, V);
+}
+
+// ============================================================ identity-stage elementwise
+__global__ void k_stage_identity(cd* __restrict__ Q, cd* __restrict__ P, const cd* __restrict__ V,
+                                 const cd* __restrict__ D, int nang, int n, int ld, double cb,
+                                 double ca) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;  // stacked row
+  if (j >= n) return;
+  int a = r / n, i = r - a * n;
+  size_t o = (size_t)r * ld + j;
+  cd m = V[(size_t)i * ld + j];
+  if (i == j) m = m + D[(size_t)a * ld + j];
+  cd p = P[o] + cb * m;
+  P[o] = p;
+  cd q = ca * p;
+  if (i == j) q.x += 1.0;
+  Q[o] = q;
+}
+
+void launch_stage_identity(cd* Q, cd* P, const cd* V, const cd* D, int nang, int n, int ld,
+                           double cb, double ca, cudaStream_t st) {
+  dim3 grid(ceil_div(n, 128), nang * n);
+  k_stage_identity<<<grid, 128, 0, st>>>(Q, P, V, D, nang, n, ld, cb, ca);
+}
+
+// ============================================================ K5 FP64 DMMA stage GEMM
+// CTA tile 64 x 64 complex, k-step 16, 4 warps (2 x 2), warp tile 32 x 32 built
+// from m16n8k4 FP64 MMAs (4 real MMAs per complex product).  3-stage cp.async
+// pipeline; shared-memory rows padded so fragment loads are conflict-free.
+namespace f64gemm {
+constexpr int BM = 64, BN = 64, BK = 16, STAGES = 3;
+constexpr int ASTR = BK + 4;   // complex elements per A row in smem (stride = 4 mod 8 x 16B)
+constexpr int BSTR = BN + 2;   // complex elements per B row in smem (stride = 2 mod 8 x 16B)
+constexpr int A_TILE = BM * ASTR, B_TILE = BK * BSTR;
+constexpr size_t SMEM = (size_t)STAGES * (A_TILE + B_TILE) * sizeof(cd);
+}  // namespace f64gemm
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double& c2, double& c3, double a0,
+                                     double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(c0), "+d"(c1), "+d"(c2), "+d"(c3)
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+__global__ void __launch_bounds__(128, 2)
+    k_stage_gemm_f64(const cd* __restrict__ Q, cd* __restrict__ P, cd* __restrict__ Qo,
+                     const cd* __restrict__ V, const cd* __restrict__ D, int rows, int n, int ld,
+                     int kpad, double cb, double ca) {
+  using namespace f64gemm;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cd* As = reinterpret_cast<cd*>(smem_raw);
+  cd* Bs = As + STAGES * A_TILE;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int bm = blockIdx.y * BM, bn = blockIdx.x * BN;
+
+  auto load_stage = [&](int s, int k0) {
+    cd* a = As + s * A_TILE;
+    cd* b = Bs + s * B_TILE;
+#pragma unroll
+    for (int it = 0; it < (BM * BK) / 128; ++it) {
+      int e = tid + it * 128;
+      int r = e / BK, kk = e % BK;
+      int gr = bm + r, gk = k0 + kk;
+      bool ok = gr < rows && gk < kpad;
+      const cd* src = ok ? Q + (size_t)gr * ld + gk : Q;
+      cp_async16(a + r * ASTR + kk, src, ok);
+    }
+#pragma unroll
+    for (int it = 0; it < (BK * BN) / 128; ++it) {
+      int e = tid + it * 128;
+      int kk = e / BN, c = e % BN;
+      int gk = k0 + kk, gc = bn + c;
+      bool ok = gk < kpad && gc < ld;
+      const cd* src = ok ? V + (size_t)gk * ld + gc : V;
+      cp_async16(b + kk * BSTR + c, src, ok);
+    }
+  };
+
+  double cr[2][4][4], ci[2][4][4];
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) cr[mi][ni][e] = ci[mi][ni][e] = 0.0;
+
+  const int nk = kpad / BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) load_stage(s, s * BK);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    int nxt = kt + STAGES - 1;
+    if (nxt < nk) load_stage(nxt % STAGES, nxt * BK);
+    cp_async_commit();
+    const cd* a = As + (kt % STAGES) * A_TILE;
+    const cd* b = Bs + (kt % STAGES) * B_TILE;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      cd af[2][2], bf[4];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi) {
+        af[mi][0] = a[(wm + mi * 16 + g) * ASTR + kk + t];
+        af[mi][1] = a[(wm + mi * 16 + g + 8) * ASTR + kk + t];
+      }
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) bf[ni] = b[(kk + t) * BSTR + wn + ni * 8 + g];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+          double* R = cr[mi][ni];
+          double* I = ci[mi][ni];
+          dmma(R[0], R[1], R[2], R[3], af[mi][0].x, af[mi][1].x, bf[ni].x);
+          dmma(R[0], R[1], R[2], R[3], -af[mi][0].y, -af[mi][1].y, bf[ni].y);
+          dmma(I[0], I[1], I[2], I[3], af[mi][0].x, af[mi][1].x, bf[ni].y);
+          dmma(I[0], I[1], I[2], I[3], af[mi][0].y, af[mi][1].y, bf[ni].x);
+        }
+    }
+  }
+  cp_async_wait<0>();
+
+  // fused epilogue: P += cb*(acc + Q o D_a); Qo = Q + ca*P
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        int r = bm + wm + mi * 16 + g + ((e >= 2) ? 8 : 0);
+        int c = bn + wn + ni * 8 + 2 * t + (e & 1);
+        if (r < rows && c < n) {
+          int ang = r / n;
+          size_t o = (size_t)r * ld + c;
+          cd q = Q[o];
+          cd d = D[(size_t)ang * ld + c];
+          cd acc = cd{cr[mi][ni][e], ci[mi][ni][e]} + q * d;
+          cd p = P[o] + cb * acc;
+          P[o] = p;
+          Qo[o] = q + ca * p;
+        }
+      }
+}
+
+void launch_stage_gemm_f64(const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D, int nang, int n,
+                           int ld, int kpad, double cb, double ca, cudaStream_t st) {
+  using namespace f64gemm;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_stage_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    attr = true;
+  }
+  int rows = nang * n;
+  dim3 grid(ceil_div(n, BN), ceil_div(rows, BM));
+  k_stage_gemm_f64<<<grid, 128, SMEM, st>>>(Q, P, Qo, V, D, rows, n, ld, kpad, cb, ca);
+}
+
+// ============================================================ identity / flags
+__global__ void k_set_identity(cd* __restrict__ Q, const int* __restrict__ flag, int n, int ld) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  int a = r / n, i = r - a * n;
+  if (j >= n) return;
+  if (flag && !flag[a]) return;
+  Q[(size_t)r * ld + j] = cd{i == j ? 1.0 : 0.0, 0.0};
+}
+
+void launch_set_identity(cd* Q, const int* flag, int nang, int n, int ld, cudaStream_t st) {
+  dim3 grid(ceil_div(n, 128), nang * n);
+  k_set_identity<<<grid, 128, 0, st>>>(Q, flag, n, ld);
+}
+
+// ============================================================ K7 Gershgorin estimate
+__global__ void k_cond_est(const cd* __restrict__ Q, int n, int ld, int force,
+                           int* __restrict__ flag, double* __restrict__ dval) {
+  const int a = blockIdx.x;
+  const cd* A = Q + (size_t)a * n * ld;
+  double mn = INFINITY, mx = 0.0;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    double tsum = 0.0;
+    for (int i = 0; i < n; ++i) {
+      if (i != j) {
+        cd v = A[(size_t)i * ld + j];
+        tsum = tsum + sqrt(v.x * v.x + v.y * v.y);
+      }
+    }
+    cd dj = A[(size_t)j * ld + j];
+    double ad = hypot(dj.x, dj.y);
+    mn = fmin(mn, ad - tsum);
+    mx = fmax(mx, ad + tsum);
+  }
+  __shared__ double smn[32], smx[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    smn[w] = mn;
+    smx[w] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int nw = (blockDim.x + 31) >> 5;
+    for (int i = 1; i < nw; ++i) {
+      mn = fmin(mn, smn[i]);
+      mx = fmax(mx, smx[i]);
+    }
+    cd a11 = A[0];
+    mx = fmax(mx, hypot(a11.x, a11.y));
+    double d = (mn < 0.0) ? 1e100 : mx / mn;
+    if (dval) dval[a] = d;
+    flag[a] = (force || d > 1e3) ? 1 : 0;
+  }
+}
+
+void launch_cond_est(const cd* Q, int nang, int n, int ld, int force, int* flag, double* dval,
+                     cudaStream_t st) {
+  k_cond_est<<<nang, 256, 0, st>>>(Q, n, ld, force, flag, dval);
+}
+
+// ============================================================ K8 blocked Gauss-Jordan
+// [Q | P] -> [I | Q^{-1} P] with partial pivoting (pivot = max |re|+|im| among the
+// rows not yet used, lowest index on ties, as zgetrf's izamax).  Panels of kW
+// columns: the panel kernel factors rows c0.. of the panel (LU with row swaps) and
+// forms W1 = B1^{-1} and the elimination multipliers L2 = B2 B1^{-1} for every
+// other row; the update kernel applies the swaps and
+//   C1 <- W1 C1,   C2 <- C2 - L2 C1
+// to all remaining columns (Q columns right of the panel and every P column).
+constexpr int kW = 16;
+constexpr int kUpdCols = 64;
+
+struct GJScratch {
+  int* piv;   // nang x kW
+  cd* W1;     // nang x kW x kW
+  cd* L2;     // nang x n x kW
+};
+
+size_t gj_scratch_bytes(int nang, int n) {
+  size_t b = (size_t)nang * kW * sizeof(int);
+  b = (b + 255) & ~size_t(255);
+  b += (size_t)nang * kW * kW * sizeof(cd);
+  b = (b + 255) & ~size_t(255);
+  b += (size_t)nang * n * kW * sizeof(cd);
+  return b + 256;
+}
+
+static GJScratch gj_carve(void* scratch, int nang, int n) {
+  GJScratch s;
+  char* p = reinterpret_cast<char*>(scratch);
+  s.piv = reinterpret_cast<int*>(p);
+  size_t b = (size_t)nang * kW * sizeof(int);
+  b = (b + 255) & ~size_t(255);
+  s.W1 = reinterpret_cast<cd*>(p + b);
+  b += (size_t)nang * kW * kW * sizeof(cd);
+  b = (b + 255) & ~size_t(255);
+  s.L2 = reinterpret_cast<cd*>(p + b);
+  return s;
+}
+
+// Column-major complex access helper for the panel held in shared memory: S[i*kW + k].
+__global__ void k_gj_panel(const cd* __restrict__ Q, const int* __restrict__ flag, int n, int ld,
+                           int c0, int w, GJScratch sc, unsigned* status) {
+  const int a = blockIdx.x;
+  if (flag && !flag[a]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cd* S = reinterpret_cast<cd*>(smem_raw);  // n x kW
+  __shared__ double rv[32];
+  __shared__ int ri[32];
+  __shared__ int s_piv;
+  __shared__ cd Linv[kW * kW], Uinv[kW * kW], W1s[kW * kW];
+  const cd* A = Q + (size_t)a * n * ld;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < n * kW; e += nt) {
+    int i = e / kW, k = e % kW;
+    S[e] = (k < w) ? A[(size_t)i * ld + c0 + k] : cd{0.0, 0.0};
+  }
+  __syncthreads();
+  // ---- LU with partial pivoting of rows c0..n-1 of the panel
+  for (int jj = 0; jj < w; ++jj) {
+    const int col = c0 + jj;
+    double best = -1.0;
+    int bi = n;
+    for (int i = col + tid; i < n; i += nt) {
+      double v = cabs1(S[i * kW + jj]);
+      if (v > best) {  // strict: keeps the lowest index within this thread's strided scan
+        best = v;
+        bi = i;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ov = __shfl_xor_sync(0xffffffffu, best, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    if ((tid & 31) == 0) {
+      rv[tid >> 5] = best;
+      ri[tid >> 5] = bi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int nw = (nt + 31) >> 5;
+      for (int q = 1; q < nw; ++q)
+        if (rv[q] > best || (rv[q] == best && ri[q] < bi)) {
+          best = rv[q];
+          bi = ri[q];
+        }
+      if (bi >= n) bi = col;
+      s_piv = bi;
+      sc.piv[a * kW + jj] = bi;
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p != col) {
+      for (int k = tid; k < kW; k += nt) {
+        cd tmp = S[col * kW + k];
+        S[col * kW + k] = S[p * kW + k];
+        S[p * kW + k] = tmp;
+      }
+    }
+    __syncthreads();
+    const cd d = S[col * kW + jj];
+    if (d.x == 0.0 && d.y == 0.0) {
+      if (tid == 0) atomicOr(status, kStatusZeroPivot);
+    }
+    const cd rinv = cdiv(cd{1.0, 0.0}, d);
+    for (int i = col + 1 + tid; i < n; i += nt) {
+      cd l = S[i * kW + jj] * rinv;
+      S[i * kW + jj] = l;
+      for (int k = jj + 1; k < w; ++k) S[i * kW + k] = S[i * kW + k] - l * S[col * kW + k];
+    }
+    __syncthreads();
+  }
+  // ---- inverses of the unit-lower L11 and upper U11 (w x w), W1 = U11^{-1} L11^{-1}
+  if (tid < kW) {
+    const int k = tid;  // column k of each inverse
+    for (int i = 0; i < kW; ++i) {  // forward substitution L11 x = e_k
+      cd s = cd{(i == k) ? 1.0 : 0.0, 0.0};
+      if (i < w)
+        for (int m = 0; m < i; ++m) s = s - S[(c0 + i) * kW + m] * Linv[m * kW + k];
+      Linv[i * kW + k] = (i < w && k < w) ? s : cd{0.0, 0.0};
+    }
+    for (int i = kW - 1; i >= 0; --i) {  // back substitution U11 x = e_k
+      cd s = cd{(i == k) ? 1.0 : 0.0, 0.0};
+      if (i < w && k < w) {
+        for (int m = i + 1; m < w; ++m) s = s - S[(c0 + i) * kW + m] * Uinv[m * kW + k];
+        s = cdiv(s, S[(c0 + i) * kW + i]);
+      } else {
+        s = cd{0.0, 0.0};
+      }
+      Uinv[i * kW + k] = s;
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < kW * kW; e += nt) {
+    int i = e / kW, k = e % kW;
+    cd s = cd{0.0, 0.0};
+    for (int m = 0; m < kW; ++m) s = s + Uinv[i * kW + m] * Linv[m * kW + k];
+    W1s[e] = s;
+    sc.W1[(size_t)a * kW * kW + e] = s;
+  }
+  __syncthreads();
+  // ---- multipliers: rows >= c0+w: L21 L11^{-1};  rows < c0: B0 W1
+  cd* L2 = sc.L2 + (size_t)a * n * kW;
+  for (int e = tid; e < n * kW; e += nt) {
+    int i = e / kW, k = e % kW;
+    cd s = cd{0.0, 0.0};
+    if (k < w) {
+      if (i >= c0 + w) {
+        for (int m = 0; m < w; ++m) s = s + S[i * kW + m] * Linv[m * kW + k];
+      } else if (i < c0) {
+        for (int m = 0; m < w; ++m) s = s + S[i * kW + m] * W1s[m * kW + k];
+      }
+    }
+    L2[e] = s;
+  }
+}
+
+// Each CTA owns kUpdCols of the remaining columns of one angle.
+__global__ void k_gj_update(cd* __restrict__ Q, cd* __restrict__ P, const int* __restrict__ flag,
+                            int n, int ld, int c0, int w, GJScratch sc) {
+  const int a = blockIdx.y;
+  if (flag && !flag[a]) return;
+  const int qrest = n - (c0 + w);          // Q columns right of the panel
+  const int vc = blockIdx.x * kUpdCols + threadIdx.x % kUpdCols;  // virtual column
+  const int total = qrest + n;
+  __shared__ cd C1[kW][kUpdCols];
+  __shared__ cd W1[kW * kW];
+  __shared__ int piv[kW];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < kW * kW; e += nt) W1[e] = sc.W1[(size_t)a * kW * kW + e];
+  if (tid < kW) piv[tid] = sc.piv[a * kW + tid];
+  __syncthreads();
+  const bool valid = vc < total;
+  cd* base = nullptr;
+  if (valid) base = (vc < qrest) ? Q + (size_t)a * n * ld + (c0 + w + vc)
+                                 : P + (size_t)a * n * ld + (vc - qrest);
+  const int lane_col = tid % kUpdCols, rgrp = tid / kUpdCols, nrg = nt / kUpdCols;
+  // row swaps (one thread per column does all of them, in order)
+  if (valid && rgrp == 0) {
+    for (int jj = 0; jj < w; ++jj) {
+      int r0 = c0 + jj, r1 = piv[jj];
+      if (r1 != r0) {
+        cd t0 = base[(size_t)r0 * ld], t1 = base[(size_t)r1 * ld];
+        base[(size_t)r0 * ld] = t1;
+        base[(size_t)r1 * ld] = t0;
+      }
+    }
+  }
+  __syncthreads();
+  // C1 = pivot rows (original values)
+  for (int k = rgrp; k < kW; k += nrg)
+    C1[k][lane_col] = (valid && k < w) ? base[(size_t)(c0 + k) * ld] : cd{0.0, 0.0};
+  __syncthreads();
+  // pivot rows <- W1 C1
+  for (int k = rgrp; k < w; k += nrg) {
+    if (!valid) continue;
+    cd s = cd{0.0, 0.0};
+    for (int m = 0; m < w; ++m) s = s + W1[k * kW + m] * C1[m][lane_col];
+    base[(size_t)(c0 + k) * ld] = s;
+  }
+  // other rows <- C2 - L2 C1
+  const cd* L2 = sc.L2 + (size_t)a * n * kW;
+  for (int i = rgrp; i < n; i += nrg) {
+    if (i >= c0 && i < c0 + w) continue;
+    if (!valid) continue;
+    cd s = base[(size_t)i * ld];
+    const cd* l = L2 + (size_t)i * kW;
+#pragma unroll 4
+    for (int m = 0; m < w; ++m) s = s - l[m] * C1[m][lane_col];
+    base[(size_t)i * ld] = s;
+  }
+}
+
+void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld, void* scratch,
+                         unsigned* status, cudaStream_t st) {
+  GJScratch sc = gj_carve(scratch, nang, n);
+  size_t smem = (size_t)n * kW * sizeof(cd);
+  static size_t attr = 0;
+  if (smem > attr) {
+    cudaFuncSetAttribute(k_gj_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = smem;
+  }
+  for (int c0 = 0; c0 < n; c0 += kW) {
+    int w = (n - c0 < kW) ? n - c0 : kW;
+    k_gj_panel<<<nang, 256, smem, st>>>(Q, flag, n, ld, c0, w, sc, status);
+    int total = (n - (c0 + w)) + n;
+    dim3 grid(ceil_div(total, kUpdCols), nang);
+    k_gj_update<<<grid, 256, 0, st>>>(Q, P, flag, n, ld, c0, w, sc);
+  }
+}
+
+// ============================================================ boundary transforms
+__global__ void k_invstransh_build(const cd* __restrict__ F, cd* __restrict__ Q,
+                                   cd* __restrict__ P, int n, int ld) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (j >= n) return;
+  int a = r / n, i = r - a * n;
+  cd fh = conj(F[((size_t)a * n + j) * n + i]);  // F^H(i,j) = conj(F(j,i))
+  size_t o = (size_t)r * ld + j;
+  if (i == j) {
+    Q[o] = cd{1.0 + fh.x, fh.y};
+    P[o] = cd{1.0 - fh.x, -fh.y};
+  } else {
+    Q[o] = fh;
+    P[o] = -fh;
+  }
+}
+
+void launch_invstransh_build(const cd* F, cd* Q, cd* P, int nang, int n, int ld, cudaStream_t st) {
+  dim3 grid(ceil_div(n, 128), nang * n);
+  k_invstransh_build<<<grid, 128, 0, st>>>(F, Q, P, n, ld);
+}
+
+__global__ void k_invstransh_finish(cd* __restrict__ P, const cd* __restrict__ gam, int n,
+                                    int ld) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (j >= n) return;
+  int a = r / n, i = r - a * n;
+  size_t o = (size_t)r * ld + j;
+  P[o] = (cd{0.0, 1.0} * P[o]) * conj(gam[(size_t)a * n + i]);
+}
+
+void launch_invstransh_finish(cd* P, const cd* gam, int nang, int n, int ld, cudaStream_t st) {
+  dim3 grid(ceil_div(n, 128), nang * n);
+  k_invstransh_finish<<<grid, 128, 0, st>>>(P, gam, n, ld);
+}
+
+__global__ void k_stransh_build(cd* __restrict__ Q, cd* __restrict__ P, const cd* __restrict__ gam,
+                                int n, int ld) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (j >= n) return;
+  int a = r / n, i = r - a * n;
+  size_t o = (size_t)r * ld + j;
+  cd p = P[o];
+  if (i == j) {
+    cd g = conj(gam[(size_t)a * n + i]);
+    Q[o] = g + cd{0.0, -1.0} * p;
+    P[o] = g + cd{0.0, 1.0} * p;
+  } else {
+    Q[o] = cd{0.0, -1.0} * p;
+    P[o] = cd{0.0, 1.0} * p;
+  }
+}
+
+void launch_stransh_build(cd* Q, cd* P, const cd* gam, int nang, int n, int ld, cudaStream_t st) {
+  dim3 grid(ceil_div(n, 128), nang * n);
+  k_stransh_build<<<grid, 128, 0, st>>>(Q, P, gam, n, ld);
+}
+
+__global__ void k_intensities(const cd* __restrict__ R, const cd* __restrict__ gam,
+                              const double* __restrict__ wnsga2, int n, int ld, int nb0,
+                              double* __restrict__ f2) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int a = blockIdx.y;
+  if (i >= n) return;
+  double s = gam[(size_t)a * n + i].x;
+  double out = 0.0;
+  if (s > 1e-10) {
+    cd f = conj(R[((size_t)a * n + nb0) * ld + i]);  // f(i, nb0) = conj(R(nb0, i))
+    out = (f * conj(f)).x * wnsga2[a] / s;
+  }
+  f2[(size_t)a * n + i] = out;
+}
+
+void launch_intensities(const cd* R, const cd* gam, const double* wnsga2, int nang, int n, int ld,
+                        int nb0, double* f2, cudaStream_t st) {
+  dim3 grid(ceil_div(n, 128), nang);
+  k_intensities<<<grid, 128, 0, st>>>(R, gam, wnsga2, n, ld, nb0, f2);
+}
+
+__global__ void k_check_finite(const cd* __restrict__ X, size_t count, unsigned* status) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool bad = false;
+  for (; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    cd v = X[i];
+    if (!isfinite(v.x) || !isfinite(v.y)) bad = true;
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, kStatusNonFinite);
+}
+
+void launch_check_finite(const cd* X, size_t count, unsigned* status, cudaStream_t st) {
+  k_check_finite<<<148 * 4, 256, 0, st>>>(X, count, status);
+}
+
+}  // namespace trhepd

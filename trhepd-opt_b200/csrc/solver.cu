@@ -1,0 +1,755 @@
+// Batched multislice surface solve and the C ABI (include/trhepd_b200.h).
+//
+// One launch sequence integrates every (azimuth, glancing angle) of a domain at
+// once: the angles' N x N states Q = X^H and P = Y^H are stacked row-wise, the
+// shared stage matrix of each integrator stage is gathered once from the
+// potential table and applied to all angles by one GEMM whose epilogue performs
+// the RKN updates (surf_prkn.f90:278-330).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/trhepd_b200.h"
+#include "host_model.h"
+#include "kernels.h"
+#include "split_gemm.h"
+
+using namespace trhepd;
+
+namespace {
+
+// Blanes-Moan RKN coefficient tables (surf_prkn.f90:11-52).
+const double kRkn46[13] = {
+    0.0829844064174052,  0.245298957184271,  0.396309801498368,  0.604872665711080,
+    -0.0390563049223486, -0.350171622895351, 0.1195241940131508, -0.350171622895351,
+    -0.0390563049223486, 0.604872665711080,  0.396309801498368,  0.245298957184271,
+    0.0829844064174052};
+const double kRkn611[23] = {
+    0.0414649985182624,  0.123229775946271,  0.198128671918067,  0.290553797799558,
+    -0.0400061921041533, -0.127049212625417, 0.0752539843015807, -0.246331761062075,
+    -0.0115113874206879, 0.357208872795928,  0.2366699247869311, 0.20477705429147,
+    0.2366699247869311,  0.357208872795928,  -0.0115113874206879, -0.246331761062075,
+    0.0752539843015807,  -0.127049212625417, -0.0400061921041533, 0.290553797799558,
+    0.198128671918067,   0.123229775946271,  0.0414649985182624};
+
+struct CudaError : std::runtime_error {
+  int code;
+  CudaError(const std::string& m, int c) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(x)                                                                              \
+  do {                                                                                     \
+    cudaError_t e_ = (x);                                                                  \
+    if (e_ != cudaSuccess)                                                                 \
+      throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_),                     \
+                      e_ == cudaErrorMemoryAllocation ? TRHEPD_ENOMEM : TRHEPD_ECUDA);     \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  void* ensure(size_t bytes) {
+    if (bytes <= n && p) return p;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (bytes == 0) bytes = 256;
+    CK(cudaMalloc(&p, bytes));
+    n = bytes;
+    return p;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+template <class T>
+T* upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+  b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+  if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return b.as<T>();
+}
+
+struct Integrator {
+  int s;
+  const double* bab;
+};
+
+Integrator integrator_for(int method) {
+  if (method == 5) return {6, kRkn46};
+  if (method == 6) return {11, kRkn611};
+  throw std::invalid_argument("int_method must be 5 (RKN-4) or 6 (RKN-6) on the GPU path");
+}
+
+// Stage depths of hp_int_init (surf_prkn.f90:184-196), same arithmetic order.
+std::vector<double> stage_depths(const Integrator& I, int ns, double dz) {
+  std::vector<double> d;
+  d.reserve((size_t)I.s * ns + 1);
+  for (int l = 1; l <= ns; ++l) {
+    double iz = dz * (l - 1);
+    for (int k = 1; k <= I.s; ++k) {
+      d.push_back(iz);
+      iz = iz + dz * I.bab[2 * k - 1];
+    }
+  }
+  d.push_back(dz * ns);
+  return d;
+}
+
+}  // namespace
+
+struct trhepd_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  int renorm_policy = 0;
+  double renorm_tau = std::log(1e3);
+  int split_slices = 4;
+  double stats[4] = {0, 0, 0, 0};
+  // device buffers (grown on demand, reused across calls)
+  DevBuf asf, b, dchg, ghk, z[3], ocr[3], ielm[3], st[3], depth, table, pair;
+  DevBuf Q0, Q1, P, V, D, gam, F, flags, dval, gj, f2, wnsga2, status, split;
+  DevBuf sgh, sgk, simg, snimg, sst;
+};
+
+namespace {
+
+int fail(trhepd_context* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+// Upload mod_scpot3 and build the stage table on the device.
+void build_table(trhepd_context* C, const trhepd_pot_state& pot, const std::vector<double>& depth,
+                 TableEntry** table_out) {
+  cudaStream_t st = C->stream;
+  const int nv = pot.nv, nelm = pot.nelm;
+  const int natm = pot.natmb + pot.natms;
+  // the table kernel stages natms + 2*natmb atom factors in shared memory
+  if (pot.natms + 2 * pot.natmb > 512)
+    throw std::invalid_argument("natms + 2*natmb exceeds 512 (potential table limit)");
+  (void)natm;
+  if (pot.nabr + pot.nabi > kMab || pot.nabr > 6) throw std::invalid_argument("nabr+nabi > 6");
+  auto up = [&](DevBuf& b, const void* src, size_t bytes) {
+    b.ensure(std::max<size_t>(bytes, 16));
+    if (bytes) CK(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, st));
+    return b.p;
+  };
+  PotInputs in{};
+  in.asf = (const double*)up(C->asf, pot.asf, (size_t)nv * kMab * nelm * sizeof(double));
+  in.b = (const double*)up(C->b, pot.b, (size_t)kMab * nelm * sizeof(double));
+  in.dchg = (const double*)up(C->dchg, pot.dchg, (size_t)nelm * sizeof(double));
+  in.ghk = (const double*)up(C->ghk, pot.Ghk, (size_t)nv * sizeof(double));
+  in.nv = nv;
+  in.nelm = nelm;
+  in.nabr = pot.nabr;
+  in.nabi = pot.nabi;
+  in.mab = kMab;
+  // parts: surface at zi - cc (all nv), top bulk at zi, second bulk at zi + cc (nvb)
+  const int first[3] = {pot.natmb, 0, 0};
+  const int count[3] = {pot.natms, pot.natmb, pot.natmb};
+  const double shift[3] = {-pot.cc, 0.0, pot.cc};
+  const double mesh[3] = {1.0, pot.smesh, pot.smesh};
+  const int nk[3] = {nv, pot.nvb, pot.nvb};
+  const double* stp[3] = {pot.st0, pot.st1, pot.st2};
+  for (int p = 0; p < 3; ++p) {
+    std::vector<int> ie(count[p]);
+    for (int j = 0; j < count[p]; ++j) {
+      int e = pot.ielm[first[p] + j];
+      if (e < 1 || e > nelm) throw std::invalid_argument("ielm out of range");
+      ie[j] = e - 1;
+    }
+    PotPart& P = in.part[p];
+    P.z = (const double*)up(C->z[p], pot.z + first[p], count[p] * sizeof(double));
+    P.ocr = (const double*)up(C->ocr[p], pot.ocr + first[p], count[p] * sizeof(double));
+    P.ielm = upload(C->ielm[p], ie, st);
+    P.st = (const cd*)up(C->st[p], stp[p], (size_t)nk[p] * count[p] * sizeof(cd));
+    P.natm = count[p];
+    P.nk = nk[p];
+    P.zshift = shift[p];
+    P.rmesh = mesh[p];
+  }
+  const double* dd = upload(C->depth, depth, st);
+  int ncol = (int)depth.size();
+  TableEntry* table = (TableEntry*)C->table.ensure((size_t)ncol * nv * sizeof(TableEntry));
+  launch_potential_table(in, dd, ncol, table, st);
+  CK(cudaGetLastError());
+  *table_out = table;
+}
+
+struct SolveArgs {
+  const trhepd_pot_state* pot;
+  int nb, ns;
+  const int32_t* iv;
+  double dz;
+  int ngr;
+  const int32_t *nbg, *iord, *ih, *ik;
+  double wn, ghx, ghy, gky, azi, daz, gi, dg;
+  int naz, ng, int_method;
+  const double* t1;
+  int precision;
+};
+
+// The batched solve behind trhepd_srfref.
+void solve(trhepd_context* C, const SolveArgs& A, double* f2_out, double* angle_out) {
+  const int n = A.nb, ns = A.ns;
+  if (n < 1 || ns < 1) throw std::invalid_argument("nb and ns must be >= 1");
+  if (n > kMaxBeams) throw std::invalid_argument("nb exceeds the GPU path limit");
+  const Integrator I = integrator_for(A.int_method);
+  const std::vector<double> depth = stage_depths(I, ns, A.dz);
+  cudaStream_t st = C->stream;
+  TableEntry* table = nullptr;
+  build_table(C, *A.pot, depth, &table);
+  const int nv = A.pot->nv;
+
+  // ---- beam-pair map for the gather: pair[k*n+j] = iv(max,min) - 1
+  std::vector<int> pair((size_t)n * n, 0);
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j) {
+      if (k == j) continue;
+      int hi = std::max(k, j), lo = std::min(k, j);
+      int e = A.iv[(size_t)lo * n + hi];
+      if (e < 1 || e > nv) throw std::invalid_argument("iv entry out of range");
+      pair[(size_t)k * n + j] = e - 1;
+    }
+  const int* d_pair = upload(C->pair, pair, st);
+
+  // ---- angle schedule (surflf.f90:43-92)
+  const bool ng_outer = A.ng > A.naz;
+  const int nrep1 = ng_outer ? A.naz : A.ng, nrep2 = ng_outer ? A.ng : A.naz;
+  const int nang = nrep1 * nrep2;
+  const int ld = round_up(n, 16), kpad = ld;
+  std::vector<cd> gam((size_t)nang * n), Dm((size_t)nang * ld, cd{0, 0}), F((size_t)nang * n * n);
+  std::vector<double> wnsga2(nang);
+  size_t per = 0;
+  for (int l = 0; l < A.ngr; ++l) per += (size_t)A.nbg[l] * A.nbg[l];
+  {
+    int sum = 0;
+    for (int l = 0; l < A.ngr; ++l) sum += A.nbg[l];
+    if (sum != n) throw std::invalid_argument("sum(nbg) != nb");
+    for (int i = 0; i < n; ++i)
+      if (A.iord[i] < 1 || A.iord[i] > n) throw std::invalid_argument("iord out of range");
+  }
+  double kappa_max = 0.0;
+  for (int t = 0; t < nang; ++t) {
+    int irep1 = t / nrep2, irep2 = t % nrep2;
+    double ga, az;
+    if (ng_outer) {
+      az = A.azi + irep1 * A.daz;
+      ga = A.gi + irep2 * A.dg;
+    } else {
+      ga = A.gi + irep1 * A.dg;
+      az = A.azi + irep2 * A.daz;
+    }
+    double cga = std::cos(ga), sga = std::sin(ga), caz = std::cos(az), saz = std::sin(az);
+    wnsga2[t] = A.wn * sga * sga;
+    double wnx = A.wn * cga * caz, wny = A.wn * cga * saz;
+    for (int i = 0; i < n; ++i) {
+      double wgx = A.ghx * A.ih[i] + wnx;
+      double wgy = A.ghy * A.ih[i] + A.gky * A.ik[i] + wny;
+      double s = A.wn * A.wn - wgx * wgx - wgy * wgy;
+      cd g = (s >= 0.0) ? cd{std::sqrt(s), 0.0} : cd{0.0, std::sqrt(-s)};
+      gam[(size_t)t * n + i] = g;
+      cd g2 = g * g;
+      Dm[(size_t)t * ld + i] = cd{-g2.x, g2.y};  // -conj(g^2)
+      if (s < 0) kappa_max = std::max(kappa_max, std::sqrt(-s));
+    }
+    if (angle_out) angle_out[t] = (ng_outer ? ga : az) * 180.0 / 3.141592654;
+    // bulk f permuted by iord (surflf.f90:105-115); F row-major (i, j)
+    const double* rec = A.t1 + 2 * per * t;
+    cd* Ft = F.data() + (size_t)t * n * n;
+    std::fill(Ft, Ft + (size_t)n * n, cd{0, 0});
+    int ib1 = 0;
+    size_t o = 0;
+    for (int l = 0; l < A.ngr; ++l) {
+      int m = A.nbg[l];
+      for (int j = 0; j < m; ++j)
+        for (int i = 0; i < m; ++i, ++o) {
+          int r = A.iord[ib1 + i] - 1, c = A.iord[ib1 + j] - 1;
+          Ft[(size_t)r * n + c] = cd{rec[2 * o], rec[2 * o + 1]};
+        }
+      ib1 += m;
+    }
+  }
+  int nb0 = 0;
+  for (int i = 0; i < n; ++i)
+    if (A.ih[i] == 0 && A.ik[i] == 0) nb0 = i;
+
+  const cd* d_gam = upload(C->gam, gam, st);
+  const cd* d_D = upload(C->D, Dm, st);
+  const cd* d_F = upload(C->F, F, st);
+  const double* d_w = upload(C->wnsga2, wnsga2, st);
+  const size_t sbytes = (size_t)nang * n * ld * sizeof(cd);
+  cd* Q = (cd*)C->Q0.ensure(sbytes);
+  cd* Qn = (cd*)C->Q1.ensure(sbytes);
+  cd* P = (cd*)C->P.ensure(sbytes);
+  CK(cudaMemsetAsync(Q, 0, sbytes, st));
+  CK(cudaMemsetAsync(Qn, 0, sbytes, st));
+  CK(cudaMemsetAsync(P, 0, sbytes, st));
+  cd* V = (cd*)C->V.ensure((size_t)kpad * ld * sizeof(cd));
+  int* flags = (int*)C->flags.ensure(std::max(nang, 4) * sizeof(int));
+  double* dval = (double*)C->dval.ensure(std::max(nang, 4) * sizeof(double));
+  void* gjs = C->gj.ensure(gj_scratch_bytes(nang, n));
+  unsigned* status = (unsigned*)C->status.ensure(16);
+  CK(cudaMemsetAsync(status, 0, 16, st));
+  const bool split = A.precision == TRHEPD_SPLIT_BF16;
+  SplitWorkspace sw{};
+  if (split) {
+    sw = split_workspace_carve(C->split.ensure(split_workspace_bytes(nang, n, C->split_slices)),
+                               nang, n, C->split_slices);
+  }
+
+  CK(cudaEventRecord(C->ev0, st));
+  // ---- invstransh: Q = I + F^H, P = I - F^H; P <- Q^{-1} P; P <- i P conj(G); Q = I
+  launch_invstransh_build(d_F, Q, P, nang, n, ld, st);
+  launch_gauss_jordan(Q, P, nullptr, nang, n, ld, gjs, status, st);
+  launch_invstransh_finish(P, d_gam, nang, n, ld, st);
+  launch_set_identity(Q, nullptr, nang, n, ld, st);
+
+  // ---- renormalisation schedule
+  const bool every_slice = (n == 1 && A.int_method == 6);  // hp_int_spa1d renormalises each slice
+  int interval = 1;
+  if (C->renorm_policy == 1 && !every_slice) {
+    double kap = kappa_max + 1.0;
+    interval = std::max(1, (int)std::floor(C->renorm_tau / (kap * A.dz)));
+  }
+  long renorms = 0, products = 0;
+  const double dz = A.dz;
+  for (int l = 1; l <= ns; ++l) {
+    for (int k = 1; k <= I.s; ++k) {
+      const int col = I.s * (l - 1) + k - 1;
+      const double ca = I.bab[2 * k - 1] * dz;
+      const TableEntry* tc = table + (size_t)col * nv;
+      if (l == 1 && k == 1) {  // Q = I: elementwise stage
+        launch_gather_stage(tc, d_pair, n, kpad, ld, false, V, st);
+        launch_stage_identity(Q, P, V, d_D, nang, n, ld, I.bab[0] * dz, ca, st);
+        continue;
+      }
+      // k == 1, l > 1 merges the end-of-slice half kick of slice l-1 (psave) with the
+      // first kick of slice l: both use the same stage column, so cb = 2 b1.
+      const double cb = (k == 1) ? 2.0 * I.bab[0] * dz : I.bab[2 * k - 2] * dz;
+      if (split) {
+        launch_gather_stage(tc, d_pair, n, kpad, ld, true, V, st);
+        split_stage(sw, Q, P, Qn, V, d_D, nang, n, ld, cb, ca, C->split_slices, st);
+      } else {
+        launch_gather_stage(tc, d_pair, n, kpad, ld, false, V, st);
+        launch_stage_gemm_f64(Q, P, Qn, V, d_D, nang, n, ld, kpad, cb, ca, st);
+      }
+      std::swap(Q, Qn);
+      ++products;
+    }
+    // end of slice: renormalisation decision on Q (the reference tests Q after the
+    // last stage; the end-of-slice kick does not change Q)
+    const bool last = (l == ns);
+    if (C->renorm_policy == 0 && !every_slice) {
+      launch_cond_est(Q, nang, n, ld, last ? 1 : 0, flags, dval, st);
+      launch_gauss_jordan(Q, P, flags, nang, n, ld, gjs, status, st);
+      launch_set_identity(Q, flags, nang, n, ld, st);
+      if (!last) ++renorms;  // upper bound; exact per-angle counts stay on the device
+    } else if (last || every_slice || (l % interval) == 0) {
+      launch_gauss_jordan(Q, P, nullptr, nang, n, ld, gjs, status, st);
+      launch_set_identity(Q, nullptr, nang, n, ld, st);
+      if (!last) ++renorms;
+    }
+  }
+  // final half kick with Q = I: P += b1 dz M(end)
+  {
+    const TableEntry* tc = table + (size_t)(I.s * ns) * nv;
+    launch_gather_stage(tc, d_pair, n, kpad, ld, false, V, st);
+    launch_stage_identity(Q, P, V, d_D, nang, n, ld, I.bab[0] * dz, 0.0, st);
+  }
+  // ---- stransh and intensities
+  launch_stransh_build(Q, P, d_gam, nang, n, ld, st);
+  launch_gauss_jordan(Q, P, nullptr, nang, n, ld, gjs, status, st);
+  launch_check_finite(P, (size_t)nang * n * ld, status, st);
+  double* d_f2 = (double*)C->f2.ensure((size_t)nang * n * sizeof(double));
+  launch_intensities(P, d_gam, d_w, nang, n, ld, nb0, d_f2, st);
+  CK(cudaEventRecord(C->ev1, st));
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(f2_out, d_f2, (size_t)nang * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  unsigned h_status[4];
+  CK(cudaMemcpyAsync(h_status, status, 16, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, C->ev0, C->ev1);
+  C->stats[0] = (double)renorms;
+  C->stats[1] = (double)products;
+  C->stats[2] = ms;
+  C->stats[3] = (double)depth.size();
+  if (h_status[0] & kStatusTimeout) throw CudaError("device wait timed out", TRHEPD_ETIMEOUT);
+  if (h_status[0] & (kStatusNonFinite | kStatusZeroPivot))
+    throw CudaError("non-finite value or zero pivot in the surface solve", TRHEPD_ENONFINITE);
+}
+
+// Structure factors of SurfaceInputs on the device.
+void structure_factors(trhepd_context* C, SurfaceInputs& S) {
+  std::vector<cd>* outs[3] = {&S.st0, &S.st1, &S.st2};
+  for (int p = 0; p < 3; ++p) {
+    const StructureFactorJob& J = S.stf[p];
+    outs[p]->assign((size_t)J.nk * J.natm, cd{0, 0});
+    if (J.natm == 0 || J.nk == 0) continue;
+    const double* gh = upload(C->sgh, S.gh, C->stream);
+    const double* gk = upload(C->sgk, S.gk, C->stream);
+    const double* img = upload(C->simg, J.img, C->stream);
+    const int* nimg = upload(C->snimg, J.nimg, C->stream);
+    cd* st = (cd*)C->sst.ensure((size_t)J.nk * J.natm * sizeof(cd));
+    launch_structure_factor(gh, gk, J.nk, img, nimg, J.natm, J.dx, J.dy, st, C->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(outs[p]->data(), st, (size_t)J.nk * J.natm * sizeof(cd),
+                       cudaMemcpyDeviceToHost, C->stream));
+    CK(cudaStreamSynchronize(C->stream));
+  }
+}
+
+trhepd_pot_state pot_view(const SurfaceInputs& S) {
+  trhepd_pot_state p{};
+  p.nv = S.nv;
+  p.nvb = S.nvb;
+  p.natms = S.natms;
+  p.natmb = S.natmb;
+  p.nelm = S.nelm;
+  p.nabr = S.nabr;
+  p.nabi = S.nabi;
+  p.ielm = S.ielm.data();
+  p.cc = S.cc;
+  p.smesh = S.smesh;
+  p.z = S.z.data();
+  p.dchg = S.dchg.data();
+  p.Ghk = S.Ghk.data();
+  p.ocr = S.ocr.data();
+  p.b = S.b.data();
+  p.asf = S.asf.data();
+  p.st0 = reinterpret_cast<const double*>(S.st0.data());
+  p.st1 = reinterpret_cast<const double*>(S.st1.data());
+  p.st2 = reinterpret_cast<const double*>(S.st2.data());
+  return p;
+}
+
+template <class F>
+int guarded(trhepd_context* ctx, F&& f) {
+  if (!ctx) return TRHEPD_EINVAL;
+  try {
+    CK(cudaSetDevice(ctx->device));
+    f();
+    ctx->err.clear();
+    return TRHEPD_OK;
+  } catch (const CudaError& e) {
+    return fail(ctx, e.code, e.what());
+  } catch (const std::invalid_argument& e) {
+    return fail(ctx, TRHEPD_EINVAL, e.what());
+  } catch (const std::bad_alloc& e) {
+    return fail(ctx, TRHEPD_ENOMEM, e.what());
+  } catch (const std::runtime_error& e) {
+    return fail(ctx, TRHEPD_EIO, e.what());
+  }
+}
+
+// ---- Fortran rocking-curve writer (surfio.f90:270-274, surflf.f90:154-165)
+std::string fortran_e(double v, int w, int d) {
+  std::string body;
+  if (v == 0.0) {
+    body = "0." + std::string(d, '0') + "E+00";
+  } else {
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%.*e", d - 1, std::fabs(v));
+    std::string s(buf);
+    size_t e = s.find('e');
+    std::string digits = s.substr(0, 1) + s.substr(2, e - 2);
+    int ex = std::atoi(s.c_str() + e + 1) + 1;
+    char eb[16];
+    if (std::abs(ex) <= 99)
+      std::snprintf(eb, sizeof eb, "E%c%02d", ex < 0 ? '-' : '+', std::abs(ex));
+    else
+      std::snprintf(eb, sizeof eb, "%c%03d", ex < 0 ? '-' : '+', std::abs(ex));
+    body = std::string(v < 0 ? "-" : "") + "0." + digits + eb;
+  }
+  if ((int)body.size() > w) return std::string(w, '*');
+  return std::string(w - body.size(), ' ') + body;
+}
+
+}  // namespace
+
+namespace trhepd {
+void write_rocking_curves(const std::string& path, const SurfaceInputs& S, const double* f2,
+                          const double* angle_deg) {
+  FILE* o = std::fopen(path.c_str(), "w");
+  if (!o) throw std::runtime_error("cannot write " + path);
+  std::fprintf(o, "#azimuths,g-angles,beams\n%4d%4d%4d\n#ih,ik\n", S.naz, S.ng, S.nb);
+  int cnt = 0;
+  for (int j = 0; j < S.nb; ++j) {
+    for (int v : {S.ih[j], S.ik[j]}) {
+      std::fprintf(o, "%4d", v);
+      if (++cnt % 400 == 0 && cnt < 2 * S.nb) std::fprintf(o, "\n");
+    }
+  }
+  std::fprintf(o, "\n");
+  const bool ng_outer = S.ng > S.naz;
+  const int nrep1 = ng_outer ? S.naz : S.ng, nrep2 = ng_outer ? S.ng : S.naz;
+  for (int r1 = 0; r1 < nrep1; ++r1) {
+    for (int r2 = 0; r2 < nrep2; ++r2) {
+      int t = r1 * nrep2 + r2;
+      std::string line = fortran_e(angle_deg[t], 12, 4);
+      for (int i = 0; i < S.nb; ++i) {
+        if (i > 0 && i % 200 == 0) {
+          std::fprintf(o, "%s\n", line.c_str());
+          line.clear();
+        }
+        line += ",";
+        line += fortran_e(f2[(size_t)t * S.nb + i], 23, 15);
+      }
+      std::fprintf(o, "%s,\n", line.c_str());
+    }
+    std::fprintf(o, "\n");
+  }
+  std::fclose(o);
+}
+}  // namespace trhepd
+
+// =============================================================================
+// C ABI
+// =============================================================================
+extern "C" {
+
+int trhepd_create(int device, trhepd_context** out) {
+  if (!out) return TRHEPD_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return TRHEPD_ECUDA;
+  if (device < 0 || device >= ndev) return TRHEPD_EINVAL;
+  auto* c = new trhepd_context();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    delete c;
+    return TRHEPD_ECUDA;
+  }
+  *out = c;
+  return TRHEPD_OK;
+}
+
+void trhepd_destroy(trhepd_context* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  DevBuf* all[] = {&c->asf, &c->b, &c->dchg, &c->ghk, &c->depth, &c->table, &c->pair,
+                   &c->Q0, &c->Q1, &c->P, &c->V, &c->D, &c->gam, &c->F, &c->flags, &c->dval,
+                   &c->gj, &c->f2, &c->wnsga2, &c->status, &c->split, &c->sgh, &c->sgk,
+                   &c->simg, &c->snimg, &c->sst};
+  for (DevBuf* b : all) b->release();
+  for (int p = 0; p < 3; ++p) {
+    c->z[p].release();
+    c->ocr[p].release();
+    c->ielm[p].release();
+    c->st[p].release();
+  }
+  cudaEventDestroy(c->ev0);
+  cudaEventDestroy(c->ev1);
+  cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* trhepd_last_error(const trhepd_context* c) { return c ? c->err.c_str() : "no context"; }
+
+int trhepd_set_option(trhepd_context* c, int option, double value) {
+  if (!c) return TRHEPD_EINVAL;
+  switch (option) {
+    case TRHEPD_OPT_RENORM_POLICY:
+      if (value != 0.0 && value != 1.0) return fail(c, TRHEPD_EINVAL, "renorm policy must be 0 or 1");
+      c->renorm_policy = (int)value;
+      return TRHEPD_OK;
+    case TRHEPD_OPT_RENORM_TAU:
+      if (!(value > 0.0)) return fail(c, TRHEPD_EINVAL, "renorm tau must be > 0");
+      c->renorm_tau = value;
+      return TRHEPD_OK;
+    case TRHEPD_OPT_SPLIT_SLICES:
+      if (value < 3 || value > 5) return fail(c, TRHEPD_EINVAL, "split slices must be 3..5");
+      c->split_slices = (int)value;
+      return TRHEPD_OK;
+  }
+  return fail(c, TRHEPD_EINVAL, "unknown option");
+}
+
+int trhepd_last_stats(const trhepd_context* c, double* out, int n) {
+  if (!c || !out) return TRHEPD_EINVAL;
+  for (int i = 0; i < n && i < 4; ++i) out[i] = c->stats[i];
+  return TRHEPD_OK;
+}
+
+int trhepd_plane_group_images(int nsg, int ma, int mb, int na, int nb, double x, double y,
+                              double* out_xy, int* count) {
+  if (!out_xy || !count || nsg < 1 || nsg > 17 || ma * nb - mb * na == 0) return TRHEPD_EINVAL;
+  *count = trhepd::plane_group_images(nsg, ma, mb, na, nb, x, y, out_xy);
+  return TRHEPD_OK;
+}
+
+int trhepd_structure_factors(trhepd_context* ctx, int nv, const double* gh, const double* gk,
+                             int natm, const double* img, const int32_t* nimg, double dx,
+                             double dy, double* st) {
+  return guarded(ctx, [&] {
+    if (nv < 0 || natm < 0 || (!st && nv * natm > 0)) throw std::invalid_argument("bad sizes");
+    for (int j = 0; j < natm; ++j)
+      if (nimg[j] < 1 || nimg[j] > 12) throw std::invalid_argument("image count must be 1..12");
+    std::vector<double> vgh(gh, gh + nv), vgk(gk, gk + nv), vimg(img, img + (size_t)natm * 24);
+    std::vector<int> vn(nimg, nimg + natm);
+    const double* a = upload(ctx->sgh, vgh, ctx->stream);
+    const double* b = upload(ctx->sgk, vgk, ctx->stream);
+    const double* c = upload(ctx->simg, vimg, ctx->stream);
+    const int* d = upload(ctx->snimg, vn, ctx->stream);
+    cd* out = (cd*)ctx->sst.ensure(std::max<size_t>((size_t)nv * natm * sizeof(cd), 16));
+    launch_structure_factor(a, b, nv, c, d, natm, dx, dy, out, ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(st, out, (size_t)nv * natm * sizeof(cd), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int trhepd_potential_table(trhepd_context* ctx, const trhepd_pot_state* pot, int int_method,
+                           int ns, double dz, double* v, double* vi, int* ncol) {
+  return guarded(ctx, [&] {
+    if (!pot || ns < 1) throw std::invalid_argument("bad arguments");
+    Integrator I = integrator_for(int_method);
+    std::vector<double> depth = stage_depths(I, ns, dz);
+    TableEntry* table = nullptr;
+    build_table(ctx, *pot, depth, &table);
+    size_t cnt = depth.size() * (size_t)pot->nv;
+    std::vector<TableEntry> h(cnt);
+    CK(cudaMemcpyAsync(h.data(), table, cnt * sizeof(TableEntry), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t e = 0; e < cnt; ++e) {  // v = (u + w) / 2, vi = (u - w) / 2
+      if (v) {
+        v[2 * e] = 0.5 * (h[e].u.x + h[e].w.x);
+        v[2 * e + 1] = 0.5 * (h[e].u.y + h[e].w.y);
+      }
+      if (vi) {
+        vi[2 * e] = 0.5 * (h[e].u.x - h[e].w.x);
+        vi[2 * e + 1] = 0.5 * (h[e].u.y - h[e].w.y);
+      }
+    }
+    if (ncol) *ncol = (int)depth.size();
+  });
+}
+
+int trhepd_srfref(trhepd_context* ctx, const trhepd_pot_state* pot, int nb, int ns,
+                  const int32_t* iv, double dz, int ngr, const int32_t* nbg, const int32_t* iord,
+                  const int32_t* ih, const int32_t* ik, double wn, double ghx, double ghy,
+                  double gky, double azi, double daz, int naz, double gi, double dg, int ng,
+                  int int_method, const double* t1_records, int precision, double* f2,
+                  double* angle_deg) {
+  return guarded(ctx, [&] {
+    if (!pot || !iv || !nbg || !iord || !ih || !ik || !t1_records || !f2)
+      throw std::invalid_argument("null argument");
+    if (naz < 1 || ng < 1 || ngr < 1) throw std::invalid_argument("naz, ng, ngr must be >= 1");
+    if (precision != TRHEPD_FP64 && precision != TRHEPD_SPLIT_BF16)
+      throw std::invalid_argument("unknown precision form");
+    SolveArgs a{pot, nb, ns, iv, dz, ngr, nbg, iord, ih, ik, wn, ghx, ghy, gky,
+                azi, daz, gi, dg, naz, ng, int_method, t1_records, precision};
+    solve(ctx, a, f2, angle_deg);
+  });
+}
+
+struct trhepd_surface_inputs {
+  SurfaceInputs S;
+};
+
+int trhepd_surf_load(trhepd_context* ctx, const char* bulkp, const char* surf, double dz2,
+                     int int_method, trhepd_surface_inputs** out) {
+  if (!out) return TRHEPD_EINVAL;
+  *out = nullptr;
+  auto* h = new trhepd_surface_inputs();
+  int rc = guarded(ctx, [&] {
+    if (!bulkp || !surf || !(dz2 > 0)) throw std::invalid_argument("bad arguments");
+    load_surface_inputs(bulkp, surf, dz2, int_method, h->S);
+    structure_factors(ctx, h->S);
+  });
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return TRHEPD_OK;
+}
+
+void trhepd_surf_free(trhepd_surface_inputs* in) { delete in; }
+
+int trhepd_surf_views(const trhepd_surface_inputs* in, trhepd_pot_state* pot,
+                      trhepd_srfref_args* a) {
+  if (!in) return TRHEPD_EINVAL;
+  const SurfaceInputs& S = in->S;
+  if (pot) *pot = pot_view(S);
+  if (a) {
+    a->nb = S.nb;
+    a->ns = S.ns;
+    a->iv = S.iv.data();
+    a->dz = S.dz;
+    a->ngr = S.ngr;
+    a->nbg = S.nbg.data();
+    a->iord = S.iord.data();
+    a->ih = S.ih.data();
+    a->ik = S.ik.data();
+    a->wn = S.wn;
+    a->ghx = S.ghx;
+    a->ghy = S.ghy;
+    a->gky = S.gky;
+    a->azi = S.azi;
+    a->daz = S.daz;
+    a->naz = S.naz;
+    a->gi = S.gi;
+    a->dg = S.dg;
+    a->ng = S.ng;
+    a->int_method = S.int_method;
+    a->t1_records = reinterpret_cast<const double*>(S.t1rec.data());
+    const bool ng_outer = S.ng > S.naz;
+    a->nrep1 = ng_outer ? S.naz : S.ng;
+    a->nrep2 = ng_outer ? S.ng : S.naz;
+  }
+  return TRHEPD_OK;
+}
+
+int trhepd_surf_run(trhepd_context* ctx, const char* bulkp, const char* surf, double dz2,
+                    int int_method, int precision, const char* out_path, double* f2, int max_f2,
+                    int* dims) {
+  return guarded(ctx, [&] {
+    if (!bulkp || !surf || !(dz2 > 0)) throw std::invalid_argument("bad arguments");
+    SurfaceInputs S;
+    load_surface_inputs(bulkp, surf, dz2, int_method, S);
+    structure_factors(ctx, S);
+    trhepd_pot_state pot = pot_view(S);
+    int nang = S.naz * S.ng;
+    std::vector<double> out((size_t)nang * S.nb), ang(nang);
+    SolveArgs a{&pot, S.nb, S.ns, S.iv.data(), S.dz, S.ngr, S.nbg.data(), S.iord.data(),
+                S.ih.data(), S.ik.data(), S.wn, S.ghx, S.ghy, S.gky, S.azi, S.daz, S.gi, S.dg,
+                S.naz, S.ng, int_method, reinterpret_cast<const double*>(S.t1rec.data()),
+                precision};
+    solve(ctx, a, out.data(), ang.data());
+    if (out_path) write_rocking_curves(out_path, S, out.data(), ang.data());
+    if (f2) {
+      if ((size_t)max_f2 < out.size()) throw std::invalid_argument("f2 buffer too small");
+      std::memcpy(f2, out.data(), out.size() * sizeof(double));
+    }
+    if (dims) {
+      dims[0] = S.nb;
+      dims[1] = nang;
+      dims[2] = S.ns;
+      dims[3] = S.nv;
+    }
+  });
+}
+
+}  // extern "C"

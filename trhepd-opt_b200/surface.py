@@ -1,0 +1,77 @@
+"""Python mirror of the reference's surface-solve interface.
+
+``SurfaceProblem`` plays surfio (sim-trhepd-rheed/src/surfio.f90:60-381): it
+reads the unchanged bulkP.b / surf.txt and exposes the mod_scpot3 state and
+srfref's arguments.  ``srfref`` calls the C-ABI replacement of srfref
+(surflf.f90:7-171) and ``potential_table`` the replacement of the integrator
+init routines (surf_prkn.f90:174-197).  Everything runs through the CUDA
+library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import native
+
+
+class SurfaceProblem:
+    def __init__(self, ctx: native.Context, bulkp, surf, dz2: float, int_method: int = 5):
+        h = ctypes.c_void_p()
+        L = native.load()
+        ctx._check(L.trhepd_surf_load(ctx._h, str(bulkp).encode(), str(surf).encode(),
+                                      float(dz2), int(int_method), ctypes.byref(h)))
+        self._h, self._L, self.ctx = h, L, ctx
+        self.pot = native.PotState()
+        self.args = native.SrfrefArgs()
+        ctx._check(L.trhepd_surf_views(h, ctypes.byref(self.pot), ctypes.byref(self.args)))
+
+    @property
+    def n_angles(self) -> int:
+        return self.args.nrep1 * self.args.nrep2
+
+    def srfref(self, precision: int = native.FP64):
+        """All (azimuth, angle) solves of the domain: (angles_deg, f2[nangles, nb])."""
+        a = self.args
+        f2 = np.zeros((self.n_angles, a.nb))
+        ang = np.zeros(self.n_angles)
+        self.ctx._check(self._L.trhepd_srfref(
+            self.ctx._h, ctypes.byref(self.pot), a.nb, a.ns, a.iv, a.dz, a.ngr, a.nbg, a.iord,
+            a.ih, a.ik, a.wn, a.ghx, a.ghy, a.gky, a.azi, a.daz, a.naz, a.gi, a.dg, a.ng,
+            a.int_method, a.t1_records, int(precision), f2.ctypes.data, ang.ctypes.data))
+        return ang, f2
+
+    def potential_table(self, int_method: int | None = None):
+        """Stage potential tables v, vi as (ncol, nv) complex arrays."""
+        m = self.args.int_method if int_method is None else int_method
+        s = {5: 6, 6: 11}[m]
+        ncol = s * self.args.ns + 1
+        v = np.zeros((ncol, self.pot.nv), dtype=np.complex128)
+        vi = np.zeros_like(v)
+        nc = ctypes.c_int(0)
+        self.ctx._check(self._L.trhepd_potential_table(
+            self.ctx._h, ctypes.byref(self.pot), m, self.args.ns, self.args.dz,
+            v.ctypes.data, vi.ctypes.data, ctypes.byref(nc)))
+        assert nc.value == ncol
+        return v, vi
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.trhepd_surf_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def potential_table(ctx: native.Context, bulkp, surf, dz2: float, int_method: int = 5):
+    return SurfaceProblem(ctx, bulkp, surf, dz2, int_method).potential_table()
+
+
+def srfref(ctx: native.Context, bulkp, surf, dz2: float, int_method: int = 5,
+           precision: int = native.FP64):
+    return SurfaceProblem(ctx, bulkp, surf, dz2, int_method).srfref(precision)
