@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Angle-solves/s of the multislice surface solve on B200.
+
+Workload (default ``dense521``): synthetic 2x2 Si/Ge surface over a 4-atom
+bulk, N = 521 beams, 61 glancing angles (0.5..6.5 deg), 2004 slices of
+0.01 A, symplectic RKN-4 (int_method 5).  One step = one solve of all 61 angles.
+
+* ``value``: split-precision (BF16 slices on tcgen05) when available, else the
+  plain FP64 form, with inputs resident in HBM (trhepd_problem_solve), device
+  time from CUDA events on the library stream, max over ranks.
+* ``e2e``: the same metric through the C ABI with host buffers
+  (trhepd_srfref: uploads, stage-table build, solve, intensities back).
+* ``fp64``: the plain FP64 form of the same workload for comparison.
+* ``roofline``: the stage-product kernel, live event timing of every launch.
+* ``cpu_baseline``: the CPU oracle (C++ restatement of the reference path,
+  OpenMP over angles, OpenBLAS) on a bounded sample of the workload.
+
+Multi-GPU (torchrun): every rank solves its own workload (independent angle
+batches, no collective on the data path): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+
+def load_package():
+    name = "trhepd_opt_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = ROOT / "trhepd-opt_b200"
+    spec = importlib.util.spec_from_file_location(name, pkg / "__init__.py",
+                                                  submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+load_package()
+from trhepd_opt_b200 import build as tbuild  # noqa: E402
+from trhepd_opt_b200 import bulkfile, generator, native, surface  # noqa: E402
+
+METRIC = "angle-solves/s at N=521, split-precision vs FP64 on 1 B200; p50/p99 latency"
+WORKLOADS = {
+    "dense521": ("dense521: N=521 beams, 61 glancing angles 0.5-6.5 deg, 20 A region in 0.01 A "
+                 "slices (sp4 RKN), synthetic 2x2 Si/Ge surface over 4-atom bulk, seed 3",
+                 lambda seed: generator.dense(521, seed=3 + seed)),
+    "dense521s": ("dense521s (profiling case): N=521 beams, 16 angles, 4 A region in 0.01 A "
+                  "slices (sp4), same generator as dense521",
+                  lambda seed: generator.dense(521, n_angles=16, region=4.0, seed=3 + seed)),
+    "small23": ("small23: N=23 beams, 61 angles, 15 A region in 0.02 A slices (sp4), seed 1",
+                lambda seed: generator.small23(1 + seed)),
+    "batch47": ("batch47: N=47 beams, 121 angles x 2 azimuths, 15 A in 0.02 A slices (sp4)",
+                lambda seed: generator.batch47(2 + seed)),
+}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            pass
+    return {}
+
+
+def fp64_gemm_peak(device: int) -> float | None:
+    """cuBLAS DGEMM 8192^3 throughput (TFLOP/s), the FP64 tensor-core reference."""
+    try:
+        import torch
+        torch.cuda.set_device(device)
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        torch.cuda.empty_cache()
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    except Exception:
+        return None
+
+
+def prepare_inputs(workload: str, seed: int, workdir: Path):
+    desc, make = WORKLOADS[workload]
+    s = make(seed)
+    s.write(workdir)
+    # bulk boundary records: non-reflecting bulk (f = 0); the surface-solve work is
+    # independent of the record values
+    bulkfile.write_bulkp(s, workdir / "bulkP.b")
+    return s, desc
+
+
+def cpu_baseline(workdir: Path, s, nangles: int, max_seconds: float = 25.0) -> dict:
+    """The oracle on the host cores: all threads, one angle per thread, the first
+    L slices of the workload (L sized for ~max_seconds), scaled to full solves."""
+    from oracle import oracle as O
+    O.build()
+    cores = O.set_threads(os.cpu_count())
+    nang = min(nangles, cores)
+    # calibrate on 2 slices, then size the sample
+    O.set_max_slices(2)
+    S = O.Surface(workdir / "bulkP.b", workdir / "surf.txt", s.surface_dz, s.int_method)
+    t0 = time.perf_counter()
+    S.solve(0, nang)
+    t_cal = time.perf_counter() - t0
+    S.close()
+    L = max(2, min(2000, int(2 * max_seconds / max(t_cal, 1e-3))))
+    O.set_max_slices(L)
+    S = O.Surface(workdir / "bulkP.b", workdir / "surf.txt", s.surface_dz, s.int_method)
+    L = S.ns
+    t0 = time.perf_counter()
+    S.solve(0, nang)
+    t = time.perf_counter() - t0
+    S.close()
+    O.set_max_slices(0)
+    return {"seconds": t, "angles": nang, "slices": L, "cores": cores}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dense521", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="auto", choices=["auto", "split", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_env()
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+
+    workdir = Path(tempfile.mkdtemp(prefix=f"trhepd_bench_r{rank}_"))
+    s, desc = prepare_inputs(args.workload, rank, workdir)
+
+    if args.impl == "reference":
+        if rank == 0:
+            b = cpu_baseline(workdir, s, 61)
+            S_ns = surface_slices(workdir, s)
+            per_angle = b["seconds"] * S_ns / b["slices"] / b["angles"]  # thread-seconds
+            value = b["angles"] / (b["seconds"] * S_ns / b["slices"])
+            line = {"impl": "reference", "metric": METRIC, "value": value,
+                    "unit": "angle-solves/s", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "dtype": "f64", "data": "synthetic",
+                    "config": {"workload": desc},
+                    "cpu_baseline": {"value": value, "unit": "angle-solves/s",
+                                     "cores": b["cores"], "kind": "port",
+                                     "sample": f"{b['angles']} angles x first {b['slices']} of "
+                                               f"{S_ns} slices, scaled by slice count"},
+                    "e2e": {"value": value, "unit": "angle-solves/s",
+                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                    "seconds_per_angle_solve_1core": per_angle}
+            print(json.dumps(line), flush=True)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+
+    tbuild.build()
+    ctx = native.Context(local)
+    sp = surface.SurfaceProblem(ctx, workdir / "bulkP.b", workdir / "surf.txt", s.surface_dz,
+                                s.int_method)
+    rp = sp.resident()
+    nang, n = rp.nangles, rp.nb
+    ctx.set_option(native.OPT_RENORM_POLICY, 1)
+    prec = {"auto": native.SPLIT_BF16, "split": native.SPLIT_BF16,
+            "fp64": native.FP64}[args.precision]
+    if prec == native.SPLIT_BF16:
+        try:
+            rp.solve(prec)
+        except native.TrhepdError:
+            if args.precision == "split":
+                raise
+            prec = native.FP64  # this build has no split form: report the FP64 form
+
+    def solve_ms(p):
+        rp.solve(p)
+        return ctx.last_stats()
+
+    for _ in range(max(args.warmup, 0)):
+        solve_ms(prec)
+    clocks = Clocks(local)
+    if pg:
+        pg.barrier()
+    clocks.start()
+    t_wall = time.perf_counter()
+    total_ms, launches = 0.0, 0
+    for _ in range(args.steps):
+        st = solve_ms(prec)
+        total_ms += st["device_ms"]
+        launches += st["launches"]
+    t_wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+    max_ms = total_ms
+    if pg:
+        import torch
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        max_ms = float(t.item())
+    value = nang * args.steps * ws / (max_ms / 1e3)
+    ms_per_step = max_ms / args.steps
+    _, f2_main = rp.fetch()
+
+    # ---- roofline of the stage-product kernel (one profiled solve)
+    ctx.set_option(native.OPT_PROFILE, 1)
+    stp = solve_ms(prec)
+    ctx.set_option(native.OPT_PROFILE, 0)
+    avg_ms = stp["stage_kernel_ms"] / max(stp["stage_products"], 1)
+    flops_per_launch = 8.0 * nang * n ** 3  # complex N x N x N product per angle
+    achieved = flops_per_launch / (avg_ms * 1e-3) / 1e12
+    peaks = measured_peaks()
+    if prec == native.SPLIT_BF16:
+        peak = peaks.get("bf16_tflops_sustained") or 1400.0
+        peak_src = ("MEASURED_PEAKS.json bf16_tflops_sustained" if peaks else
+                    "fallback 1.4 PFLOP/s sustained")
+    else:
+        peak = fp64_gemm_peak(local) if rank == 0 else None
+        peak_src = "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor peak)"
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if peak else None, "traffic": None,
+            "kernel": "stage product (split BF16 tcgen05)" if prec == native.SPLIT_BF16
+            else "k_stage_gemm_f64 (FP64 DMMA)",
+            "peak_source": peak_src, "avg_launch_ms": avg_ms,
+            "flops_per_launch": flops_per_launch,
+            "note": "algorithmic FP64-equivalent flops 8*nangles*N^3 per stage product"}
+
+    # ---- FP64 comparison
+    fp64 = None
+    if prec == native.SPLIT_BF16 and not args.no_fp64:
+        solve_ms(native.FP64)
+        st = solve_ms(native.FP64)
+        _, f2_64 = rp.fetch()
+        rowmax = np.maximum(np.abs(f2_64).max(axis=1, keepdims=True), 1e-300)
+        d = np.abs(f2_main - f2_64)
+        big = np.abs(f2_64) >= 1e-3 * rowmax
+        fp64 = {"value": nang / (st["device_ms"] / 1e3), "ms_per_step": st["device_ms"],
+                "split_speedup": (st["device_ms"] / ms_per_step),
+                "split_max_err_vs_rowmax": float((d / rowmax).max()),
+                "split_max_rel_err_spots_ge_1e-3_rowmax": float((d / np.where(big, np.abs(f2_64), np.inf)).max())}
+
+    # ---- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        h2d = h2d_bytes(sp, rp)
+        t0 = time.perf_counter()
+        ang, f2 = sp.srfref(prec)
+        first = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for _ in range(max(1, args.steps // 2)):
+            sp.srfref(prec)
+        e_s = (time.perf_counter() - t0) / max(1, args.steps // 2)
+        e2e = {"value": nang * ws / e_s, "unit": "angle-solves/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": int(f2.nbytes), "seconds_per_step": e_s,
+               "first_call_seconds": first}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        b = cpu_baseline(workdir, s, nang)
+        ns = rp.ns
+        cpu_value = b["angles"] / (b["seconds"] * ns / b["slices"])
+        cpu = {"value": cpu_value, "unit": "angle-solves/s", "cores": b["cores"], "kind": "port",
+               "sample": f"{b['angles']} angles x first {b['slices']} of {ns} slices on "
+                         f"{b['cores']} threads, scaled by slice count"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "angle-solves/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "bf16x4-split/f64" if prec == native.SPLIT_BF16 else "f64",
+                "data": "synthetic",
+                "config": {"workload": desc, "nb": n, "nangles": nang, "slices": rp.ns,
+                           "precision": "split-bf16" if prec == native.SPLIT_BF16 else "fp64",
+                           "renormalisation": "growth bound ln(1e3)",
+                           "bulk_boundary": "non-reflecting bulk records (f = 0)",
+                           "l2": "inputs larger than L2 (state + stage table > 1 GB)",
+                           "parallelism": f"replicas x{ws}"},
+                "roofline": roof, "fp64": fp64, "e2e": e2e, "cpu_baseline": cpu,
+                "gpu_launches": launches, "clocks": clk, "wall_seconds_timed": t_wall}
+        print(json.dumps(line), flush=True)
+    rp.close()
+    sp.close()
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def surface_slices(workdir: Path, s) -> int:
+    from oracle import oracle as O
+    S = O.Surface(workdir / "bulkP.b", workdir / "surf.txt", s.surface_dz, s.int_method)
+    ns = S.ns
+    S.close()
+    return ns
+
+
+def h2d_bytes(sp, rp) -> int:
+    """Bytes trhepd_srfref copies host->device per call: the mod_scpot3 arrays, the
+    stage depths, the beam-pair map and the per-angle gammas, energies and bulk f."""
+    p = sp.pot
+    natm = p.natms + p.natmb
+    b = 8 * (p.nv * 6 * p.nelm + 6 * p.nelm + p.nelm + p.nv)        # asf, b, dchg, Ghk
+    b += 8 * 2 * (p.natms + 2 * p.natmb) + 4 * (p.natms + 2 * p.natmb)  # z, ocr, ielm per part
+    b += 16 * (p.nv * p.natms + 2 * p.nvb * p.natmb)                 # st0, st1, st2
+    b += 8 * rp.ncol + 4 * rp.nb * rp.nb                             # depths, pair map
+    ld = -(-rp.nb // 16) * 16
+    b += rp.nangles * (16 * rp.nb + 16 * ld + 16 * rp.nb * rp.nb + 8)  # gam, D, F, w
+    del natm
+    return int(b)
+
+
+if __name__ == "__main__":
+    main()

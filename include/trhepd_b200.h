@@ -43,7 +43,8 @@ enum trhepd_option {
   TRHEPD_OPT_RENORM_POLICY = 1, /* 0: Gershgorin test > 1e3 per angle and slice (reference)
                                    1: growth bound, uniform schedule (see DESIGN) */
   TRHEPD_OPT_RENORM_TAU = 2,    /* growth bound ln(cond) between renormalisations (policy 1) */
-  TRHEPD_OPT_SPLIT_SLICES = 3   /* BF16 slices per operand in the split form (3..5) */
+  TRHEPD_OPT_SPLIT_SLICES = 3,  /* BF16 slices per operand in the split form (3..5) */
+  TRHEPD_OPT_PROFILE = 4        /* nonzero: time every stage-product launch with CUDA events */
 };
 
 typedef struct trhepd_context trhepd_context;
@@ -53,7 +54,9 @@ void trhepd_destroy(trhepd_context* ctx);
 const char* trhepd_last_error(const trhepd_context* ctx);
 int trhepd_set_option(trhepd_context* ctx, int option, double value);
 /* counters of the last solve: out[0] renormalisations, out[1] stage products,
-   out[2] device milliseconds of the solve, out[3] stage columns */
+   out[2] device milliseconds of the solve, out[3] stage columns, out[4] summed
+   device milliseconds of the stage-product kernels (TRHEPD_OPT_PROFILE only),
+   out[5] kernels launched, out[6] of which renormalisation kernels */
 int trhepd_last_stats(const trhepd_context* ctx, double* out, int n);
 
 /*
@@ -141,6 +144,23 @@ int trhepd_surf_load(trhepd_context* ctx, const char* bulkp, const char* surf, d
 void trhepd_surf_free(trhepd_surface_inputs* in);
 int trhepd_surf_views(const trhepd_surface_inputs* in, trhepd_pot_state* pot,
                       trhepd_srfref_args* args);
+
+/*
+ * Device-resident form of one srfref call, for callers that solve the same
+ * structure repeatedly (structure refinement, serving, benchmarking): create
+ * uploads the inputs and builds the stage tables in device memory once; solve
+ * integrates every angle reading device memory only and leaves the intensities
+ * on the device; fetch copies them (and the printed angles) to the host.
+ * trhepd_srfref is create + solve + fetch + destroy.
+ * info: out[0..5] = nb, nangles, ns, nv, stage columns, device bytes held.
+ */
+typedef struct trhepd_problem trhepd_problem;
+int trhepd_problem_create(trhepd_context* ctx, const trhepd_pot_state* pot,
+                          const trhepd_srfref_args* args, trhepd_problem** out);
+int trhepd_problem_solve(trhepd_context* ctx, trhepd_problem* pb, int precision);
+int trhepd_problem_fetch(trhepd_context* ctx, trhepd_problem* pb, double* f2, double* angle_deg);
+int trhepd_problem_info(const trhepd_problem* pb, int64_t* out, int n);
+void trhepd_problem_destroy(trhepd_problem* pb);
 
 /*
  * surf.exe for the first domain (surfm.f90:6-97 + surfio.f90:60-381): reads

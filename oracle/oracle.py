@@ -51,6 +51,7 @@ def lib():
         L.oracle_bulk_run.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                       ctypes.c_int]
         L.oracle_set_threads.argtypes = [ctypes.c_int]
+        L.oracle_set_max_slices.argtypes = [ctypes.c_int]
         _lib = L
     return _lib
 
@@ -125,3 +126,8 @@ def bulk_run(bulk_txt, out_path) -> None:
     rc = lib().oracle_bulk_run(str(bulk_txt).encode(), str(out_path).encode(), err, 512)
     if rc:
         raise RuntimeError("oracle bulk: " + err.value.decode())
+
+
+def set_max_slices(n: int) -> None:
+    """Integrate only the first n slices (0 = all); for bounded timing samples."""
+    lib().oracle_set_max_slices(int(n))

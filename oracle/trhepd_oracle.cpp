@@ -2063,6 +2063,10 @@ static void bulk_run(const std::string& bulk_txt, const std::string& out_path) {
 // =============================================================================
 using namespace oracle;
 
+// Timing-sample knob: > 0 integrates only the first L slices (same dz), so a CPU
+// baseline can time a bounded, representative share of a long solve.
+static int g_max_slices = 0;
+
 struct OracleSurface {
   SurfModel S;
   int method = 5;
@@ -2090,6 +2094,7 @@ int oracle_plane_group_images(int nsg, int ma, int mb, int na, int nb, double x,
   return ndeg;
 }
 void oracle_set_split_slices(int s) { g_split_slices = s; }
+void oracle_set_max_slices(int l) { g_max_slices = l; }
 void oracle_set_split_diag(int d) { g_split_diag = d; }
 
 void oracle_set_threads(int n) {
@@ -2105,6 +2110,7 @@ void* oracle_surface_open(const char* bulkp, const char* surf, double dz2, int m
     auto* h = new OracleSurface();
     h->method = method;
     load_surface(bulkp, surf, dz2, h->S);
+    if (g_max_slices > 0 && h->S.ns > g_max_slices) h->S.ns = g_max_slices;
     h->ncol = build_potential(h->S, h->S.dom[0], method, h->v, h->vi);
     return h;
   } catch (const std::exception& e) {

@@ -1,0 +1,74 @@
+"""Split-precision form (BF16 slices on tcgen05, FP64 elsewhere) against the
+plain FP64 form and the oracle.  Target: every spot within 1e-6 of its row
+maximum and within 1e-5 relative on spots >= 1e-3 of the row maximum, with 4
+slices.  (At 2000 chained slices the FP64 result itself moves by ~4e-7 relative
+on weak spots when only the renormalisation points change, so weaker spots are
+bounded relative to the row maximum.)"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import spot_errors
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from trhepd_opt_b200 import build, native
+    build.build()
+    c = native.Context(0)
+    yield c
+    c.close()
+
+
+def _resident(ctx, tmp_path, s):
+    from trhepd_opt_b200 import bulkfile, surface
+    s.write(tmp_path)
+    bulkfile.write_bulkp(s, tmp_path / "bulkP.b")
+    sp = surface.SurfaceProblem(ctx, tmp_path / "bulkP.b", tmp_path / "surf.txt", s.surface_dz,
+                                s.int_method)
+    return sp, sp.resident()
+
+
+@pytest.mark.parametrize("case", ["small23", "dense95"])
+def test_split_matches_fp64(ctx, tmp_path, case):
+    from trhepd_opt_b200 import generator, native
+    s = generator.small23() if case == "small23" else generator.dense(95, n_angles=8, region=6.0)
+    sp, rp = _resident(ctx, tmp_path, s)
+    rp.solve(native.FP64)
+    _, ref = rp.fetch()
+    ctx.set_option(native.OPT_SPLIT_SLICES, 4)
+    rp.solve(native.SPLIT_BF16)
+    _, got = rp.fetch()
+    abs_err, _ = spot_errors(got, ref)
+    _, rel_big = spot_errors(got, ref, floor=1e-3)
+    assert abs_err <= 1e-6, abs_err
+    assert rel_big <= 1e-5, rel_big
+
+
+def test_split_against_reference_output(ctx, golden):
+    """The split form on the reference's own N=47 case at 0.22 A slices."""
+    from trhepd_opt_b200 import native
+    d = golden / "test47"
+    ref = np.load(d / "perf-5-0.22.npz")
+    ctx.set_option(native.OPT_SPLIT_SLICES, 4)
+    f2, _ = ctx.surf_run(d / "bulkP.b", d / "surf.txt", 0.22, 5, native.SPLIT_BF16)
+    abs_err, _ = spot_errors(f2, ref["f2"])
+    assert abs_err <= 1e-6, abs_err
+
+
+def test_more_slices_is_more_accurate(ctx, tmp_path):
+    from trhepd_opt_b200 import generator, native
+    sp, rp = _resident(ctx, tmp_path, generator.small23())
+    rp.solve(native.FP64)
+    _, ref = rp.fetch()
+    errs = []
+    for S in (3, 4, 5):
+        ctx.set_option(native.OPT_SPLIT_SLICES, S)
+        rp.solve(native.SPLIT_BF16)
+        _, got = rp.fetch()
+        errs.append(spot_errors(got, ref)[0])
+    ctx.set_option(native.OPT_SPLIT_SLICES, 4)
+    assert errs[0] > errs[1] > errs[2], errs

@@ -47,7 +47,8 @@ void launch_structure_factor(const double* gh, const double* gk, int nv, const d
 
 // K4: shared stage matrix V (kpad x ld, row-major) from table column `col`.
 // pair[k * n + j] = 0-based table index of beam pair (k, j) (diagonal: 0).
-// drop_diag: zero the diagonal (the split path applies it in FP64).
+// drop_diag: zero the diagonal (the split path applies it in FP64) and store its
+// value at V[kpad * ld]; V must hold (kpad + 1) * ld elements.
 void launch_gather_stage(const TableEntry* table_col, const int* pair, int n, int kpad, int ld,
                          bool drop_diag, cd* V, cudaStream_t st);
 

@@ -159,6 +159,8 @@ __global__ void k_gather_stage(const TableEntry* __restrict__ tc, const int* __r
     }
   }
   V[(size_t)k * ld + j] = v;
+  // with the diagonal dropped, its (constant) value is kept in the slot after the matrix
+  if (drop_diag && k == 0 && j == 0) V[(size_t)kpad * ld] = -conj(tc[0].u);
 }
 
 void launch_gather_stage(const TableEntry* table_col, const int* pair, int n, int kpad, int ld,

@@ -119,7 +119,9 @@ struct trhepd_context {
   int renorm_policy = 0;
   double renorm_tau = std::log(1e3);
   int split_slices = 4;
-  double stats[4] = {0, 0, 0, 0};
+  int profile = 0;               // 1: time every stage-product launch with events
+  double stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  std::vector<cudaEvent_t> evpool;
   // device buffers (grown on demand, reused across calls)
   DevBuf asf, b, dchg, ghk, z[3], ocr[3], ielm[3], st[3], depth, table, pair;
   DevBuf Q0, Q1, P, V, D, gam, F, flags, dval, gj, f2, wnsga2, status, split;
@@ -135,7 +137,7 @@ int fail(trhepd_context* ctx, int code, const std::string& msg) {
 
 // Upload mod_scpot3 and build the stage table on the device.
 void build_table(trhepd_context* C, const trhepd_pot_state& pot, const std::vector<double>& depth,
-                 TableEntry** table_out) {
+                 DevBuf& out, TableEntry** table_out) {
   cudaStream_t st = C->stream;
   const int nv = pot.nv, nelm = pot.nelm;
   const int natm = pot.natmb + pot.natms;
@@ -185,7 +187,7 @@ void build_table(trhepd_context* C, const trhepd_pot_state& pot, const std::vect
   }
   const double* dd = upload(C->depth, depth, st);
   int ncol = (int)depth.size();
-  TableEntry* table = (TableEntry*)C->table.ensure((size_t)ncol * nv * sizeof(TableEntry));
+  TableEntry* table = (TableEntry*)out.ensure((size_t)ncol * nv * sizeof(TableEntry));
   launch_potential_table(in, dd, ncol, table, st);
   CK(cudaGetLastError());
   *table_out = table;
@@ -201,22 +203,49 @@ struct SolveArgs {
   double wn, ghx, ghy, gky, azi, daz, gi, dg;
   int naz, ng, int_method;
   const double* t1;
-  int precision;
 };
 
-// The batched solve behind trhepd_srfref.
-void solve(trhepd_context* C, const SolveArgs& A, double* f2_out, double* angle_out) {
+}  // namespace
+
+// Device-resident problem: stage table, beam-pair map, bulk boundary, gammas.
+// Solving it reads only device memory; the result stays on the device until
+// fetched.
+struct trhepd_problem {
+  int n = 0, ns = 0, nv = 0, nang = 0, ld = 0, nb0 = 0, int_method = 5;
+  Integrator I{6, nullptr};
+  double dz = 0, kappa_max = 0;
+  int ncol = 0;
+  DevBuf table, pair, gam, D, F, wnsga2, f2;
+  std::vector<double> angle_deg;
+  size_t bytes() const {
+    return table.n + pair.n + gam.n + D.n + F.n + wnsga2.n + f2.n;
+  }
+  void release() {
+    for (DevBuf* b : {&table, &pair, &gam, &D, &F, &wnsga2, &f2}) b->release();
+  }
+};
+
+namespace {
+
+// Upload inputs, build the stage table (K2/K3 outputs) and the per-angle data.
+void prepare(trhepd_context* C, const SolveArgs& A, trhepd_problem& Pb) {
   const int n = A.nb, ns = A.ns;
   if (n < 1 || ns < 1) throw std::invalid_argument("nb and ns must be >= 1");
   if (n > kMaxBeams) throw std::invalid_argument("nb exceeds the GPU path limit");
-  const Integrator I = integrator_for(A.int_method);
-  const std::vector<double> depth = stage_depths(I, ns, A.dz);
+  Pb.I = integrator_for(A.int_method);
+  Pb.int_method = A.int_method;
+  const std::vector<double> depth = stage_depths(Pb.I, ns, A.dz);
   cudaStream_t st = C->stream;
   TableEntry* table = nullptr;
-  build_table(C, *A.pot, depth, &table);
+  build_table(C, *A.pot, depth, Pb.table, &table);
   const int nv = A.pot->nv;
+  Pb.n = n;
+  Pb.ns = ns;
+  Pb.nv = nv;
+  Pb.dz = A.dz;
+  Pb.ncol = (int)depth.size();
 
-  // ---- beam-pair map for the gather: pair[k*n+j] = iv(max,min) - 1
+  // beam-pair map for the gather: pair[k*n+j] = iv(max,min) - 1
   std::vector<int> pair((size_t)n * n, 0);
   for (int k = 0; k < n; ++k)
     for (int j = 0; j < n; ++j) {
@@ -226,24 +255,28 @@ void solve(trhepd_context* C, const SolveArgs& A, double* f2_out, double* angle_
       if (e < 1 || e > nv) throw std::invalid_argument("iv entry out of range");
       pair[(size_t)k * n + j] = e - 1;
     }
-  const int* d_pair = upload(C->pair, pair, st);
+  upload(Pb.pair, pair, st);
 
-  // ---- angle schedule (surflf.f90:43-92)
+  // angle schedule (surflf.f90:43-92)
   const bool ng_outer = A.ng > A.naz;
   const int nrep1 = ng_outer ? A.naz : A.ng, nrep2 = ng_outer ? A.ng : A.naz;
   const int nang = nrep1 * nrep2;
-  const int ld = round_up(n, 16), kpad = ld;
+  const int ld = round_up(n, 16);
+  Pb.nang = nang;
+  Pb.ld = ld;
   std::vector<cd> gam((size_t)nang * n), Dm((size_t)nang * ld, cd{0, 0}), F((size_t)nang * n * n);
   std::vector<double> wnsga2(nang);
+  Pb.angle_deg.assign(nang, 0.0);
   size_t per = 0;
-  for (int l = 0; l < A.ngr; ++l) per += (size_t)A.nbg[l] * A.nbg[l];
-  {
-    int sum = 0;
-    for (int l = 0; l < A.ngr; ++l) sum += A.nbg[l];
-    if (sum != n) throw std::invalid_argument("sum(nbg) != nb");
-    for (int i = 0; i < n; ++i)
-      if (A.iord[i] < 1 || A.iord[i] > n) throw std::invalid_argument("iord out of range");
+  int sum = 0;
+  for (int l = 0; l < A.ngr; ++l) {
+    if (A.nbg[l] < 1) throw std::invalid_argument("nbg entries must be >= 1");
+    per += (size_t)A.nbg[l] * A.nbg[l];
+    sum += A.nbg[l];
   }
+  if (sum != n) throw std::invalid_argument("sum(nbg) != nb");
+  for (int i = 0; i < n; ++i)
+    if (A.iord[i] < 1 || A.iord[i] > n) throw std::invalid_argument("iord out of range");
   double kappa_max = 0.0;
   for (int t = 0; t < nang; ++t) {
     int irep1 = t / nrep2, irep2 = t % nrep2;
@@ -268,11 +301,10 @@ void solve(trhepd_context* C, const SolveArgs& A, double* f2_out, double* angle_
       Dm[(size_t)t * ld + i] = cd{-g2.x, g2.y};  // -conj(g^2)
       if (s < 0) kappa_max = std::max(kappa_max, std::sqrt(-s));
     }
-    if (angle_out) angle_out[t] = (ng_outer ? ga : az) * 180.0 / 3.141592654;
+    Pb.angle_deg[t] = (ng_outer ? ga : az) * 180.0 / 3.141592654;
     // bulk f permuted by iord (surflf.f90:105-115); F row-major (i, j)
     const double* rec = A.t1 + 2 * per * t;
     cd* Ft = F.data() + (size_t)t * n * n;
-    std::fill(Ft, Ft + (size_t)n * n, cd{0, 0});
     int ib1 = 0;
     size_t o = 0;
     for (int l = 0; l < A.ngr; ++l) {
@@ -285,50 +317,72 @@ void solve(trhepd_context* C, const SolveArgs& A, double* f2_out, double* angle_
       ib1 += m;
     }
   }
-  int nb0 = 0;
+  Pb.kappa_max = kappa_max;
+  Pb.nb0 = 0;
   for (int i = 0; i < n; ++i)
-    if (A.ih[i] == 0 && A.ik[i] == 0) nb0 = i;
+    if (A.ih[i] == 0 && A.ik[i] == 0) Pb.nb0 = i;
+  upload(Pb.gam, gam, st);
+  upload(Pb.D, Dm, st);
+  upload(Pb.F, F, st);
+  upload(Pb.wnsga2, wnsga2, st);
+  Pb.f2.ensure((size_t)nang * n * sizeof(double));
+}
 
-  const cd* d_gam = upload(C->gam, gam, st);
-  const cd* d_D = upload(C->D, Dm, st);
-  const cd* d_F = upload(C->F, F, st);
-  const double* d_w = upload(C->wnsga2, wnsga2, st);
+// Integrate every angle of a resident problem (surf_prkn.f90:278-330 batched over
+// angles); intensities land in Pb.f2 on the device.  Device time of the whole
+// sequence is recorded with events on the context stream.
+void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
+  const int n = Pb.n, ns = Pb.ns, nv = Pb.nv, nang = Pb.nang, ld = Pb.ld, kpad = ld;
+  const Integrator& I = Pb.I;
+  cudaStream_t st = C->stream;
+  const TableEntry* table = Pb.table.as<TableEntry>();
+  const int* d_pair = Pb.pair.as<int>();
+  const cd* d_gam = Pb.gam.as<cd>();
+  const cd* d_D = Pb.D.as<cd>();
   const size_t sbytes = (size_t)nang * n * ld * sizeof(cd);
   cd* Q = (cd*)C->Q0.ensure(sbytes);
   cd* Qn = (cd*)C->Q1.ensure(sbytes);
   cd* P = (cd*)C->P.ensure(sbytes);
-  CK(cudaMemsetAsync(Q, 0, sbytes, st));
-  CK(cudaMemsetAsync(Qn, 0, sbytes, st));
-  CK(cudaMemsetAsync(P, 0, sbytes, st));
-  cd* V = (cd*)C->V.ensure((size_t)kpad * ld * sizeof(cd));
+  cd* V = (cd*)C->V.ensure((size_t)(kpad + 1) * ld * sizeof(cd));
   int* flags = (int*)C->flags.ensure(std::max(nang, 4) * sizeof(int));
   double* dval = (double*)C->dval.ensure(std::max(nang, 4) * sizeof(double));
   void* gjs = C->gj.ensure(gj_scratch_bytes(nang, n));
   unsigned* status = (unsigned*)C->status.ensure(16);
-  CK(cudaMemsetAsync(status, 0, 16, st));
-  const bool split = A.precision == TRHEPD_SPLIT_BF16;
+  const bool split = precision == TRHEPD_SPLIT_BF16;
   SplitWorkspace sw{};
-  if (split) {
+  if (split)
     sw = split_workspace_carve(C->split.ensure(split_workspace_bytes(nang, n, C->split_slices)),
-                               nang, n, C->split_slices);
-  }
+                               nang, n, C->split_slices, status, st);
 
   CK(cudaEventRecord(C->ev0, st));
-  // ---- invstransh: Q = I + F^H, P = I - F^H; P <- Q^{-1} P; P <- i P conj(G); Q = I
-  launch_invstransh_build(d_F, Q, P, nang, n, ld, st);
+  CK(cudaMemsetAsync(status, 0, 16, st));
+  CK(cudaMemsetAsync(Q, 0, sbytes, st));
+  CK(cudaMemsetAsync(Qn, 0, sbytes, st));
+  CK(cudaMemsetAsync(P, 0, sbytes, st));
+  // invstransh: Q = I + F^H, P = I - F^H; P <- Q^{-1} P; P <- i P conj(G); Q = I
+  launch_invstransh_build(Pb.F.as<cd>(), Q, P, nang, n, ld, st);
   launch_gauss_jordan(Q, P, nullptr, nang, n, ld, gjs, status, st);
   launch_invstransh_finish(P, d_gam, nang, n, ld, st);
   launch_set_identity(Q, nullptr, nang, n, ld, st);
 
-  // ---- renormalisation schedule
-  const bool every_slice = (n == 1 && A.int_method == 6);  // hp_int_spa1d renormalises each slice
+  // renormalisation schedule
+  const bool every_slice = (n == 1 && Pb.int_method == 6);  // hp_int_spa1d renormalises each slice
   int interval = 1;
   if (C->renorm_policy == 1 && !every_slice) {
-    double kap = kappa_max + 1.0;
-    interval = std::max(1, (int)std::floor(C->renorm_tau / (kap * A.dz)));
+    double kap = Pb.kappa_max + 1.0;
+    interval = std::max(1, (int)std::floor(C->renorm_tau / (kap * Pb.dz)));
   }
-  long renorms = 0, products = 0;
-  const double dz = A.dz;
+  long renorms = 0, products = 0, launches = 0, gj_launches = 0;
+  const double dz = Pb.dz;
+  const int nprod_max = I.s * ns;
+  if (C->profile && (int)C->evpool.size() < 2 * nprod_max) {
+    while ((int)C->evpool.size() < 2 * nprod_max) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      C->evpool.push_back(e);
+    }
+  }
+  const int gj_per = 2 * ceil_div(n, 16);
   for (int l = 1; l <= ns; ++l) {
     for (int k = 1; k <= I.s; ++k) {
       const int col = I.s * (l - 1) + k - 1;
@@ -337,18 +391,22 @@ void solve(trhepd_context* C, const SolveArgs& A, double* f2_out, double* angle_
       if (l == 1 && k == 1) {  // Q = I: elementwise stage
         launch_gather_stage(tc, d_pair, n, kpad, ld, false, V, st);
         launch_stage_identity(Q, P, V, d_D, nang, n, ld, I.bab[0] * dz, ca, st);
+        launches += 2;
         continue;
       }
       // k == 1, l > 1 merges the end-of-slice half kick of slice l-1 (psave) with the
       // first kick of slice l: both use the same stage column, so cb = 2 b1.
       const double cb = (k == 1) ? 2.0 * I.bab[0] * dz : I.bab[2 * k - 2] * dz;
+      launch_gather_stage(tc, d_pair, n, kpad, ld, split, V, st);
+      if (C->profile) CK(cudaEventRecord(C->evpool[2 * products], st));
       if (split) {
-        launch_gather_stage(tc, d_pair, n, kpad, ld, true, V, st);
-        split_stage(sw, Q, P, Qn, V, d_D, nang, n, ld, cb, ca, C->split_slices, st);
+        launches += split_stage(sw, Q, P, Qn, V, d_D, nang, n, ld, cb, ca, C->split_slices, st);
       } else {
-        launch_gather_stage(tc, d_pair, n, kpad, ld, false, V, st);
         launch_stage_gemm_f64(Q, P, Qn, V, d_D, nang, n, ld, kpad, cb, ca, st);
+        launches += 1;
       }
+      if (C->profile) CK(cudaEventRecord(C->evpool[2 * products + 1], st));
+      launches += 1;  // gather
       std::swap(Q, Qn);
       ++products;
     }
@@ -359,10 +417,14 @@ void solve(trhepd_context* C, const SolveArgs& A, double* f2_out, double* angle_
       launch_cond_est(Q, nang, n, ld, last ? 1 : 0, flags, dval, st);
       launch_gauss_jordan(Q, P, flags, nang, n, ld, gjs, status, st);
       launch_set_identity(Q, flags, nang, n, ld, st);
-      if (!last) ++renorms;  // upper bound; exact per-angle counts stay on the device
+      launches += 2 + gj_per;
+      gj_launches += gj_per;
+      if (!last) ++renorms;  // upper bound; per-angle decisions stay on the device
     } else if (last || every_slice || (l % interval) == 0) {
       launch_gauss_jordan(Q, P, nullptr, nang, n, ld, gjs, status, st);
       launch_set_identity(Q, nullptr, nang, n, ld, st);
+      launches += 1 + gj_per;
+      gj_launches += gj_per;
       if (!last) ++renorms;
     }
   }
@@ -372,27 +434,61 @@ void solve(trhepd_context* C, const SolveArgs& A, double* f2_out, double* angle_
     launch_gather_stage(tc, d_pair, n, kpad, ld, false, V, st);
     launch_stage_identity(Q, P, V, d_D, nang, n, ld, I.bab[0] * dz, 0.0, st);
   }
-  // ---- stransh and intensities
+  // stransh and intensities
   launch_stransh_build(Q, P, d_gam, nang, n, ld, st);
   launch_gauss_jordan(Q, P, nullptr, nang, n, ld, gjs, status, st);
   launch_check_finite(P, (size_t)nang * n * ld, status, st);
-  double* d_f2 = (double*)C->f2.ensure((size_t)nang * n * sizeof(double));
-  launch_intensities(P, d_gam, d_w, nang, n, ld, nb0, d_f2, st);
+  launch_intensities(P, d_gam, Pb.wnsga2.as<double>(), nang, n, ld, Pb.nb0, Pb.f2.as<double>(),
+                     st);
   CK(cudaEventRecord(C->ev1, st));
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(f2_out, d_f2, (size_t)nang * n * sizeof(double), cudaMemcpyDeviceToHost, st));
   unsigned h_status[4];
   CK(cudaMemcpyAsync(h_status, status, 16, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   float ms = 0;
   cudaEventElapsedTime(&ms, C->ev0, C->ev1);
+  launches += 4 + gj_per + 2 + 2 + 3 + gj_per + 2;  // boundary transforms, final kick, intensities
+  double prod_ms = 0.0;
+  if (C->profile)
+    for (long p = 0; p < products; ++p) {
+      float e = 0;
+      cudaEventElapsedTime(&e, C->evpool[2 * p], C->evpool[2 * p + 1]);
+      prod_ms += e;
+    }
   C->stats[0] = (double)renorms;
   C->stats[1] = (double)products;
   C->stats[2] = ms;
-  C->stats[3] = (double)depth.size();
+  C->stats[3] = (double)Pb.ncol;
+  C->stats[4] = prod_ms;
+  C->stats[5] = (double)launches;
+  C->stats[6] = (double)gj_launches;
   if (h_status[0] & kStatusTimeout) throw CudaError("device wait timed out", TRHEPD_ETIMEOUT);
   if (h_status[0] & (kStatusNonFinite | kStatusZeroPivot))
     throw CudaError("non-finite value or zero pivot in the surface solve", TRHEPD_ENONFINITE);
+}
+
+void fetch(trhepd_context* C, trhepd_problem& Pb, double* f2, double* angle_deg) {
+  if (f2)
+    CK(cudaMemcpyAsync(f2, Pb.f2.p, (size_t)Pb.nang * Pb.n * sizeof(double),
+                       cudaMemcpyDeviceToHost, C->stream));
+  CK(cudaStreamSynchronize(C->stream));
+  if (angle_deg) std::copy(Pb.angle_deg.begin(), Pb.angle_deg.end(), angle_deg);
+}
+
+// The end-to-end solve behind trhepd_srfref: prepare, run, fetch, release.
+void solve(trhepd_context* C, const SolveArgs& A, int precision, double* f2_out,
+           double* angle_out) {
+  trhepd_problem Pb;
+  try {
+    prepare(C, A, Pb);
+    run(C, Pb, precision);
+    fetch(C, Pb, f2_out, angle_out);
+  } catch (...) {
+    cudaStreamSynchronize(C->stream);
+    Pb.release();
+    throw;
+  }
+  Pb.release();
 }
 
 // Structure factors of SurfaceInputs on the device.
@@ -557,6 +653,7 @@ void trhepd_destroy(trhepd_context* c) {
     c->ielm[p].release();
     c->st[p].release();
   }
+  for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
   cudaStreamDestroy(c->stream);
@@ -580,13 +677,16 @@ int trhepd_set_option(trhepd_context* c, int option, double value) {
       if (value < 3 || value > 5) return fail(c, TRHEPD_EINVAL, "split slices must be 3..5");
       c->split_slices = (int)value;
       return TRHEPD_OK;
+    case TRHEPD_OPT_PROFILE:
+      c->profile = value != 0.0;
+      return TRHEPD_OK;
   }
   return fail(c, TRHEPD_EINVAL, "unknown option");
 }
 
 int trhepd_last_stats(const trhepd_context* c, double* out, int n) {
   if (!c || !out) return TRHEPD_EINVAL;
-  for (int i = 0; i < n && i < 4; ++i) out[i] = c->stats[i];
+  for (int i = 0; i < n && i < 8; ++i) out[i] = c->stats[i];
   return TRHEPD_OK;
 }
 
@@ -626,7 +726,7 @@ int trhepd_potential_table(trhepd_context* ctx, const trhepd_pot_state* pot, int
     Integrator I = integrator_for(int_method);
     std::vector<double> depth = stage_depths(I, ns, dz);
     TableEntry* table = nullptr;
-    build_table(ctx, *pot, depth, &table);
+    build_table(ctx, *pot, depth, ctx->table, &table);
     size_t cnt = depth.size() * (size_t)pot->nv;
     std::vector<TableEntry> h(cnt);
     CK(cudaMemcpyAsync(h.data(), table, cnt * sizeof(TableEntry), cudaMemcpyDeviceToHost,
@@ -659,9 +759,62 @@ int trhepd_srfref(trhepd_context* ctx, const trhepd_pot_state* pot, int nb, int 
     if (precision != TRHEPD_FP64 && precision != TRHEPD_SPLIT_BF16)
       throw std::invalid_argument("unknown precision form");
     SolveArgs a{pot, nb, ns, iv, dz, ngr, nbg, iord, ih, ik, wn, ghx, ghy, gky,
-                azi, daz, gi, dg, naz, ng, int_method, t1_records, precision};
-    solve(ctx, a, f2, angle_deg);
+                azi, daz, gi, dg, naz, ng, int_method, t1_records};
+    solve(ctx, a, precision, f2, angle_deg);
   });
+}
+
+int trhepd_problem_create(trhepd_context* ctx, const trhepd_pot_state* pot,
+                          const trhepd_srfref_args* a, trhepd_problem** out) {
+  if (!out) return TRHEPD_EINVAL;
+  *out = nullptr;
+  auto* pb = new trhepd_problem();
+  int rc = guarded(ctx, [&] {
+    if (!pot || !a || !a->iv || !a->nbg || !a->iord || !a->ih || !a->ik || !a->t1_records)
+      throw std::invalid_argument("null argument");
+    if (a->naz < 1 || a->ng < 1 || a->ngr < 1) throw std::invalid_argument("naz, ng, ngr >= 1");
+    SolveArgs s{pot, a->nb, a->ns, a->iv, a->dz, a->ngr, a->nbg, a->iord, a->ih, a->ik,
+                a->wn, a->ghx, a->ghy, a->gky, a->azi, a->daz, a->gi, a->dg, a->naz, a->ng,
+                a->int_method, a->t1_records};
+    prepare(ctx, s, *pb);
+    CK(cudaStreamSynchronize(ctx->stream));
+  });
+  if (rc) {
+    pb->release();
+    delete pb;
+    return rc;
+  }
+  *out = pb;
+  return TRHEPD_OK;
+}
+
+int trhepd_problem_solve(trhepd_context* ctx, trhepd_problem* pb, int precision) {
+  return guarded(ctx, [&] {
+    if (!pb) throw std::invalid_argument("null problem");
+    if (precision != TRHEPD_FP64 && precision != TRHEPD_SPLIT_BF16)
+      throw std::invalid_argument("unknown precision form");
+    run(ctx, *pb, precision);
+  });
+}
+
+int trhepd_problem_fetch(trhepd_context* ctx, trhepd_problem* pb, double* f2, double* angle_deg) {
+  return guarded(ctx, [&] {
+    if (!pb) throw std::invalid_argument("null problem");
+    fetch(ctx, *pb, f2, angle_deg);
+  });
+}
+
+int trhepd_problem_info(const trhepd_problem* pb, int64_t* out, int n) {
+  if (!pb || !out) return TRHEPD_EINVAL;
+  int64_t v[6] = {pb->n, pb->nang, pb->ns, pb->nv, pb->ncol, (int64_t)pb->bytes()};
+  for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
+  return TRHEPD_OK;
+}
+
+void trhepd_problem_destroy(trhepd_problem* pb) {
+  if (!pb) return;
+  pb->release();
+  delete pb;
 }
 
 struct trhepd_surface_inputs {
@@ -735,9 +888,8 @@ int trhepd_surf_run(trhepd_context* ctx, const char* bulkp, const char* surf, do
     std::vector<double> out((size_t)nang * S.nb), ang(nang);
     SolveArgs a{&pot, S.nb, S.ns, S.iv.data(), S.dz, S.ngr, S.nbg.data(), S.iord.data(),
                 S.ih.data(), S.ik.data(), S.wn, S.ghx, S.ghy, S.gky, S.azi, S.daz, S.gi, S.dg,
-                S.naz, S.ng, int_method, reinterpret_cast<const double*>(S.t1rec.data()),
-                precision};
-    solve(ctx, a, out.data(), ang.data());
+                S.naz, S.ng, int_method, reinterpret_cast<const double*>(S.t1rec.data())};
+    solve(ctx, a, precision, out.data(), ang.data());
     if (out_path) write_rocking_curves(out_path, S, out.data(), ang.data());
     if (f2) {
       if ((size_t)max_f2 < out.size()) throw std::invalid_argument("f2 buffer too small");

@@ -1,14 +1,537 @@
-#include <stdexcept>
+// Split-precision stage product on the 5th-generation tensor cores (sm_100a).
+//
+// The integrator stage (surf_prkn.f90:222-276, batched over angles)
+//     P += cb * Q M,   M = Voff + diag(vd + d_a),   Q <- Q + ca * P
+// is formed as
+//     Q M = Qoff Voff  +  diag(q) Voff  +  Q diag(vd + d_a)
+// where Qoff / Voff are Q and the shared potential matrix with their diagonals
+// removed and q is Q's diagonal.  The last two terms are exact FP64 work in the
+// epilogue; Qoff Voff runs on tcgen05 from BF16 slices:
+//
+//   * every row r of Qoff is scaled by a power of two 2^-e_r (row maximum), every
+//     column j of Voff by 2^-f_j, and the scaled values are cut into S signed
+//     base-256 digits d_s in [-128, 128] with rounding; slice s holds d_s * 2^-8s,
+//     so each slice is exact in BF16 and a slice pair (s, t) carries its weight;
+//   * complex is handled as a real product with interleaved components:
+//     A = [Re Q, Im Q] per column pair, B^T rows (Re-out, Im-out) per column pair;
+//   * the slice pairs with s + t < S are issued into three FP32 TMEM accumulators
+//     (s+t = 0, s+t = 1, s+t >= 2).  The first two hold integer sums well inside
+//     FP32's 24-bit exact range, so only the small third one rounds;
+//   * the epilogue combines the accumulators in FP64, rescales by 2^(e_r + f_j - 14)
+//     and performs the RKN update with the exact diagonal terms.
+//
+// Layouts: A slices [S][R][KR] and B^T slices [S][NR][KR], BF16, K-major, loaded by
+// TMA with 64-byte swizzle in 32-element k-blocks; one CTA computes 128 rows x
+// 128 real columns (64 complex); warp 0 issues TMA, warp 1 issues MMA, warps 2-5
+// drain TMEM.  All waits are bounded and report kStatusTimeout instead of hanging.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
 
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "kernels.h"
 #include "split_gemm.h"
 
 namespace trhepd {
-size_t split_workspace_bytes(int, int, int) { return 256; }
-SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices) {
-  return SplitWorkspace{base, nang, n, slices};
+namespace split {
+
+constexpr int BM = 128;               // UMMA M: stacked rows per CTA
+constexpr int NT = 128;               // UMMA N: real output columns per CTA (64 complex)
+constexpr int NC = NT / 2;            // complex columns per CTA
+constexpr int BK = 32;                // real k per pipeline stage (64-byte rows)
+constexpr int NACC = 3;
+constexpr int TMEM_COLS = 512;
+constexpr int THREADS = 192;
+constexpr int A_SLICE_BYTES = BM * BK * 2;
+constexpr int B_SLICE_BYTES = NT * BK * 2;
+constexpr int EPI_STRIDE = NC + 1;    // complex elements per staged row (odd: conflict-free)
+constexpr uint64_t kWaitNs = 2000000000ull;  // bounded waits give up after ~2 s
+
+__host__ __device__ constexpr int stages_for(int S) { return S <= 4 ? 3 : 2; }
+__host__ __device__ constexpr size_t stage_bytes(int S) {
+  return (size_t)S * (A_SLICE_BYTES + B_SLICE_BYTES);
 }
-void split_stage(const SplitWorkspace&, const cd*, cd*, cd*, const cd*, const cd*, int, int, int,
-                 double, double, int, cudaStream_t) {
-  throw std::invalid_argument("split precision form is not available in this build");
+inline size_t smem_bytes(int S) {
+  size_t pipe = stages_for(S) * stage_bytes(S);
+  size_t epi = (size_t)BM * EPI_STRIDE * sizeof(cd);
+  return 1024 + (pipe > epi ? pipe : epi);
 }
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait on phase `parity`; returns false once ~2 s have passed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t a = smem_u32(bar);
+  const uint64_t t0 = globaltimer();
+  for (uint32_t it = 0;; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((it & 1023) == 1023 && globaltimer() - t0 > kWaitNs) return false;
+  }
+}
+__device__ __forceinline__ void tma_load_3d(const CUtensorMap* map, uint64_t* bar, void* dst,
+                                            int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 64-byte swizzle, 8-row groups 512 B apart.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);       // start address
+  d |= (uint64_t)1 << 16;                       // leading byte offset (16 B units)
+  d |= (uint64_t)(512 >> 4) << 32;              // stride byte offset
+  d |= (uint64_t)1 << 46;                       // descriptor version
+  d |= (uint64_t)4 << 61;                       // SWIZZLE_64B
+  return d;
+}
+
+// Instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = NT.
+__host__ __device__ constexpr uint32_t instr_desc() {
+  return (1u << 4)                      // D format F32
+         | (1u << 7) | (1u << 10)       // A, B format BF16
+         | ((uint32_t)(NT >> 3) << 17)  // N
+         | ((uint32_t)(BM >> 4) << 24); // M
+}
+
+struct EpiArgs {
+  const cd* Q;
+  cd* P;
+  cd* Qo;
+  const cd* V;         // Voff (kpad + 1 rows, the last one holds the dropped diagonal)
+  const cd* D;         // -conj(gamma^2) per angle (nang x ld)
+  const int* erow;     // row exponents
+  const int* fcol;     // column exponents (complex columns)
+  unsigned* status;
+  int rows, n, ld, kpad, S;
+  double cb, ca;
+};
+
+// ------------------------------------------------------------ slicing kernels
+// Digits of x * 2^(7 - e): d0 = rint(y), y <- (y - d0) * 256, ...; slice s = d_s 2^-8s.
+template <int S>
+__device__ __forceinline__ void digits(double x, int e, float* out) {
+  double y = ldexp(x, 7 - e);
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    double d = rint(y);
+    out[s] = ldexpf((float)d, -8 * s);
+    y = (y - d) * 256.0;
+  }
+}
+
+// One warp per stacked row: exponent of the off-diagonal row maximum, then the
+// S interleaved (Re, Im) slices of the row.
+template <int S>
+__global__ void k_slice_rows(const cd* __restrict__ Q, int rows, int n, int ld, int kr,
+                             __nv_bfloat162* __restrict__ A, int* __restrict__ erow) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= rows) return;
+  const int r = warp, i = r % n;
+  const cd* q = Q + (size_t)r * ld;
+  double m = 0.0;
+  for (int k = lane; k < n; k += 32)
+    if (k != i) m = fmax(m, fmax(fabs(q[k].x), fabs(q[k].y)));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  int e = 0;
+  if (m > 0.0) frexp(m, &e);  // m < 2^e
+  if (lane == 0) erow[r] = e;
+  const int kc = kr / 2;
+  for (int k = lane; k < kc; k += 32) {
+    cd v = (k < n && k != i) ? q[k] : cd{0.0, 0.0};
+    float dr[S], di[S];
+    digits<S>(v.x, e, dr);
+    digits<S>(v.y, e, di);
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+      A[((size_t)s * rows + r) * kc + k] = __floats2bfloat162_rn(dr[s], di[s]);
+  }
+}
+
+// Column exponents of Voff (thread per complex column).
+__global__ void k_col_exponents(const cd* __restrict__ V, int n, int ld, int* __restrict__ fcol) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double m = 0.0;
+  for (int k = 0; k < n; ++k) {
+    cd v = V[(size_t)k * ld + j];
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  int e = 0;
+  if (m > 0.0) frexp(m, &e);
+  fcol[j] = e;
+}
+
+// B^T slices: row 2j (Re-out) = [Vr(k,j), -Vi(k,j)]_k, row 2j+1 (Im-out) = [Vi, Vr]_k.
+template <int S>
+__global__ void k_slice_cols(const cd* __restrict__ V, int n, int ld, int kc, int nrows,
+                             const int* __restrict__ fcol, __nv_bfloat162* __restrict__ B) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (k >= kc || j >= n) return;
+  cd v = (k < n) ? V[(size_t)k * ld + j] : cd{0.0, 0.0};
+  const int e = fcol[j];
+  float dr[S], di[S];
+  digits<S>(v.x, e, dr);
+  digits<S>(v.y, e, di);
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    B[((size_t)s * nrows + 2 * j) * kc + k] = __floats2bfloat162_rn(dr[s], -di[s]);
+    B[((size_t)s * nrows + 2 * j + 1) * kc + k] = __floats2bfloat162_rn(di[s], dr[s]);
+  }
+}
+
+// ------------------------------------------------------------ tcgen05 GEMM + epilogue
+template <int S>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_split_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                 EpiArgs ep, int nkb) {
+  constexpr int STAGES = stages_for(S);
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t full_bar[3], empty_bar[3], done_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int fexp_sh[NC];
+  __shared__ int abort_sh;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * BM;
+  const int n0 = blockIdx.x * NT;        // real column
+  const int j0 = blockIdx.x * NC;        // complex column
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&done_bar, 1);
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_sh)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  for (int t = threadIdx.x; t < NC; t += THREADS) {
+    int j = j0 + t;
+    fexp_sh[t] = (j < ep.n) ? ep.fcol[j] : 0;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  const size_t sbytes = stage_bytes(S);
+
+  if (warp == 0) {
+    // ---------------- TMA producer
+    if (lane == 0) {
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int st = kb % STAGES, round = kb / STAGES;
+        if (round > 0 && !mbar_wait(&empty_bar[st], (round - 1) & 1)) {
+          atomicOr(ep.status, kStatusTimeout);
+          abort_sh = 1;
+          break;
+        }
+        if (abort_sh) break;
+        unsigned char* sa = smem + st * sbytes;
+        unsigned char* sb = sa + S * A_SLICE_BYTES;
+        mbar_expect_tx(&full_bar[st], (uint32_t)sbytes);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          tma_load_3d(&tmA, &full_bar[st], sa + s * A_SLICE_BYTES, kb * BK, m0, s);
+          tma_load_3d(&tmB, &full_bar[st], sb + s * B_SLICE_BYTES, kb * BK, n0, s);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = instr_desc();
+      bool started[NACC] = {false, false, false};
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int st = kb % STAGES, round = kb / STAGES;
+        if (!mbar_wait(&full_bar[st], round & 1)) {
+          atomicOr(ep.status, kStatusTimeout);
+          abort_sh = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + st * sbytes);
+        const uint32_t sb = sa + S * A_SLICE_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk) {
+#pragma unroll
+          for (int s = 0; s < S; ++s) {
+#pragma unroll
+            for (int t = 0; t < S - s; ++t) {
+              const int acc = (s + t < 2) ? s + t : 2;
+              const uint64_t ad = sw64_desc(sa + s * A_SLICE_BYTES + kk * 32);
+              const uint64_t bd = sw64_desc(sb + t * B_SLICE_BYTES + kk * 32);
+              tc_mma(tmem + acc * NT, ad, bd, idesc, started[acc] ? 1u : 0u);
+              started[acc] = true;
+            }
+          }
+        }
+        tc_commit(&empty_bar[st]);  // frees the stage once these MMAs complete
+      }
+      tc_commit(&done_bar);
+    }
+  } else {
+    // ---------------- TMEM drain (warps 2..5): rows 32*(warp%4) .. +31
+    const int q4 = warp & 3;
+    const int rl = q4 * 32 + lane;  // local row of this thread
+    const int r = m0 + rl;
+    const bool ok = mbar_wait(&done_bar, 0);
+    if (!ok) atomicOr(ep.status, kStatusTimeout);
+    tc_fence_after();
+    cd* stage_out = reinterpret_cast<cd*>(smem);
+    const int er = (r < ep.rows) ? ep.erow[r] : 0;
+    const uint32_t lane_base = tmem + ((uint32_t)(q4 * 32) << 16);
+    for (int c = 0; c < NT / 16; ++c) {
+      uint32_t a0[16], a1[16], a2[16];
+      tmem_ld16(lane_base + 0 * NT + c * 16, a0);
+      tmem_ld16(lane_base + 1 * NT + c * 16, a1);
+      tmem_ld16(lane_base + 2 * NT + c * 16, a2);
+      tmem_wait_ld();
+#pragma unroll
+      for (int e2 = 0; e2 < 8; ++e2) {
+        const int jl = c * 8 + e2;  // local complex column
+        const int sc = er + fexp_sh[jl] - 14;
+        double re = (double)__uint_as_float(a2[2 * e2]) + (double)__uint_as_float(a1[2 * e2]) +
+                    (double)__uint_as_float(a0[2 * e2]);
+        double im = (double)__uint_as_float(a2[2 * e2 + 1]) +
+                    (double)__uint_as_float(a1[2 * e2 + 1]) +
+                    (double)__uint_as_float(a0[2 * e2 + 1]);
+        stage_out[rl * EPI_STRIDE + jl] = cd{ldexp(re, sc), ldexp(im, sc)};
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  // ---------------- fused FP64 epilogue, coalesced over columns
+  if (!abort_sh) {
+    const cd* stage_out = reinterpret_cast<const cd*>(smem);
+    const cd vd = ep.V[(size_t)ep.kpad * ep.ld];
+    for (int rl = warp; rl < BM; rl += THREADS / 32) {
+      const int r = m0 + rl;
+      if (r >= ep.rows) break;
+      const int a = r / ep.n, i = r - a * ep.n;
+      const size_t ro = (size_t)r * ep.ld;
+      const cd qd = ep.Q[ro + i];
+      for (int jl = lane; jl < NC; jl += 32) {
+        const int j = j0 + jl;
+        if (j >= ep.n) break;
+        const cd q = ep.Q[ro + j];
+        const cd d = ep.D[(size_t)a * ep.ld + j] + vd;
+        const cd acc = stage_out[rl * EPI_STRIDE + jl] + qd * ep.V[(size_t)i * ep.ld + j] + q * d;
+        const cd p = ep.P[ro + j] + ep.cb * acc;
+        ep.P[ro + j] = p;
+        ep.Qo[ro + j] = q + ep.ca * p;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS));
+  }
+}
+
+}  // namespace split
+
+// ============================================================ host side
+namespace {
+
+struct Carve {
+  __nv_bfloat162* A;
+  __nv_bfloat162* B;
+  int* erow;
+  int* fcol;
+  int rows, kc, npad, nrows;
+};
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+Carve carve(void* base, int nang, int n, int S) {
+  Carve c;
+  c.rows = nang * n;
+  c.kc = round_up(n, 16);                 // complex k (= ld of the state)
+  c.npad = round_up(n, split::NC);
+  c.nrows = 2 * c.npad;
+  char* p = reinterpret_cast<char*>(base);
+  size_t o = 0;
+  c.A = reinterpret_cast<__nv_bfloat162*>(p + o);
+  o = align256(o + (size_t)S * c.rows * c.kc * sizeof(__nv_bfloat162));
+  c.B = reinterpret_cast<__nv_bfloat162*>(p + o);
+  o = align256(o + (size_t)S * c.nrows * c.kc * sizeof(__nv_bfloat162));
+  c.erow = reinterpret_cast<int*>(p + o);
+  o = align256(o + (size_t)c.rows * sizeof(int));
+  c.fcol = reinterpret_cast<int*>(p + o);
+  return c;
+}
+
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+  static EncodeTiled fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+      throw std::runtime_error("cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  return fn;
+}
+
+// 3-D map over [S][rows][kr] BF16 with a (32 x 128 x 1) box and 64-byte swizzle.
+CUtensorMap make_map(void* base, int kr, int rows, int S) {
+  CUtensorMap m;
+  cuuint64_t dims[3] = {(cuuint64_t)kr, (cuuint64_t)rows, (cuuint64_t)S};
+  cuuint64_t strides[2] = {(cuuint64_t)kr * 2, (cuuint64_t)kr * 2 * rows};
+  cuuint32_t box[3] = {split::BK, split::BM, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return m;
+}
+
+template <int S>
+void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
+               int nang, int n, int ld, double cb, double ca, cudaStream_t st) {
+  Carve c = carve(w.base, nang, n, S);
+  const int kr = 2 * c.kc;
+  // slices of the shared potential matrix (one set for every angle)
+  split::k_col_exponents<<<ceil_div(n, 128), 128, 0, st>>>(V, n, ld, c.fcol);
+  {
+    dim3 grid(ceil_div(c.kc, 128), n);
+    split::k_slice_cols<S><<<grid, 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, c.B);
+  }
+  // slices of the stacked states
+  split::k_slice_rows<S><<<ceil_div(c.rows, 8), 256, 0, st>>>(Q, c.rows, n, ld, kr, c.A, c.erow);
+  CUtensorMap ta = make_map(c.A, kr, c.rows, S);
+  CUtensorMap tb = make_map(c.B, kr, c.nrows, S);
+  split::EpiArgs ep{Q, P, Qo, V, D, c.erow, c.fcol, w.status, c.rows, n, ld, c.kc, S, cb, ca};
+  const size_t smem = split::smem_bytes(S);
+  static bool attr[6] = {false, false, false, false, false, false};
+  if (!attr[S]) {
+    cudaFuncSetAttribute(split::k_split_gemm<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr[S] = true;
+  }
+  dim3 grid(c.nrows / split::NT, ceil_div(c.rows, split::BM));
+  split::k_split_gemm<S><<<grid, split::THREADS, smem, st>>>(ta, tb, ep, kr / split::BK);
+}
+
+}  // namespace
+
+size_t split_workspace_bytes(int nang, int n, int slices) {
+  Carve c = carve(nullptr, nang, n, slices);
+  return reinterpret_cast<size_t>(c.fcol) + align256((size_t)c.npad * sizeof(int)) + 256;
+}
+
+SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, unsigned* status,
+                                     cudaStream_t st) {
+  SplitWorkspace w;
+  w.base = base;
+  w.nang = nang;
+  w.n = n;
+  w.slices = slices;
+  w.status = status;
+  // padded rows of the slice buffers are never written by the slicing kernels
+  cudaMemsetAsync(base, 0, split_workspace_bytes(nang, n, slices), st);
+  return w;
+}
+
+int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
+                int nang, int n, int ld, double cb, double ca, int slices, cudaStream_t st) {
+  switch (slices) {
+    case 3:
+      run_split<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, st);
+      break;
+    case 4:
+      run_split<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, st);
+      break;
+    case 5:
+      run_split<5>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, st);
+      break;
+    default:
+      throw std::invalid_argument("split slices must be 3, 4 or 5");
+  }
+  return 4;
+}
+
 }  // namespace trhepd

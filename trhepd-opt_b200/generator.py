@@ -34,6 +34,11 @@ A_SQ = 3.84      # square bulk lattice constant (A)
 C_SQ = 3.14      # bulk layer spacing (A)
 
 
+def _r6(x: float) -> float:
+    """Values are held at the 6 decimals the text files carry."""
+    return float(f"{x:.6f}")
+
+
 @dataclasses.dataclass
 class Element:
     z: int
@@ -43,6 +48,9 @@ class Element:
     bk: float = 0.4
     bz: float = 0.4
 
+    def __post_init__(self):
+        self.bh, self.bk, self.bz = _r6(self.bh), _r6(self.bk), _r6(self.bz)
+
 
 @dataclasses.dataclass
 class Atom:
@@ -51,6 +59,9 @@ class Atom:
     y: float
     z: float
     occ: float = 1.0
+
+    def __post_init__(self):
+        self.x, self.y, self.z, self.occ = _r6(self.x), _r6(self.y), _r6(self.z), _r6(self.occ)
 
 
 @dataclasses.dataclass
@@ -155,7 +166,7 @@ def _region_thickness(s: Structure, total: float) -> None:
     zb = [a.z for a in s.bulk_atoms]
     zoffset = 0.5 * (s.cc - max(zb) - min(zb))
     zz = max(0.0, max(a.z for a in s.surf_atoms) + zoffset)
-    s.dthick = max(0.5, total - s.cc - zz)
+    s.dthick = _r6(max(0.5, total - s.cc - zz))
 
 
 def small23(seed: int = 1) -> Structure:
@@ -175,6 +186,7 @@ def small23(seed: int = 1) -> Structure:
                   nsa=0, nsb=1, dthick=0.0, dxs=0.0, dys=0.0, surf_atoms=surf,
                   surface_dz=0.02, int_method=5)
     _region_thickness(s, 15.0)
+    s.dthick = _r6(s.dthick)
     return s
 
 

@@ -20,13 +20,15 @@ SPLIT_BF16 = 1
 OPT_RENORM_POLICY = 1
 OPT_RENORM_TAU = 2
 OPT_SPLIT_SLICES = 3
+OPT_PROFILE = 4
 
 # every symbol include/trhepd_b200.h declares
 EXPORTS = [
     "trhepd_create", "trhepd_destroy", "trhepd_last_error", "trhepd_set_option",
     "trhepd_last_stats", "trhepd_structure_factors", "trhepd_plane_group_images",
     "trhepd_potential_table", "trhepd_srfref", "trhepd_surf_run", "trhepd_surf_load",
-    "trhepd_surf_free", "trhepd_surf_views",
+    "trhepd_surf_free", "trhepd_surf_views", "trhepd_problem_create", "trhepd_problem_solve",
+    "trhepd_problem_fetch", "trhepd_problem_info", "trhepd_problem_destroy",
 ]
 
 
@@ -100,8 +102,16 @@ def load():
     L.trhepd_surf_free.argtypes = [_P]
     L.trhepd_surf_free.restype = None
     L.trhepd_surf_views.argtypes = [_P, ctypes.POINTER(PotState), ctypes.POINTER(SrfrefArgs)]
+    L.trhepd_problem_create.argtypes = [_P, ctypes.POINTER(PotState), ctypes.POINTER(SrfrefArgs),
+                                        ctypes.POINTER(_P)]
+    L.trhepd_problem_solve.argtypes = [_P, _P, _I]
+    L.trhepd_problem_fetch.argtypes = [_P, _P, _P, _P]
+    L.trhepd_problem_info.argtypes = [_P, _P, _I]
+    L.trhepd_problem_destroy.argtypes = [_P]
+    L.trhepd_problem_destroy.restype = None
     for name in EXPORTS:
-        if name not in ("trhepd_destroy", "trhepd_last_error", "trhepd_surf_free"):
+        if name not in ("trhepd_destroy", "trhepd_last_error", "trhepd_surf_free",
+                        "trhepd_problem_destroy"):
             getattr(L, name).restype = _I
     _lib = L
     return L
@@ -138,10 +148,12 @@ class Context:
         self._check(self._L.trhepd_set_option(self._h, option, float(value)))
 
     def last_stats(self) -> dict:
-        out = np.zeros(4)
-        self._check(self._L.trhepd_last_stats(self._h, out.ctypes.data, 4))
+        out = np.zeros(8)
+        self._check(self._L.trhepd_last_stats(self._h, out.ctypes.data, 8))
         return {"renormalisations": int(out[0]), "stage_products": int(out[1]),
-                "device_ms": float(out[2]), "stage_columns": int(out[3])}
+                "device_ms": float(out[2]), "stage_columns": int(out[3]),
+                "stage_kernel_ms": float(out[4]), "launches": int(out[5]),
+                "renorm_launches": int(out[6])}
 
     def surf_run(self, bulkp, surf, dz2: float, int_method: int = 5, precision: int = FP64,
                  out_path=None):

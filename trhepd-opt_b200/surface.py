@@ -56,6 +56,10 @@ class SurfaceProblem:
         assert nc.value == ncol
         return v, vi
 
+    def resident(self) -> "ResidentProblem":
+        """Upload this problem and build its stage tables in device memory."""
+        return ResidentProblem(self)
+
     def close(self):
         if getattr(self, "_h", None):
             self._L.trhepd_surf_free(self._h)
@@ -75,3 +79,39 @@ def potential_table(ctx: native.Context, bulkp, surf, dz2: float, int_method: in
 def srfref(ctx: native.Context, bulkp, surf, dz2: float, int_method: int = 5,
            precision: int = native.FP64):
     return SurfaceProblem(ctx, bulkp, surf, dz2, int_method).srfref(precision)
+
+
+class ResidentProblem:
+    """A srfref problem held in device memory (trhepd_problem_*)."""
+
+    def __init__(self, sp: SurfaceProblem):
+        self.sp, self.ctx, self._L = sp, sp.ctx, sp._L
+        h = ctypes.c_void_p()
+        self.ctx._check(self._L.trhepd_problem_create(self.ctx._h, ctypes.byref(sp.pot),
+                                                      ctypes.byref(sp.args), ctypes.byref(h)))
+        self._h = h
+        info = np.zeros(6, dtype=np.int64)
+        self._L.trhepd_problem_info(h, info.ctypes.data, 6)
+        self.nb, self.nangles, self.ns, self.nv, self.ncol, self.device_bytes = map(int, info)
+
+    def solve(self, precision: int = native.FP64):
+        """Integrate every angle; the intensities stay on the device."""
+        self.ctx._check(self._L.trhepd_problem_solve(self.ctx._h, self._h, int(precision)))
+
+    def fetch(self):
+        f2 = np.zeros((self.nangles, self.nb))
+        ang = np.zeros(self.nangles)
+        self.ctx._check(self._L.trhepd_problem_fetch(self.ctx._h, self._h, f2.ctypes.data,
+                                                     ang.ctypes.data))
+        return ang, f2
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.trhepd_problem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
