@@ -163,6 +163,16 @@ int trhepd_problem_info(const trhepd_problem* pb, int64_t* out, int n);
 void trhepd_problem_destroy(trhepd_problem* pb);
 
 /*
+ * bulk.exe (sim-trhepd-rheed/src/bulkm.f90:207-256 + bulkio.f90:10-223 + blkref
+ * bulk.f90:7-128) for one domain, positron mode: reads bulk.txt, computes every
+ * (angle, beam group) reflection matrix on the GPU and writes bulkP.b in the
+ * reference's record layout.  stats (optional): out[0] device ms, out[1] layers
+ * iterated, out[2] double-angle steps, out[3] (angle, group) items.
+ */
+int trhepd_bulk_run(trhepd_context* ctx, const char* bulk_txt, const char* out_path,
+                    double* stats);
+
+/*
  * surf.exe for the first domain (surfm.f90:6-97 + surfio.f90:60-381): reads
  * bulkP.b and surf.txt, slices the surface for dz2, solves on the GPU and, if
  * out_path is not NULL, writes the rocking-curve file in the reference format.

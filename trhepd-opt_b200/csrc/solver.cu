@@ -17,6 +17,8 @@
 #include <vector>
 
 #include "../../include/trhepd_b200.h"
+#include "bulk.h"
+#include "bulk_model.h"
 #include "host_model.h"
 #include "kernels.h"
 #include "split_gemm.h"
@@ -126,6 +128,7 @@ struct trhepd_context {
   DevBuf asf, b, dchg, ghk, z[3], ocr[3], ielm[3], st[3], depth, table, pair;
   DevBuf Q0, Q1, P, V, D, gam, F, flags, dval, gj, f2, wnsga2, status, split;
   DevBuf sgh, sgk, simg, snimg, sst;
+  DevBuf bk[24];  // bulk-solve work arrays
 };
 
 namespace {
@@ -489,6 +492,247 @@ void solve(trhepd_context* C, const SolveArgs& A, int precision, double* f2_out,
     throw;
   }
   Pb.release();
+}
+
+
+// ---------------------------------------------------------------- bulk solve
+// blkref (bulk.f90:7-128) for every (angle, group) item at once; see bulk.cu.
+void bulk_solve(trhepd_context* C, BulkInputs& B, std::vector<std::vector<cd>>& records,
+                double* stats) {
+  cudaStream_t st = C->stream;
+  const int nv = B.nv, ns = B.ns, ngr = B.ngr, n = B.nbgm;
+  if (n > kMaxBeams) throw std::invalid_argument("bulk beam group exceeds the GPU path limit");
+  if (3 * B.natm > 512) throw std::invalid_argument("bulk atoms exceed the potential table limit");
+  // structure factors (K2) for the three parts
+  std::vector<cd> stv[3];
+  for (int p = 0; p < 3; ++p) {
+    const StructureFactorJob& J = B.stf[p];
+    const double* gh = upload(C->sgh, B.gh, st);
+    const double* gk = upload(C->sgk, B.gk, st);
+    const double* img = upload(C->simg, J.img, st);
+    const int* nimg = upload(C->snimg, J.nimg, st);
+    cd* out = (cd*)C->sst.ensure((size_t)nv * B.natm * sizeof(cd));
+    launch_structure_factor(gh, gk, nv, img, nimg, B.natm, J.dx, J.dy, out, st);
+    stv[p].resize((size_t)nv * B.natm);
+    CK(cudaMemcpyAsync(stv[p].data(), out, stv[p].size() * sizeof(cd), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  // potential table at the slice centres: parts at zi, zi+cc, zi-cc (bulkio.f90:194-199)
+  std::vector<double> depth(ns);
+  for (int i = 1; i <= ns; ++i) depth[i - 1] = B.dz * (i - 0.5);
+  PotInputs in{};
+  in.asf = upload(C->asf, B.asf, st);
+  in.b = upload(C->b, B.bcoef, st);
+  in.dchg = upload(C->dchg, B.dchg, st);
+  in.ghk = upload(C->ghk, B.Ghk, st);
+  in.nv = nv;
+  in.nelm = B.nelm;
+  in.nabr = B.nabr;
+  in.nabi = B.nabi;
+  in.mab = kMab;
+  std::vector<int> ie(B.natm);
+  for (int j = 0; j < B.natm; ++j) ie[j] = B.ielm[j] - 1;
+  const double shift[3] = {0.0, B.cc, -B.cc};
+  for (int p = 0; p < 3; ++p) {
+    PotPart& P = in.part[p];
+    P.z = upload(C->z[p], B.z, st);
+    P.ocr = upload(C->ocr[p], B.ocr, st);
+    P.ielm = upload(C->ielm[p], ie, st);
+    P.st = upload(C->st[p], stv[p], st);
+    P.natm = B.natm;
+    P.nk = nv;
+    P.zshift = shift[p];
+    P.rmesh = 1.0;
+  }
+  const double* dd = upload(C->depth, depth, st);
+  TableEntry* table = (TableEntry*)C->table.ensure((size_t)ns * nv * sizeof(TableEntry));
+  launch_potential_table(in, dd, ns, table, st);
+  CK(cudaGetLastError());
+  std::vector<TableEntry> htab((size_t)ns * nv);
+  CK(cudaMemcpyAsync(htab.data(), table, htab.size() * sizeof(TableEntry), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  double vmax = 0.0;
+  for (const TableEntry& e : htab)
+    vmax = std::max(vmax, std::max(std::hypot(e.u.x, e.u.y), std::hypot(e.w.x, e.w.y)));
+
+  // items: (angle t, group g) -> b = t * ngr + g, padded to n beams
+  const bool ng_outer = B.ng > B.naz;
+  const int nrep1 = ng_outer ? B.naz : B.ng, nrep2 = ng_outer ? B.ng : B.naz;
+  const int nitem = nrep1 * nrep2 * ngr;
+  const int ld = round_up(n, 16), n2 = 2 * n, ld2 = round_up(n2, 16);
+  std::vector<int> gsize(ngr), goff(ngr + 1, 0);
+  for (int g = 0; g < ngr; ++g) {
+    gsize[g] = B.nbg[g];
+    goff[g + 1] = goff[g] + B.nbg[g];
+  }
+  std::vector<int> pair((size_t)ngr * n * n, 0);
+  for (int g = 0; g < ngr; ++g)
+    for (int i = 0; i < gsize[g]; ++i)
+      for (int j = 0; j < gsize[g]; ++j) {
+        if (i == j) continue;
+        int hi = std::max(i, j), lo = std::min(i, j);
+        int e = B.iv[(size_t)(goff[g] + lo) * B.nbgm + hi];
+        if (e < 1 || e > nv) throw std::invalid_argument("bulk beam-pair index out of range");
+        pair[((size_t)g * n + i) * n + j] = e - 1;
+      }
+  std::vector<cd> gam((size_t)nitem * n, cd{1.0, 0.0}), phase((size_t)nitem * n, cd{1.0, 0.0});
+  const double pi2 = std::atan(1.0) * 8.0;
+  const bool shifted = std::fabs(B.dx) > 1e-4 || std::fabs(B.dy) > 1e-4;
+  const double azr = B.azi + B.rdom;
+  double g2max = 0.0;
+  for (int t = 0; t < nrep1 * nrep2; ++t) {
+    int irep1 = t / nrep2, irep2 = t % nrep2;
+    double az, cga;
+    if (ng_outer) {
+      az = azr + irep1 * B.daz;
+      cga = std::cos(B.gi + irep2 * B.dg);
+    } else {
+      cga = std::cos(B.gi + irep1 * B.dg);
+      az = azr + irep2 * B.daz;
+    }
+    double wnx = B.wn * cga * std::cos(az), wny = B.wn * cga * std::sin(az);
+    for (int g = 0; g < ngr; ++g)
+      for (int i = 0; i < gsize[g]; ++i) {
+        int k = goff[g] + i;
+        double wgx = B.ghx * B.ihs[k] + wnx, wgy = B.ghy * B.ihs[k] + B.gky * B.iks[k] + wny;
+        double s = B.wn * B.wn - wgx * wgx - wgy * wgy;
+        size_t o = ((size_t)t * ngr + g) * n + i;
+        gam[o] = (s >= 0.0) ? cd{std::sqrt(s), 0.0} : cd{0.0, std::sqrt(-s)};
+        g2max = std::max(g2max, std::fabs(s));
+        if (shifted) {
+          double a = B.dx * pi2 / B.nh * B.ihs[k] + B.dy * pi2 / B.nk * B.iks[k];
+          phase[o] = cd{std::cos(a), std::sin(a)};
+        }
+      }
+  }
+  // double-angle steps: ||H|| h^2 <= 1/4 with h = dz / 2^m
+  const double hnorm = g2max + (double)n * vmax;
+  int m = 0;
+  while (hnorm * std::pow(B.dz / std::ldexp(1.0, m), 2) > 0.25) ++m;
+  const double h = B.dz / std::ldexp(1.0, m);
+
+  const int* d_pair = upload(C->pair, pair, st);
+  const cd* d_gam = upload(C->gam, gam, st);
+  const cd* d_ph = upload(C->F, phase, st);
+  const int* d_gsize = upload(C->flags, gsize, st);
+  const size_t nb1 = (size_t)nitem * n * ld, nb2 = (size_t)nitem * n2 * ld2;
+  auto buf1 = [&](int k) { return (cd*)C->bk[k].ensure(nb1 * sizeof(cd)); };
+  auto buf2 = [&](int k) { return (cd*)C->bk[k].ensure(nb2 * sizeof(cd)); };
+  cd *H = buf1(0), *X = buf1(1), *X2 = buf1(2), *X3 = buf1(3), *X4 = buf1(4), *Cm = buf1(5);
+  cd *Sm = buf1(6), *T1 = buf1(7), *T2 = buf1(8), *Hs = buf1(9);
+  cd *E = buf2(10), *Et = buf2(11), *En = buf2(12);
+  if (nitem > 65535) throw std::invalid_argument("too many (angle, group) items for one bulk batch");
+  // per-item matrices: n x n at ld (stride s1) or 2n x 2n at ld2 (stride s2)
+  const long long s1 = (long long)n * ld, s2 = (long long)n2 * ld2;
+  auto gemm1 = [&](const cd* A, const cd* Bm, cd* Cc, int beta, const int* active) {
+    BatchedGemm g{A, Bm, Cc, n, n, n, ld, ld, ld, s1, s1, s1, cd{1.0, 0.0}, beta, nitem, active};
+    launch_zgemm_batched(g, st);
+  };
+  auto gemm2 = [&](const cd* A, const cd* Bm, cd* Cc) {
+    BatchedGemm g{A, Bm, Cc, n2, n2, n2, ld2, ld2, ld2, s2, s2, s2, cd{1.0, 0.0}, 0, nitem,
+                  nullptr};
+    launch_zgemm_batched(g, st);
+  };
+  // T11 R or T21 R: A is the n x n block of T at row offset `row0` (ld2, stride s2)
+  auto gemm_t = [&](const cd* Tblk, const cd* Rm, cd* Cc, const int* active) {
+    BatchedGemm g{Tblk, Rm, Cc, n, n, n, ld2, ld, ld, s2, s1, s1, cd{1.0, 0.0}, 1, nitem, active};
+    launch_zgemm_batched(g, st);
+  };
+  // Taylor coefficients 1/(2k)! and 1/(2k+1)!, k = 0..8
+  double fc[9], fs[9];
+  {
+    double f = 1.0;
+    for (int k = 0; k <= 17; ++k) {
+      if (k > 0) f *= k;
+      if (k % 2 == 0) fc[k / 2] = 1.0 / f;
+      else fs[k / 2] = 1.0 / f;
+    }
+  }
+  CK(cudaEventRecord(C->ev0, st));
+  for (int l = 0; l < ns; ++l) {
+    launch_bulk_hamiltonian(table + (size_t)l * nv, d_pair, d_gam, d_gsize, ngr, n, ld, nitem,
+                            h * h, H, X, st);
+    gemm1(X, X, X2, 0, nullptr);
+    gemm1(X2, X, X3, 0, nullptr);
+    gemm1(X2, X2, X4, 0, nullptr);
+    const double c1[5] = {fc[0], fc[1], fc[2], fc[3], 0.0}, c2[5] = {fc[4], fc[5], fc[6], fc[7], fc[8]};
+    const double s1[5] = {fs[0], fs[1], fs[2], fs[3], 0.0}, s2[5] = {fs[4], fs[5], fs[6], fs[7], fs[8]};
+    launch_bulk_poly(X, X2, X3, nullptr, c1, n, ld, nitem, Cm, st);
+    launch_bulk_poly(X, X2, X3, X4, c2, n, ld, nitem, T1, st);
+    gemm1(X4, T1, Cm, 1, nullptr);   // C = P1 + X^4 P2
+    launch_bulk_poly(X, X2, X3, nullptr, s1, n, ld, nitem, Sm, st);
+    launch_bulk_poly(X, X2, X3, X4, s2, n, ld, nitem, T1, st);
+    gemm1(X4, T1, Sm, 1, nullptr);
+    launch_bulk_axpby(Sm, nullptr, h, 0.0, 0.0, n, ld, nitem, st);  // s = h * series
+    for (int q = 0; q < m; ++q) {  // C <- 2C^2 - I, s <- 2 s C
+      gemm1(Sm, Cm, T2, 0, nullptr);
+      gemm1(Cm, Cm, T1, 0, nullptr);
+      launch_bulk_axpby(Cm, T1, 0.0, 2.0, -1.0, n, ld, nitem, st);
+      launch_bulk_axpby(Sm, T2, 0.0, 2.0, 0.0, n, ld, nitem, st);
+    }
+    gemm1(H, Sm, Hs, 0, nullptr);
+    launch_bulk_build_e(Cm, Sm, Hs, n, ld, ld2, nitem, l == 0 ? Et : E, st);
+    if (l > 0) {  // E_tot <- E_l E_tot
+      gemm2(E, Et, En);
+      std::swap(Et, En);
+    }
+  }
+  cd* Tm = En;  // the free 2n buffer receives T = S E S^-1
+  launch_bulk_similarity(Et, d_gam, d_ph, d_gsize, ngr, n, ld2, nitem, Tm, st);
+  // layer recursion with the convergence exit
+  std::vector<int> act(nitem, 1);
+  int* d_act = upload(C->bk[13], act, st);
+  double* r20 = (double*)C->bk[14].ensure((size_t)nitem * n * sizeof(double));
+  cd* R = buf1(15);
+  cd* Qg = buf1(16);
+  cd* Pg = buf1(17);
+  unsigned* status = (unsigned*)C->status.ensure(16);
+  CK(cudaMemsetAsync(status, 0, 16, st));
+  CK(cudaMemsetAsync(R, 0, nb1 * sizeof(cd), st));
+  void* gjs = C->gj.ensure(gj_scratch_bytes(nitem, n));
+  int layers = 0;
+  for (int l = 1; l <= B.ml; ++l) {
+    launch_bulk_layer_init(Tm, d_act, n, ld, ld2, nitem, T1, T2, st);
+    if (l > 1) {
+      gemm_t(Tm, R, T1, d_act);                       // T12 + T11 R
+      gemm_t(Tm + (size_t)n * ld2, R, T2, d_act);     // T22 + T21 R
+    }
+    launch_bulk_transpose_pair(T1, T2, d_act, d_gsize, ngr, n, ld, nitem, Qg, Pg, st);
+    launch_gauss_jordan(Qg, Pg, d_act, nitem, n, ld, gjs, status, st);
+    launch_bulk_layer_finish(Pg, d_act, d_gsize, ngr, n, ld, nitem, l, B.epsb, r20, R, st);
+    layers = l;
+    if (l >= 21) {
+      CK(cudaMemcpyAsync(act.data(), d_act, nitem * sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      int live = 0;
+      for (int a : act) live += a;
+      if (!live) break;
+    }
+  }
+  CK(cudaEventRecord(C->ev1, st));
+  std::vector<cd> hR(nb1);
+  CK(cudaMemcpyAsync(hR.data(), R, nb1 * sizeof(cd), cudaMemcpyDeviceToHost, st));
+  unsigned hs[4];
+  CK(cudaMemcpyAsync(hs, status, 16, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  CK(cudaGetLastError());
+  float ms = 0;
+  cudaEventElapsedTime(&ms, C->ev0, C->ev1);
+  if (hs[0] & kStatusZeroPivot) throw CudaError("zero pivot in the bulk layer solve", TRHEPD_ENONFINITE);
+  records.assign(nitem, {});
+  for (int b = 0; b < nitem; ++b) {
+    int g = b % ngr, mg = gsize[g];
+    auto& rec = records[b];
+    rec.resize((size_t)mg * mg);
+    for (int j = 0; j < mg; ++j)
+      for (int i = 0; i < mg; ++i) rec[(size_t)j * mg + i] = hR[((size_t)b * n + i) * ld + j];
+  }
+  if (stats) {
+    stats[0] = ms;
+    stats[1] = layers;
+    stats[2] = m;
+    stats[3] = nitem;
+  }
 }
 
 // Structure factors of SurfaceInputs on the device.
@@ -873,6 +1117,18 @@ int trhepd_surf_views(const trhepd_surface_inputs* in, trhepd_pot_state* pot,
     a->nrep2 = ng_outer ? S.ng : S.naz;
   }
   return TRHEPD_OK;
+}
+
+int trhepd_bulk_run(trhepd_context* ctx, const char* bulk_txt, const char* out_path,
+                    double* stats) {
+  return guarded(ctx, [&] {
+    if (!bulk_txt || !out_path) throw std::invalid_argument("null path");
+    BulkInputs B;
+    load_bulk_inputs(bulk_txt, B);
+    std::vector<std::vector<cd>> records;
+    bulk_solve(ctx, B, records, stats);
+    write_bulkp(out_path, B, records);
+  });
 }
 
 int trhepd_surf_run(trhepd_context* ctx, const char* bulkp, const char* surf, double dz2,

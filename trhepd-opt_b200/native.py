@@ -29,6 +29,7 @@ EXPORTS = [
     "trhepd_potential_table", "trhepd_srfref", "trhepd_surf_run", "trhepd_surf_load",
     "trhepd_surf_free", "trhepd_surf_views", "trhepd_problem_create", "trhepd_problem_solve",
     "trhepd_problem_fetch", "trhepd_problem_info", "trhepd_problem_destroy",
+    "trhepd_bulk_run",
 ]
 
 
@@ -107,6 +108,7 @@ def load():
     L.trhepd_problem_solve.argtypes = [_P, _P, _I]
     L.trhepd_problem_fetch.argtypes = [_P, _P, _P, _P]
     L.trhepd_problem_info.argtypes = [_P, _P, _I]
+    L.trhepd_bulk_run.argtypes = [_P, ctypes.c_char_p, ctypes.c_char_p, _P]
     L.trhepd_problem_destroy.argtypes = [_P]
     L.trhepd_problem_destroy.restype = None
     for name in EXPORTS:
@@ -170,6 +172,14 @@ class Context:
         nb, nang = dims[0], dims[1]
         return f2[: nb * nang].reshape(nang, nb).copy(), {
             "nb": nb, "nangles": nang, "ns": dims[2], "nv": dims[3]}
+
+    def bulk_run(self, bulk_txt, out_path) -> dict:
+        """bulk.exe on the GPU: bulk.txt -> bulkP.b."""
+        st = np.zeros(4)
+        self._check(self._L.trhepd_bulk_run(self._h, str(bulk_txt).encode(),
+                                            str(out_path).encode(), st.ctypes.data))
+        return {"device_ms": float(st[0]), "layers": int(st[1]), "double_angle_steps": int(st[2]),
+                "items": int(st[3])}
 
     def close(self):
         if getattr(self, "_h", None):

@@ -1,0 +1,221 @@
+"""Continuous-batching request loop for structure-refinement traffic.
+
+Requests are candidate surfaces (a base structure with jittered surface atoms)
+with their own beam count N and glancing-angle grid.  The server keeps `slots`
+solver contexts, each with its own CUDA stream; a request is admitted when a
+slot is free and its device bytes fit the memory budget, so requests arriving
+while others run are started at once and their kernels overlap on the device.
+Each admitted request gets a device-resident problem (stage table, boundary
+data; trhepd_problem_*), is solved, and its intensities are returned.  The
+bulk boundary of a (base structure, angle grid) is written once and reused by
+every candidate of that base.
+
+Latency is completion minus arrival; the report gives p50/p99 and angle-solves/s.
+"""
+from __future__ import annotations
+
+import dataclasses
+import queue
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import bulkfile, generator, native, surface
+
+DEFAULT_MIX = {23: 0.30, 47: 0.30, 95: 0.20, 191: 0.15, 521: 0.05}
+GRIDS = (31, 61, 121)
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    n: int
+    n_angles: int
+    sigma: float
+    seed: int
+    arrival: float = 0.0          # seconds from stream start
+    # filled by the server
+    start: float = 0.0
+    finish: float = 0.0
+    f2: np.ndarray | None = None
+    error: str | None = None
+    device_ms: float = 0.0
+
+    @property
+    def latency(self) -> float:
+        return self.finish - self.arrival
+
+
+def base_structure(n: int, n_angles: int, region: float, dz: float) -> generator.Structure:
+    return generator.dense(n, seed=11, n_angles=n_angles, region=region, dz=dz)
+
+
+def poisson_stream(rate: float, duration: float, seed: int = 0, mix=None,
+                   grids=GRIDS) -> list[Request]:
+    """Poisson arrivals (mean `rate` per second) for `duration` seconds."""
+    mix = mix or DEFAULT_MIX
+    rng = np.random.default_rng(seed)
+    ns, ws = list(mix), np.array(list(mix.values()), dtype=float)
+    ws /= ws.sum()
+    out, t, rid = [], 0.0, 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            return out
+        out.append(Request(rid=rid, n=int(rng.choice(ns, p=ws)), n_angles=int(rng.choice(grids)),
+                           sigma=float(rng.uniform(0.05, 0.2)), seed=int(rng.integers(1 << 30)),
+                           arrival=t))
+        rid += 1
+
+
+class Server:
+    def __init__(self, device: int = 0, slots: int = 4, mem_budget_gb: float = 120.0,
+                 precision: int = native.FP64, region: float = 15.0, dz: float = 0.02,
+                 renorm_policy: int = 1):
+        self.device, self.slots, self.precision = device, slots, precision
+        self.region, self.dz = region, dz
+        self.budget = mem_budget_gb * 1e9
+        self.in_use = 0.0
+        self.cv = threading.Condition()
+        self.q: queue.Queue = queue.Queue()
+        self.tmp = Path(tempfile.mkdtemp(prefix="trhepd_serve_"))
+        self.bulk_cache: dict = {}
+        self.bulk_lock = threading.Lock()
+        self.t0 = time.perf_counter()
+        self.ctxs = [native.Context(device) for _ in range(slots)]
+        for c in self.ctxs:
+            c.set_option(native.OPT_RENORM_POLICY, renorm_policy)
+        self.workers = [threading.Thread(target=self._work, args=(c,), daemon=True)
+                        for c in self.ctxs]
+        self.done: list[Request] = []
+        for w in self.workers:
+            w.start()
+
+    # ---- inputs
+    def _bulk(self, n: int, n_angles: int) -> tuple[generator.Structure, Path]:
+        key = (n, n_angles)
+        with self.bulk_lock:
+            if key not in self.bulk_cache:
+                base = base_structure(n, n_angles, self.region, self.dz)
+                d = self.tmp / f"base_{n}_{n_angles}"
+                base.write(d)
+                bulkfile.write_bulkp(base, d / "bulkP.b")
+                self.bulk_cache[key] = (base, d / "bulkP.b")
+            return self.bulk_cache[key]
+
+    def _inputs(self, r: Request) -> tuple[Path, Path, float]:
+        base, bulkp = self._bulk(r.n, r.n_angles)
+        cand = generator.jitter(base, r.sigma, r.seed)
+        d = self.tmp / f"req_{r.rid}"
+        cand.write(d)
+        return bulkp, d / "surf.txt", base.surface_dz
+
+    @staticmethod
+    def device_bytes(n: int, n_angles: int, nv: int, ncol: int) -> float:
+        ld = -(-n // 16) * 16
+        state = 3 * n_angles * n * ld * 16
+        table = ncol * nv * 32
+        split = 4 * n_angles * n * 2 * ld * 2
+        return state + table + split + n_angles * n * n * 16
+
+    # ---- scheduling
+    def submit(self, r: Request) -> None:
+        self.q.put(r)
+
+    def _admit(self, need: float) -> None:
+        with self.cv:
+            while self.in_use + need > self.budget and self.in_use > 0:
+                self.cv.wait(timeout=1.0)
+            self.in_use += need
+
+    def _release(self, need: float) -> None:
+        with self.cv:
+            self.in_use -= need
+            self.cv.notify_all()
+
+    def _work(self, ctx: native.Context) -> None:
+        while True:
+            r = self.q.get()
+            if r is None:
+                return
+            need = 0.0
+            try:
+                bulkp, surf, dz = self._inputs(r)
+                sp = surface.SurfaceProblem(ctx, bulkp, surf, dz, 5)
+                need = self.device_bytes(sp.args.nb, sp.n_angles, sp.pot.nv,
+                                         6 * sp.args.ns + 1)
+                self._admit(need)
+                r.start = time.perf_counter() - self.t0
+                rp = sp.resident()
+                rp.solve(self.precision)
+                r.device_ms = ctx.last_stats()["device_ms"]
+                _, r.f2 = rp.fetch()
+                rp.close()
+                sp.close()
+            except Exception as e:  # reported per request
+                r.error = str(e)
+            finally:
+                if need:
+                    self._release(need)
+                r.finish = time.perf_counter() - self.t0
+                with self.cv:
+                    self.done.append(r)
+                self.q.task_done()
+
+    def close(self) -> None:
+        for _ in self.workers:
+            self.q.put(None)
+        for w in self.workers:
+            w.join(timeout=600)
+        for c in self.ctxs:
+            c.close()
+
+
+def run_stream(server: Server, stream: list[Request], time_scale: float = 1.0) -> dict:
+    """Replay arrivals in real time (scaled), wait for all, and summarise."""
+    server.t0 = time.perf_counter()
+    for r in stream:
+        delay = r.arrival * time_scale - (time.perf_counter() - server.t0)
+        if delay > 0:
+            time.sleep(delay)
+        r.arrival = time.perf_counter() - server.t0
+        server.submit(r)
+    server.q.join()
+    wall = time.perf_counter() - server.t0
+    return summarize(stream, wall)
+
+
+def summarize(stream: list[Request], wall: float) -> dict:
+    ok = [r for r in stream if r.error is None and r.finish > 0]
+    lat = np.array([r.latency for r in ok]) if ok else np.zeros(1)
+    angles = sum(r.n_angles for r in ok)
+    by_n = {}
+    for n in sorted({r.n for r in ok}):
+        ln = np.array([r.latency for r in ok if r.n == n])
+        by_n[n] = {"count": int(len(ln)), "p50_s": float(np.percentile(ln, 50)),
+                   "p99_s": float(np.percentile(ln, 99))}
+    return {"requests": len(stream), "completed": len(ok),
+            "errors": len(stream) - len(ok), "wall_s": wall,
+            "angle_solves_per_s": angles / wall if wall > 0 else 0.0,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "by_n": by_n}
+
+
+def isolated_times(server: Server, cases: list[tuple[int, int]], reps: int = 1) -> dict:
+    """Latency of each (N, angle grid) request solved alone on an idle server."""
+    out = {}
+    for n, g in cases:
+        best = None
+        for k in range(reps):
+            r = Request(rid=10**9 + len(out) * 10 + k, n=n, n_angles=g, sigma=0.1, seed=k)
+            t0 = time.perf_counter()
+            r.arrival = t0 - server.t0
+            server.submit(r)
+            server.q.join()
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out[(n, g)] = best
+    return out
