@@ -101,6 +101,23 @@ int trhepd_potential_table(trhepd_context* ctx, const trhepd_pot_state* pot, int
                            int ns, double dz, double* v, double* vi, int* ncol);
 
 /*
+ * Same tables as trhepd_potential_table, for callers that cannot allocate device
+ * memory (a host that hands the whole GPU to its own memory pool at start-up, or
+ * a service whose device memory is planned once): no cudaMalloc/cudaFree, no
+ * context.  Its device scratch (input copies and the table) is one 32 MiB array
+ * inside the library, held by every GPU that loads it until the process exits.
+ * Works on the current device and the legacy default stream, synchronously.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  Calls share the array (it keeps the last
+ * call's contents; nothing in it has to start at zero, since each call writes what
+ * it reads), so calls whose GPU work overlaps race.  Returns
+ * TRHEPD_ENOMEM when the inputs and the table need more than the 32 MiB.
+ * This entry point has no counterpart in the reference.
+ */
+int trhepd_potential_table_noalloc(const trhepd_pot_state* pot, int int_method, int ns,
+                                   double dz, double* v, double* vi, int* ncol);
+
+/*
  * Surface solve of every (azimuth, glancing angle) of one domain in one batch.
  * Replaces srfref (sim-trhepd-rheed/src/surflf.f90:7-171) including its
  * integrator call (hp_int4 / hp_int6, surf_prkn.f90:123-141) and the intensity

@@ -29,7 +29,7 @@ EXPORTS = [
     "trhepd_potential_table", "trhepd_srfref", "trhepd_surf_run", "trhepd_surf_load",
     "trhepd_surf_free", "trhepd_surf_views", "trhepd_problem_create", "trhepd_problem_solve",
     "trhepd_problem_fetch", "trhepd_problem_info", "trhepd_problem_destroy",
-    "trhepd_bulk_run",
+    "trhepd_potential_table_noalloc", "trhepd_bulk_run",
 ]
 
 
@@ -108,6 +108,7 @@ def load():
     L.trhepd_problem_solve.argtypes = [_P, _P, _I]
     L.trhepd_problem_fetch.argtypes = [_P, _P, _P, _P]
     L.trhepd_problem_info.argtypes = [_P, _P, _I]
+    L.trhepd_potential_table_noalloc.argtypes = [_P, _I, _I, _D, _P, _P, _P]
     L.trhepd_bulk_run.argtypes = [_P, ctypes.c_char_p, ctypes.c_char_p, _P]
     L.trhepd_problem_destroy.argtypes = [_P]
     L.trhepd_problem_destroy.restype = None
