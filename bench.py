@@ -173,30 +173,70 @@ def prepare_inputs(workload: str, seed: int, workdir: Path):
     return s, desc
 
 
-def cpu_baseline(workdir: Path, s, nangles: int, max_seconds: float = 25.0) -> dict:
-    """The oracle on the host cores: all threads, one angle per thread, the first
-    L slices of the workload (L sized for ~max_seconds), scaled to full solves."""
+def cpu_sample_plan(workdir: Path, s, nangles: int, seconds: float) -> dict:
+    """Size a bounded sample of the workload for the oracle on the host cores: all
+    threads, one angle per thread, the first L slices with L chosen so that one
+    sample takes about `seconds`."""
     from oracle import oracle as O
     O.build()
     cores = O.set_threads(os.cpu_count())
     nang = min(nangles, cores)
-    # calibrate on 2 slices, then size the sample
     O.set_max_slices(2)
     S = O.Surface(workdir / "bulkP.b", workdir / "surf.txt", s.surface_dz, s.int_method)
     t0 = time.perf_counter()
     S.solve(0, nang)
     t_cal = time.perf_counter() - t0
     S.close()
-    L = max(2, min(2000, int(2 * max_seconds / max(t_cal, 1e-3))))
-    O.set_max_slices(L)
+    O.set_max_slices(0)
+    L = max(2, min(2000, int(2 * seconds / max(t_cal, 1e-3))))
+    return {"angles": nang, "slices": L, "cores": cores}
+
+
+def cpu_sample(workdir: Path, s, plan: dict) -> tuple[float, int]:
+    """One timed sample: (seconds, slices actually integrated)."""
+    from oracle import oracle as O
+    O.set_max_slices(plan["slices"])
     S = O.Surface(workdir / "bulkP.b", workdir / "surf.txt", s.surface_dz, s.int_method)
     L = S.ns
     t0 = time.perf_counter()
-    S.solve(0, nang)
+    S.solve(0, plan["angles"])
     t = time.perf_counter() - t0
     S.close()
     O.set_max_slices(0)
-    return {"seconds": t, "angles": nang, "slices": L, "cores": cores}
+    return t, L
+
+
+def cpu_baseline(workdir: Path, s, nangles: int, max_seconds: float = 25.0) -> dict:
+    plan = cpu_sample_plan(workdir, s, nangles, max_seconds)
+    t, L = cpu_sample(workdir, s, plan)
+    return {"seconds": t, "angles": plan["angles"], "slices": L, "cores": plan["cores"]}
+
+
+def serve_leg(device: int, seconds: float, load: float, precision: int, seed: int = 0) -> dict:
+    """Poisson stream of mixed-N refinement requests through the serving loop at
+    `load` times the throughput the isolated solve times allow; reports p50/p99
+    latency, angle-solves/s and each request's latency over its isolated time."""
+    from trhepd_opt_b200 import serving
+    srv = serving.Server(device=device, slots=4, mem_budget_gb=120.0, precision=precision)
+    try:
+        cases = [(n, g) for n in serving.DEFAULT_MIX for g in serving.GRIDS]
+        iso = serving.isolated_times(srv, cases)
+        busy = serving.expected_busy_seconds(iso)
+        rate = load / busy
+        stream = serving.poisson_stream(rate, seconds, seed=seed)
+        out = serving.run_stream(srv, stream)
+        out["latency_over_isolated"] = serving.slowdowns(stream, iso)
+    finally:
+        srv.close()
+    out["by_n"] = {str(k): v for k, v in out["by_n"].items()}
+    out.update({"arrival_rate_req_s": rate, "duration_s": seconds, "target_load": load,
+                "mean_isolated_request_s": busy,
+                "isolated_s": {f"{n}x{g}": t for (n, g), t in iso.items()},
+                "mix": {str(k): v for k, v in serving.DEFAULT_MIX.items()},
+                "grids": list(serving.GRIDS), "slots": 4, "hbm_budget_gb": 120.0,
+                "structures": "dense(N) base per (N, grid), 15 A region in 0.02 A slices, "
+                              "surface atoms jittered by sigma in [0.05, 0.2] A per request"})
+    return out
 
 
 def main():
@@ -210,6 +250,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=40.0)
+    ap.add_argument("--serve-load", type=float, default=0.5,
+                    help="arrival rate as a fraction of the isolated-solve throughput")
+    ap.add_argument("--serve-fp64", action="store_true",
+                    help="also run the serving stream with the plain FP64 form")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     pg = None
@@ -227,22 +273,29 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            b = cpu_baseline(workdir, s, 61)
             S_ns = surface_slices(workdir, s)
-            per_angle = b["seconds"] * S_ns / b["slices"] / b["angles"]  # thread-seconds
-            value = b["angles"] / (b["seconds"] * S_ns / b["slices"])
+            plan = cpu_sample_plan(workdir, s, 61, seconds=8.0)
+            for _ in range(max(args.warmup, 0)):
+                cpu_sample(workdir, s, plan)
+            tot, L = 0.0, plan["slices"]
+            for _ in range(args.steps):
+                t, L = cpu_sample(workdir, s, plan)
+                tot += t
+            full = tot * S_ns / L  # seconds for the sampled angles over every slice
+            value = plan["angles"] * args.steps / full
             line = {"impl": "reference", "metric": METRIC, "value": value,
-                    "unit": "angle-solves/s", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+                    "unit": "angle-solves/s", "n_gpus": args.gpus, "steps": args.steps,
+                    "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
                     "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                     "dtype": "f64", "data": "synthetic",
                     "config": {"workload": desc},
                     "cpu_baseline": {"value": value, "unit": "angle-solves/s",
-                                     "cores": b["cores"], "kind": "port",
-                                     "sample": f"{b['angles']} angles x first {b['slices']} of "
-                                               f"{S_ns} slices, scaled by slice count"},
+                                     "cores": plan["cores"], "kind": "port",
+                                     "sample": f"per step {plan['angles']} angles x first {L} "
+                                               f"of {S_ns} slices on {plan['cores']} threads, "
+                                               "scaled by slice count"},
                     "e2e": {"value": value, "unit": "angle-solves/s",
-                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                    "seconds_per_angle_solve_1core": per_angle}
+                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
             print(json.dumps(line), flush=True)
         if pg:
             pg.barrier()
@@ -355,6 +408,17 @@ def main():
                "sample": f"{b['angles']} angles x first {b['slices']} of {ns} slices on "
                          f"{b['cores']} threads, scaled by slice count"}
 
+    rp.close()
+    sp.close()
+    ctx.close()
+
+    serve = None
+    if rank == 0 and ws == 1 and not args.no_serve:
+        serve = {"split" if prec == native.SPLIT_BF16 else "fp64":
+                 serve_leg(local, args.serve_seconds, args.serve_load, prec)}
+        if args.serve_fp64 and prec != native.FP64:
+            serve["fp64"] = serve_leg(local, args.serve_seconds, args.serve_load, native.FP64)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "angle-solves/s", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -368,11 +432,9 @@ def main():
                            "l2": "inputs larger than L2 (state + stage table > 1 GB)",
                            "parallelism": f"replicas x{ws}"},
                 "roofline": roof, "fp64": fp64, "e2e": e2e, "cpu_baseline": cpu,
-                "gpu_launches": launches, "clocks": clk, "wall_seconds_timed": t_wall}
+                "gpu_launches": launches, "clocks": clk, "wall_seconds_timed": t_wall,
+                "serving": serve}
         print(json.dumps(line), flush=True)
-    rp.close()
-    sp.close()
-    ctx.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()

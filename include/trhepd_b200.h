@@ -44,7 +44,9 @@ enum trhepd_option {
                                    1: growth bound, uniform schedule (see DESIGN) */
   TRHEPD_OPT_RENORM_TAU = 2,    /* growth bound ln(cond) between renormalisations (policy 1) */
   TRHEPD_OPT_SPLIT_SLICES = 3,  /* BF16 slices per operand in the split form (3..5) */
-  TRHEPD_OPT_PROFILE = 4        /* nonzero: time every stage-product launch with CUDA events */
+  TRHEPD_OPT_PROFILE = 4,       /* nonzero: time every stage-product launch with CUDA events */
+  TRHEPD_OPT_SPLIT_KERNEL = 5   /* split-form kernel: 0 persistent, two accumulators, epilogue
+                                   overlapped (default); 1 one CTA per tile, three accumulators */
 };
 
 typedef struct trhepd_context trhepd_context;
@@ -94,8 +96,10 @@ int trhepd_plane_group_images(int nsg, int ma, int mb, int na, int nb, double x,
 
 /*
  * Stage potential tables of an integrator: v, vi complex (nv, ncol) with
- * ncol = s*ns+1 for int_method 5/6 (s = 6 / 11).  Replaces hp_int_init4/6
- * (sim-trhepd-rheed/src/surf_prkn.f90:174-197) and comp_scpot (surfio.f90:29-41).
+ * ncol = ns for int_method 4, 6*ns+1 for 5, 11*ns+1 for 6 and 2*ns+1 for 7.
+ * Replaces hp_int_init4/6 (sim-trhepd-rheed/src/surf_prkn.f90:174-197),
+ * m2_int_init (surf_magnus.f90:4-20), rk4_int_init (surf_rk.f90:4-25) and
+ * comp_scpot (surfio.f90:29-41).
  */
 int trhepd_potential_table(trhepd_context* ctx, const trhepd_pot_state* pot, int int_method,
                            int ns, double dz, double* v, double* vi, int* ncol);
@@ -120,7 +124,8 @@ int trhepd_potential_table_noalloc(const trhepd_pot_state* pot, int int_method, 
 /*
  * Surface solve of every (azimuth, glancing angle) of one domain in one batch.
  * Replaces srfref (sim-trhepd-rheed/src/surflf.f90:7-171) including its
- * integrator call (hp_int4 / hp_int6, surf_prkn.f90:123-141) and the intensity
+ * integrator call (lf_int_spa surf_magnus.f90:46-110, hp_int4 / hp_int6
+ * surf_prkn.f90:123-141, rk4_int surf_rk.f90:27-91: int_method 4-7) and the intensity
  * formula (surflf.f90:142-151).  Arguments keep srfref's names and meaning;
  * t1_records holds the bulk reflection records srfref reads from unit 1
  * (surflf.f90:65-72): nrep1*nrep2 angles, each ngr blocks of nbg(l)^2 complex

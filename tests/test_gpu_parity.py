@@ -22,8 +22,9 @@ def ctx():
     c.close()
 
 
-GOLD = [("test23", m, dz) for m in (5, 6) for dz in ("0.68", "0.1", "0.022")]
+GOLD = [("test23", m, dz) for m in (4, 5, 6, 7) for dz in ("0.68", "0.1", "0.022")]
 GOLD += [("test47", 5, "0.68"), ("test47", 6, "0.68"), ("test47", 5, "0.22"),
+         ("test47", 7, "0.22"),
          ("test521", 5, "0.68"), ("test521", 6, "0.68"), ("test521", 5, "0.33")]
 # test521 sp6 at 0.68 A slices: eleven 0.68 A stages per slice make the step
 # ill-conditioned; the CPU oracle itself differs from the reference's MKL output
@@ -106,6 +107,38 @@ def test_potential_table_matches_oracle(ctx, golden, oracle_mod):
     S = oracle_mod.Surface(d / "bulkP.b", d / "surf.txt", 0.1, 5)
     v_ref, vi_ref, _ = S.tables()
     v, vi = surface.potential_table(ctx, d / "bulkP.b", d / "surf.txt", 0.1, 5)
+    scale = np.abs(v_ref).max()
+    assert np.abs(v - v_ref).max() <= 1e-13 * scale
+    assert np.abs(vi - vi_ref).max() <= 1e-13 * scale
+
+
+@pytest.mark.parametrize("method", [1, 2, 3])
+@pytest.mark.parametrize("dz", ["0.1", "0.68"])
+def test_magnus_matches_oracle(ctx, golden, oracle_mod, method, dz):
+    """Magnus m2/m4/m6 (no reference output ships for them) against the oracle's
+    restatement of surf_magnus.f90 on the reference's N=23 inputs, both with the
+    reference's Gershgorin renormalisation."""
+    from trhepd_opt_b200 import native
+    d = golden / "test23"
+    S = oracle_mod.Surface(d / "bulkP.b", d / "surf.txt", float(dz), method)
+    ref, _, _ = S.solve()
+    S.close()
+    ctx.set_option(native.OPT_RENORM_POLICY, 0)
+    f2, _ = ctx.surf_run(d / "bulkP.b", d / "surf.txt", float(dz), method, native.FP64)
+    abs_err, rel_err = spot_errors(f2, ref)
+    assert abs_err <= 1e-10 and rel_err <= 1e-9, (abs_err, rel_err)
+
+
+@pytest.mark.parametrize("method", [1, 2, 3, 4, 7])
+def test_potential_table_other_integrators(ctx, golden, oracle_mod, method):
+    """Stage-table columns of m2/m4/m6, leapfrog and RK4 against the oracle."""
+    from trhepd_opt_b200 import surface
+    d = golden / "test23"
+    S = oracle_mod.Surface(d / "bulkP.b", d / "surf.txt", 0.1, method)
+    v_ref, vi_ref, _ = S.tables()
+    S.close()
+    v, vi = surface.potential_table(ctx, d / "bulkP.b", d / "surf.txt", 0.1, method)
+    assert v.shape == v_ref.shape
     scale = np.abs(v_ref).max()
     assert np.abs(v - v_ref).max() <= 1e-13 * scale
     assert np.abs(vi - vi_ref).max() <= 1e-13 * scale

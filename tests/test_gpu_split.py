@@ -32,16 +32,26 @@ def _resident(ctx, tmp_path, s):
     return sp, sp.resident()
 
 
-@pytest.mark.parametrize("case", ["small23", "dense95"])
-def test_split_matches_fp64(ctx, tmp_path, case):
+@pytest.mark.parametrize("variant", [0, 1], ids=["persistent", "per_tile"])
+@pytest.mark.parametrize("case", ["small23", "dense95", "dense200"])
+def test_split_matches_fp64(ctx, tmp_path, case, variant):
     from trhepd_opt_b200 import generator, native
-    s = generator.small23() if case == "small23" else generator.dense(95, n_angles=8, region=6.0)
+    if case == "small23":
+        s = generator.small23()
+    elif case == "dense95":
+        s = generator.dense(95, n_angles=8, region=6.0)
+    else:  # several row and column tiles, a ragged last tile, 13 angles
+        s = generator.dense(200, n_angles=13, region=4.0)
     sp, rp = _resident(ctx, tmp_path, s)
     rp.solve(native.FP64)
     _, ref = rp.fetch()
     ctx.set_option(native.OPT_SPLIT_SLICES, 4)
-    rp.solve(native.SPLIT_BF16)
-    _, got = rp.fetch()
+    ctx.set_option(native.OPT_SPLIT_KERNEL, variant)
+    try:
+        rp.solve(native.SPLIT_BF16)
+        _, got = rp.fetch()
+    finally:
+        ctx.set_option(native.OPT_SPLIT_KERNEL, 0)
     abs_err, _ = spot_errors(got, ref)
     _, rel_big = spot_errors(got, ref, floor=1e-3)
     assert abs_err <= 1e-6, abs_err
@@ -72,3 +82,19 @@ def test_more_slices_is_more_accurate(ctx, tmp_path):
         errs.append(spot_errors(got, ref)[0])
     ctx.set_option(native.OPT_SPLIT_SLICES, 4)
     assert errs[0] > errs[1] > errs[2], errs
+
+
+@pytest.mark.parametrize("method", [4, 7])
+def test_split_other_integrators(ctx, tmp_path, method):
+    """The leapfrog and RK4 paths take the same split stage product."""
+    from trhepd_opt_b200 import generator, native
+    s = generator.small23()
+    s.int_method = method
+    sp, rp = _resident(ctx, tmp_path, s)
+    rp.solve(native.FP64)
+    _, ref = rp.fetch()
+    ctx.set_option(native.OPT_SPLIT_SLICES, 4)
+    rp.solve(native.SPLIT_BF16)
+    _, got = rp.fetch()
+    abs_err, _ = spot_errors(got, ref)
+    assert abs_err <= 1e-6, abs_err

@@ -77,6 +77,9 @@ size_t gj_scratch_bytes(int nang, int n);
 void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld, void* scratch,
                          unsigned* status, cudaStream_t st);
 
+// RK4 stage combination (rk4_int, surf_rk.f90:27-91); see kernels_f64.cu.
+void launch_rk4_combine(cd* Q, cd* P, cd* Qt, cd* Pt, cd* KP, cd* SQ, cd* SP, int j, double w,
+                        double step, double h6, int nang, int n, int ld, cudaStream_t st);
 // invstransh (matcomp.f90:140-172): Q = I + F^H, P = I - F^H, from F (nang x n x n, row-major).
 void launch_invstransh_build(const cd* F, cd* Q, cd* P, int nang, int n, int ld, cudaStream_t st);
 // P(i,j) = i * P(i,j) * conj(g_i)  (after the solve)

@@ -85,7 +85,7 @@ __global__ void k_potential_table(PotInputs in, const double* __restrict__ depth
   }
   __syncthreads();
   for (int k = threadIdx.x; k < nv; k += blockDim.x) {
-    double vr = 0.0, vim = 0.0, wr = 0.0, wim = 0.0;  // v and vi accumulated separately
+    double vr = 0.0, vim = 0.0;  // v and vi accumulated separately
     double vir = 0.0, vii = 0.0;
     for (int p = 0; p < 3; ++p) {
       const PotPart& P = in.part[p];
@@ -109,12 +109,9 @@ __global__ void k_potential_table(PotInputs in, const double* __restrict__ depth
         if (in.nabi == 1) {
           double sap = asf_e[(size_t)nabr * nv + 0];
           for (int i = 0; i < nabr; ++i) {
-            double e = sE[t * kMaxGauss + i];
-            if (e != 0.0 || true) {
-              double aex = asf_e[(size_t)i * nv + k] * e;
-              tv = tv + aex;
-              tvi = tvi + fabs(sap * aex);
-            }
+            double aex = asf_e[(size_t)i * nv + k] * sE[t * kMaxGauss + i];
+            tv = tv + aex;
+            tvi = tvi + fabs(sap * aex);
           }
         } else {
           for (int i = 0; i < nabr; ++i) tv = tv + asf_e[(size_t)i * nv + k] * sE[t * kMaxGauss + i];
@@ -127,8 +124,6 @@ __global__ void k_potential_table(PotInputs in, const double* __restrict__ depth
         vii = vii + (0.0 * ct.y + tvi * ct.x);
       }
     }
-    (void)wr;
-    (void)wim;
     TableEntry e;
     e.u = cd{vr + vir, vim + vii};
     e.w = cd{vr - vir, vim - vii};
@@ -610,16 +605,29 @@ __global__ void k_gj_update(cd* __restrict__ Q, cd* __restrict__ P, const int* _
     for (int m = 0; m < w; ++m) s = s + W1[k * kW + m] * C1[m][lane_col];
     base[(size_t)(c0 + k) * ld] = s;
   }
-  // other rows <- C2 - L2 C1
+  // other rows <- C2 - L2 C1; eight rows per thread at a time so that their
+  // loads are in flight together
+  if (!valid) return;
   const cd* L2 = sc.L2 + (size_t)a * n * kW;
-  for (int i = rgrp; i < n; i += nrg) {
-    if (i >= c0 && i < c0 + w) continue;
-    if (!valid) continue;
-    cd s = base[(size_t)i * ld];
-    const cd* l = L2 + (size_t)i * kW;
-#pragma unroll 4
-    for (int m = 0; m < w; ++m) s = s - l[m] * C1[m][lane_col];
-    base[(size_t)i * ld] = s;
+  constexpr int U = 8;
+  for (int i0 = rgrp; i0 < n; i0 += U * nrg) {
+    cd s[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * nrg;
+      const bool row = i < n && !(i >= c0 && i < c0 + w);
+      s[u] = row ? base[(size_t)i * ld] : cd{0.0, 0.0};
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * nrg;
+      if (i < n && !(i >= c0 && i < c0 + w)) {
+        const cd* l = L2 + (size_t)i * kW;
+        cd v = s[u];
+        for (int m = 0; m < w; ++m) v = v - l[m] * C1[m][lane_col];
+        base[(size_t)i * ld] = v;
+      }
+    }
   }
 }
 
@@ -639,6 +647,48 @@ void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld,
     dim3 grid(ceil_div(total, kUpdCols), nang);
     k_gj_update<<<grid, 256, 0, st>>>(Q, P, flag, n, ld, c0, w, sc);
   }
+}
+
+// ============================================================ RK4 stage combination
+// After the product KP = A M of RK4 stage j (0..3, rk4_int surf_rk.f90:27-91):
+// the stage derivative is k_j = (kq, KP) with kq = P (j = 0) or Pt; accumulate
+// SQ/SP = k1 + 2 k2 + 2 k3 + k4 in that order, form the next stage point
+// (Qt, Pt) = (Q, P) + step k_j, and after the last stage (Q, P) += dz/6 (SQ, SP).
+// KP is cleared for the next product.  Only the n x n block is touched.
+__global__ void k_rk4_combine(cd* __restrict__ Q, cd* __restrict__ P, cd* __restrict__ Qt,
+                              cd* __restrict__ Pt, cd* __restrict__ KP, cd* __restrict__ SQ,
+                              cd* __restrict__ SP, int j, double w, double step, double h6, int n,
+                              int ld) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (c >= n) return;
+  const size_t o = (size_t)r * ld + c;
+  const cd kq = (j == 0) ? P[o] : Pt[o];
+  const cd kp = KP[o];
+  cd sq, sp;
+  if (j == 0) {
+    sq = kq;
+    sp = kp;
+  } else {
+    sq = SQ[o] + w * kq;
+    sp = SP[o] + w * kp;
+  }
+  if (j < 3) {
+    SQ[o] = sq;
+    SP[o] = sp;
+    Qt[o] = Q[o] + step * kq;
+    Pt[o] = P[o] + step * kp;
+  } else {
+    Q[o] = Q[o] + h6 * sq;
+    P[o] = P[o] + h6 * sp;
+  }
+  KP[o] = cd{0.0, 0.0};
+}
+
+void launch_rk4_combine(cd* Q, cd* P, cd* Qt, cd* Pt, cd* KP, cd* SQ, cd* SP, int j, double w,
+                        double step, double h6, int nang, int n, int ld, cudaStream_t st) {
+  dim3 grid(ceil_div(n, 128), nang * n);
+  k_rk4_combine<<<grid, 128, 0, st>>>(Q, P, Qt, Pt, KP, SQ, SP, j, w, step, h6, n, ld);
 }
 
 // ============================================================ boundary transforms

@@ -18,6 +18,7 @@
 
 #include "../../include/trhepd_b200.h"
 #include "bulk.h"
+#include "magnus.h"
 #include "bulk_model.h"
 #include "host_model.h"
 #include "kernels.h"
@@ -85,29 +86,73 @@ T* upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
   return b.as<T>();
 }
 
+// Integrator families of srfref (surflf.f90:118-140) on the GPU path.
+enum Family { kRkn = 0, kLeapfrog = 1, kRk4 = 2, kMagnus2 = 3, kMagnus4 = 4, kMagnus6 = 5 };
+
 struct Integrator {
-  int s;
-  const double* bab;
+  int method = 5;
+  Family family = kRkn;
+  int s = 6;                   // RKN stages per slice
+  const double* bab = nullptr; // RKN coefficients (b1, a1, b2, a2, ...)
 };
 
 Integrator integrator_for(int method) {
-  if (method == 5) return {6, kRkn46};
-  if (method == 6) return {11, kRkn611};
-  throw std::invalid_argument("int_method must be 5 (RKN-4) or 6 (RKN-6) on the GPU path");
+  switch (method) {
+    case 1: return {1, kMagnus2, 1, nullptr};
+    case 2: return {2, kMagnus4, 3, nullptr};
+    case 3: return {3, kMagnus6, 3, nullptr};
+    case 4: return {4, kLeapfrog, 1, nullptr};
+    case 5: return {5, kRkn, 6, kRkn46};
+    case 6: return {6, kRkn, 11, kRkn611};
+    case 7: return {7, kRk4, 2, nullptr};
+    default:
+      throw std::invalid_argument(
+          "int_method must be 1-3 (Magnus 2/4/6), 4 (leapfrog), 5 (RKN-4), 6 (RKN-6) or 7 (RK4)"
+          " on the GPU path");
+  }
 }
 
-// Stage depths of hp_int_init (surf_prkn.f90:184-196), same arithmetic order.
+// Depths of the stage potential table, same arithmetic order as the reference's
+// init routines: hp_int_init4/6 (surf_prkn.f90:184-196), m2_int_init
+// (surf_magnus.f90:4-20, used by m2 and leapfrog), m4_int_init (:24-42, m4 and m6),
+// rk4_int_init (surf_rk.f90:4-25).
 std::vector<double> stage_depths(const Integrator& I, int ns, double dz) {
   std::vector<double> d;
-  d.reserve((size_t)I.s * ns + 1);
-  for (int l = 1; l <= ns; ++l) {
-    double iz = dz * (l - 1);
-    for (int k = 1; k <= I.s; ++k) {
-      d.push_back(iz);
-      iz = iz + dz * I.bab[2 * k - 1];
+  switch (I.family) {
+    case kRkn:
+      d.reserve((size_t)I.s * ns + 1);
+      for (int l = 1; l <= ns; ++l) {
+        double iz = dz * (l - 1);
+        for (int k = 1; k <= I.s; ++k) {
+          d.push_back(iz);
+          iz = iz + dz * I.bab[2 * k - 1];
+        }
+      }
+      d.push_back(dz * ns);
+      break;
+    case kLeapfrog:
+    case kMagnus2:
+      for (int l = 1; l <= ns; ++l) d.push_back(dz * (l - 0.5));
+      break;
+    case kMagnus4:
+    case kMagnus6: {  // m4_int_init (surf_magnus.f90:24-42): the three Gauss points
+      const double c0 = (5.0 - std::sqrt(15.0)) / 10, c1 = 0.5, c2 = (5.0 + std::sqrt(15.0)) / 10;
+      for (int l = 1; l <= ns; ++l) {
+        d.push_back(dz * ((l - 1) + c0));
+        d.push_back(dz * ((l - 1) + c1));
+        d.push_back(dz * ((l - 1) + c2));
+      }
+      break;
     }
+    case kRk4:
+      for (int l = 1; l <= ns; ++l) {
+        const double iz = dz * (l - 1);
+        d.push_back(iz);
+        d.push_back(iz + 0.5 * dz);
+      }
+      d.push_back(dz * ns);
+      break;
   }
-  d.push_back(dz * ns);
   return d;
 }
 
@@ -121,6 +166,7 @@ struct trhepd_context {
   int renorm_policy = 0;
   double renorm_tau = std::log(1e3);
   int split_slices = 4;
+  int split_variant = kSplitPersistent;
   int profile = 0;               // 1: time every stage-product launch with events
   double stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<cudaEvent_t> evpool;
@@ -129,6 +175,8 @@ struct trhepd_context {
   DevBuf Q0, Q1, P, V, D, gam, F, flags, dval, gj, f2, wnsga2, status, split;
   DevBuf sgh, sgk, simg, snimg, sst;
   DevBuf bk[24];  // bulk-solve work arrays
+  DevBuf rk[5];   // RK4 / Magnus stage buffers
+  DevBuf mg[9];   // Magnus shared matrices
 };
 
 namespace {
@@ -215,7 +263,7 @@ struct SolveArgs {
 // fetched.
 struct trhepd_problem {
   int n = 0, ns = 0, nv = 0, nang = 0, ld = 0, nb0 = 0, int_method = 5;
-  Integrator I{6, nullptr};
+  Integrator I{};
   double dz = 0, kappa_max = 0;
   int ncol = 0;
   DevBuf table, pair, gam, D, F, wnsga2, f2;
@@ -265,6 +313,9 @@ void prepare(trhepd_context* C, const SolveArgs& A, trhepd_problem& Pb) {
   const int nrep1 = ng_outer ? A.naz : A.ng, nrep2 = ng_outer ? A.ng : A.naz;
   const int nang = nrep1 * nrep2;
   const int ld = round_up(n, 16);
+  // row-parallel kernels index the nang*n stacked rows with the grid's y dimension
+  if ((long long)nang * n > 65535)
+    throw std::invalid_argument("angles x beams exceeds 65535 stacked rows; split the scan");
   Pb.nang = nang;
   Pb.ld = ld;
   std::vector<cd> gam((size_t)nang * n), Dm((size_t)nang * ld, cd{0, 0}), F((size_t)nang * n * n);
@@ -331,53 +382,57 @@ void prepare(trhepd_context* C, const SolveArgs& A, trhepd_problem& Pb) {
   Pb.f2.ensure((size_t)nang * n * sizeof(double));
 }
 
-// Integrate every angle of a resident problem (surf_prkn.f90:278-330 batched over
-// angles); intensities land in Pb.f2 on the device.  Device time of the whole
-// sequence is recorded with events on the context stream.
-void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
-  const int n = Pb.n, ns = Pb.ns, nv = Pb.nv, nang = Pb.nang, ld = Pb.ld, kpad = ld;
-  const Integrator& I = Pb.I;
-  cudaStream_t st = C->stream;
-  const TableEntry* table = Pb.table.as<TableEntry>();
-  const int* d_pair = Pb.pair.as<int>();
-  const cd* d_gam = Pb.gam.as<cd>();
-  const cd* d_D = Pb.D.as<cd>();
-  const size_t sbytes = (size_t)nang * n * ld * sizeof(cd);
-  cd* Q = (cd*)C->Q0.ensure(sbytes);
-  cd* Qn = (cd*)C->Q1.ensure(sbytes);
-  cd* P = (cd*)C->P.ensure(sbytes);
-  cd* V = (cd*)C->V.ensure((size_t)(kpad + 1) * ld * sizeof(cd));
-  int* flags = (int*)C->flags.ensure(std::max(nang, 4) * sizeof(int));
-  double* dval = (double*)C->dval.ensure(std::max(nang, 4) * sizeof(double));
-  void* gjs = C->gj.ensure(gj_scratch_bytes(nang, n));
-  unsigned* status = (unsigned*)C->status.ensure(16);
-  const bool split = precision == TRHEPD_SPLIT_BF16;
+// Device buffers and counters of one integration of a resident problem.
+struct RunState {
+  int n = 0, ns = 0, nv = 0, nang = 0, ld = 0, kpad = 0;
+  bool split = false;
+  cudaStream_t st = nullptr;
+  const TableEntry* table = nullptr;
+  const int* pair = nullptr;
+  const cd* gam = nullptr;
+  const cd* D = nullptr;
+  size_t sbytes = 0;
+  cd *Q = nullptr, *Qn = nullptr, *P = nullptr, *V = nullptr;
+  int* flags = nullptr;
+  double* dval = nullptr;
+  void* gjs = nullptr;
+  unsigned* status = nullptr;
   SplitWorkspace sw{};
-  if (split)
-    sw = split_workspace_carve(C->split.ensure(split_workspace_bytes(nang, n, C->split_slices)),
-                               nang, n, C->split_slices, status, st);
-
-  CK(cudaEventRecord(C->ev0, st));
-  CK(cudaMemsetAsync(status, 0, 16, st));
-  CK(cudaMemsetAsync(Q, 0, sbytes, st));
-  CK(cudaMemsetAsync(Qn, 0, sbytes, st));
-  CK(cudaMemsetAsync(P, 0, sbytes, st));
-  // invstransh: Q = I + F^H, P = I - F^H; P <- Q^{-1} P; P <- i P conj(G); Q = I
-  launch_invstransh_build(Pb.F.as<cd>(), Q, P, nang, n, ld, st);
-  launch_gauss_jordan(Q, P, nullptr, nang, n, ld, gjs, status, st);
-  launch_invstransh_finish(P, d_gam, nang, n, ld, st);
-  launch_set_identity(Q, nullptr, nang, n, ld, st);
-
-  // renormalisation schedule
-  const bool every_slice = (n == 1 && Pb.int_method == 6);  // hp_int_spa1d renormalises each slice
-  int interval = 1;
-  if (C->renorm_policy == 1 && !every_slice) {
-    double kap = Pb.kappa_max + 1.0;
-    interval = std::max(1, (int)std::floor(C->renorm_tau / (kap * Pb.dz)));
-  }
+  int interval = 1;          // renormalisation interval of the growth-bound policy
   long renorms = 0, products = 0, launches = 0, gj_launches = 0;
-  const double dz = Pb.dz;
-  const int nprod_max = I.s * ns;
+  int gj_per = 0;
+};
+
+// Buffers, the boundary transform invstransh (matcomp.f90:140-172) and the
+// renormalisation schedule; Q = I and P = P0 afterwards.
+void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_max, RunState& R) {
+  R.n = Pb.n;
+  R.ns = Pb.ns;
+  R.nv = Pb.nv;
+  R.nang = Pb.nang;
+  R.ld = Pb.ld;
+  R.kpad = Pb.ld;
+  R.st = C->stream;
+  R.table = Pb.table.as<TableEntry>();
+  R.pair = Pb.pair.as<int>();
+  R.gam = Pb.gam.as<cd>();
+  R.D = Pb.D.as<cd>();
+  const int n = R.n, nang = R.nang, ld = R.ld;
+  cudaStream_t st = R.st;
+  R.sbytes = (size_t)nang * n * ld * sizeof(cd);
+  R.Q = (cd*)C->Q0.ensure(R.sbytes);
+  R.Qn = (cd*)C->Q1.ensure(R.sbytes);
+  R.P = (cd*)C->P.ensure(R.sbytes);
+  R.V = (cd*)C->V.ensure((size_t)(R.kpad + 1) * ld * sizeof(cd));
+  R.flags = (int*)C->flags.ensure(std::max(nang, 4) * sizeof(int));
+  R.dval = (double*)C->dval.ensure(std::max(nang, 4) * sizeof(double));
+  R.gjs = C->gj.ensure(gj_scratch_bytes(nang, n));
+  R.status = (unsigned*)C->status.ensure(16);
+  R.split = precision == TRHEPD_SPLIT_BF16;
+  if (R.split)
+    R.sw = split_workspace_carve(C->split.ensure(split_workspace_bytes(nang, n, C->split_slices)),
+                                 nang, n, C->split_slices, R.status, st);
+  R.gj_per = 2 * ceil_div(n, 16);
   if (C->profile && (int)C->evpool.size() < 2 * nprod_max) {
     while ((int)C->evpool.size() < 2 * nprod_max) {
       cudaEvent_t e;
@@ -385,89 +440,306 @@ void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
       C->evpool.push_back(e);
     }
   }
-  const int gj_per = 2 * ceil_div(n, 16);
-  for (int l = 1; l <= ns; ++l) {
+  CK(cudaEventRecord(C->ev0, st));
+  CK(cudaMemsetAsync(R.status, 0, 16, st));
+  CK(cudaMemsetAsync(R.Q, 0, R.sbytes, st));
+  CK(cudaMemsetAsync(R.Qn, 0, R.sbytes, st));
+  CK(cudaMemsetAsync(R.P, 0, R.sbytes, st));
+  // invstransh: Q = I + F^H, P = I - F^H; P <- Q^{-1} P; P <- i P conj(G); Q = I
+  launch_invstransh_build(Pb.F.as<cd>(), R.Q, R.P, nang, n, ld, st);
+  launch_gauss_jordan(R.Q, R.P, nullptr, nang, n, ld, R.gjs, R.status, st);
+  launch_invstransh_finish(R.P, R.gam, nang, n, ld, st);
+  launch_set_identity(R.Q, nullptr, nang, n, ld, st);
+  R.launches += 4 + R.gj_per;
+  if (C->renorm_policy == 1) {
+    double kap = Pb.kappa_max + 1.0;
+    R.interval = std::max(1, (int)std::floor(C->renorm_tau / (kap * Pb.dz)));
+  }
+}
+
+// Gather the stage matrix of table column `col` into R.V.
+void gather(RunState& R, int col, bool drop_diag) {
+  launch_gather_stage(R.table + (size_t)col * R.nv, R.pair, R.n, R.kpad, R.ld, drop_diag, R.V,
+                      R.st);
+  R.launches += 1;
+}
+
+// P += cb (Q M), Qo = Q + ca P with M from R.V (gathered for the chosen form).
+void stage_product(trhepd_context* C, RunState& R, const cd* Q, cd* P, cd* Qo, double cb,
+                   double ca) {
+  if (C->profile) CK(cudaEventRecord(C->evpool[2 * R.products], R.st));
+  if (R.split) {
+    R.launches += split_stage(R.sw, Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, cb, ca,
+                              C->split_slices, C->split_variant, R.st);
+  } else {
+    launch_stage_gemm_f64(Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, R.kpad, cb, ca, R.st);
+    R.launches += 1;
+  }
+  if (C->profile) CK(cudaEventRecord(C->evpool[2 * R.products + 1], R.st));
+  ++R.products;
+}
+
+// End-of-slice renormalisation: the reference's Gershgorin test per angle
+// (policy 0, cond_est matcomp.f90:498-528 > 1e3, matAbdivB :53-69) or the
+// growth bound every R.interval slices (policy 1); always on the last slice.
+void renormalise(trhepd_context* C, RunState& R, int l, bool every_slice) {
+  const bool last = (l == R.ns);
+  if (C->renorm_policy == 0 && !every_slice) {
+    launch_cond_est(R.Q, R.nang, R.n, R.ld, last ? 1 : 0, R.flags, R.dval, R.st);
+    launch_gauss_jordan(R.Q, R.P, R.flags, R.nang, R.n, R.ld, R.gjs, R.status, R.st);
+    launch_set_identity(R.Q, R.flags, R.nang, R.n, R.ld, R.st);
+    R.launches += 2 + R.gj_per;
+    R.gj_launches += R.gj_per;
+    if (!last) ++R.renorms;  // upper bound; per-angle decisions stay on the device
+  } else if (last || every_slice || (l % R.interval) == 0) {
+    launch_gauss_jordan(R.Q, R.P, nullptr, R.nang, R.n, R.ld, R.gjs, R.status, R.st);
+    launch_set_identity(R.Q, nullptr, R.nang, R.n, R.ld, R.st);
+    R.launches += 1 + R.gj_per;
+    R.gj_launches += R.gj_per;
+    if (!last) ++R.renorms;
+  }
+}
+
+// stransh (matcomp.f90:174-196), the intensities (surflf.f90:142-151) and the
+// status and timing of the whole run.
+void finish_run(trhepd_context* C, trhepd_problem& Pb, RunState& R) {
+  cudaStream_t st = R.st;
+  const int n = R.n, nang = R.nang, ld = R.ld;
+  launch_stransh_build(R.Q, R.P, R.gam, nang, n, ld, st);
+  launch_gauss_jordan(R.Q, R.P, nullptr, nang, n, ld, R.gjs, R.status, st);
+  launch_check_finite(R.P, (size_t)nang * n * ld, R.status, st);
+  launch_intensities(R.P, R.gam, Pb.wnsga2.as<double>(), nang, n, ld, Pb.nb0,
+                     Pb.f2.as<double>(), st);
+  R.launches += 3 + R.gj_per;
+  CK(cudaEventRecord(C->ev1, st));
+  CK(cudaGetLastError());
+  unsigned h_status[4];
+  CK(cudaMemcpyAsync(h_status, R.status, 16, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, C->ev0, C->ev1);
+  double prod_ms = 0.0;
+  if (C->profile)
+    for (long p = 0; p < R.products; ++p) {
+      float e = 0;
+      cudaEventElapsedTime(&e, C->evpool[2 * p], C->evpool[2 * p + 1]);
+      prod_ms += e;
+    }
+  C->stats[0] = (double)R.renorms;
+  C->stats[1] = (double)R.products;
+  C->stats[2] = ms;
+  C->stats[3] = (double)Pb.ncol;
+  C->stats[4] = prod_ms;
+  C->stats[5] = (double)R.launches;
+  C->stats[6] = (double)R.gj_launches;
+  if (h_status[0] & kStatusTimeout) throw CudaError("device wait timed out", TRHEPD_ETIMEOUT);
+  if (h_status[0] & (kStatusNonFinite | kStatusZeroPivot))
+    throw CudaError("non-finite value or zero pivot in the surface solve", TRHEPD_ENONFINITE);
+}
+
+// Symplectic RKN (hp_int_spa, surf_prkn.f90:278-330) batched over angles.
+void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision) {
+  const Integrator& I = Pb.I;
+  const double dz = Pb.dz;
+  RunState R;
+  begin_run(C, Pb, precision, I.s * Pb.ns, R);
+  const bool every_slice = (Pb.n == 1 && Pb.int_method == 6);  // hp_int_spa1d renormalises each slice
+  for (int l = 1; l <= R.ns; ++l) {
     for (int k = 1; k <= I.s; ++k) {
       const int col = I.s * (l - 1) + k - 1;
       const double ca = I.bab[2 * k - 1] * dz;
-      const TableEntry* tc = table + (size_t)col * nv;
       if (l == 1 && k == 1) {  // Q = I: elementwise stage
-        launch_gather_stage(tc, d_pair, n, kpad, ld, false, V, st);
-        launch_stage_identity(Q, P, V, d_D, nang, n, ld, I.bab[0] * dz, ca, st);
-        launches += 2;
+        gather(R, col, false);
+        launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, I.bab[0] * dz, ca, R.st);
+        R.launches += 1;
         continue;
       }
       // k == 1, l > 1 merges the end-of-slice half kick of slice l-1 (psave) with the
       // first kick of slice l: both use the same stage column, so cb = 2 b1.
       const double cb = (k == 1) ? 2.0 * I.bab[0] * dz : I.bab[2 * k - 2] * dz;
-      launch_gather_stage(tc, d_pair, n, kpad, ld, split, V, st);
-      if (C->profile) CK(cudaEventRecord(C->evpool[2 * products], st));
-      if (split) {
-        launches += split_stage(sw, Q, P, Qn, V, d_D, nang, n, ld, cb, ca, C->split_slices, st);
-      } else {
-        launch_stage_gemm_f64(Q, P, Qn, V, d_D, nang, n, ld, kpad, cb, ca, st);
-        launches += 1;
-      }
-      if (C->profile) CK(cudaEventRecord(C->evpool[2 * products + 1], st));
-      launches += 1;  // gather
-      std::swap(Q, Qn);
-      ++products;
+      gather(R, col, R.split);
+      stage_product(C, R, R.Q, R.P, R.Qn, cb, ca);
+      std::swap(R.Q, R.Qn);
     }
     // end of slice: renormalisation decision on Q (the reference tests Q after the
     // last stage; the end-of-slice kick does not change Q)
-    const bool last = (l == ns);
-    if (C->renorm_policy == 0 && !every_slice) {
-      launch_cond_est(Q, nang, n, ld, last ? 1 : 0, flags, dval, st);
-      launch_gauss_jordan(Q, P, flags, nang, n, ld, gjs, status, st);
-      launch_set_identity(Q, flags, nang, n, ld, st);
-      launches += 2 + gj_per;
-      gj_launches += gj_per;
-      if (!last) ++renorms;  // upper bound; per-angle decisions stay on the device
-    } else if (last || every_slice || (l % interval) == 0) {
-      launch_gauss_jordan(Q, P, nullptr, nang, n, ld, gjs, status, st);
-      launch_set_identity(Q, nullptr, nang, n, ld, st);
-      launches += 1 + gj_per;
-      gj_launches += gj_per;
-      if (!last) ++renorms;
-    }
+    renormalise(C, R, l, every_slice);
   }
   // final half kick with Q = I: P += b1 dz M(end)
-  {
-    const TableEntry* tc = table + (size_t)(I.s * ns) * nv;
-    launch_gather_stage(tc, d_pair, n, kpad, ld, false, V, st);
-    launch_stage_identity(Q, P, V, d_D, nang, n, ld, I.bab[0] * dz, 0.0, st);
+  gather(R, I.s * R.ns, false);
+  launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, I.bab[0] * dz, 0.0, R.st);
+  R.launches += 1;
+  finish_run(C, Pb, R);
+}
+
+// Stormer-Verlet leapfrog (lf_int_spa, surf_magnus.f90:46-110) batched over
+// angles: Q = I + dz/2 P, then per slice P += dz Q M(l), Q += dz P (dz/2 on the
+// last slice).  A renormalised Q = I enters the next product as the identity,
+// which gives the reference's Q = I shortcut exactly.
+void run_lf(trhepd_context* C, trhepd_problem& Pb, int precision) {
+  const double dz = Pb.dz;
+  RunState R;
+  begin_run(C, Pb, precision, Pb.ns, R);
+  gather(R, 0, false);  // any finite stage matrix: cb = 0 below
+  launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, 0.0, 0.5 * dz, R.st);
+  R.launches += 1;
+  for (int l = 1; l <= R.ns; ++l) {
+    const double dz2 = (l == R.ns) ? dz / 2 : dz;
+    gather(R, l - 1, R.split);
+    stage_product(C, R, R.Q, R.P, R.Qn, dz, dz2);
+    std::swap(R.Q, R.Qn);
+    renormalise(C, R, l, false);
   }
-  // stransh and intensities
-  launch_stransh_build(Q, P, d_gam, nang, n, ld, st);
-  launch_gauss_jordan(Q, P, nullptr, nang, n, ld, gjs, status, st);
-  launch_check_finite(P, (size_t)nang * n * ld, status, st);
-  launch_intensities(P, d_gam, Pb.wnsga2.as<double>(), nang, n, ld, Pb.nb0, Pb.f2.as<double>(),
-                     st);
-  CK(cudaEventRecord(C->ev1, st));
-  CK(cudaGetLastError());
-  unsigned h_status[4];
-  CK(cudaMemcpyAsync(h_status, status, 16, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  float ms = 0;
-  cudaEventElapsedTime(&ms, C->ev0, C->ev1);
-  launches += 4 + gj_per + 2 + 2 + 3 + gj_per + 2;  // boundary transforms, final kick, intensities
-  double prod_ms = 0.0;
-  if (C->profile)
-    for (long p = 0; p < products; ++p) {
-      float e = 0;
-      cudaEventElapsedTime(&e, C->evpool[2 * p], C->evpool[2 * p + 1]);
-      prod_ms += e;
+  finish_run(C, Pb, R);
+}
+
+// Classical RK4 on [Q | P] (rk4_int, surf_rk.f90:27-91) batched over angles:
+// k = (P', Q' M) at the stage points, each product Q' M formed by the stage
+// kernel into a zeroed buffer (cb = 1, ca = 0).
+void run_rk4(trhepd_context* C, trhepd_problem& Pb, int precision) {
+  const double dz = Pb.dz;
+  RunState R;
+  begin_run(C, Pb, precision, 4 * Pb.ns, R);
+  const size_t sb = R.sbytes;
+  cd* Qt = (cd*)C->rk[0].ensure(sb);
+  cd* Pt = (cd*)C->rk[1].ensure(sb);
+  cd* KP = (cd*)C->rk[2].ensure(sb);
+  cd* SQ = (cd*)C->rk[3].ensure(sb);
+  cd* SP = (cd*)C->rk[4].ensure(sb);
+  CK(cudaMemsetAsync(KP, 0, sb, R.st));
+  CK(cudaMemsetAsync(Qt, 0, sb, R.st));
+  CK(cudaMemsetAsync(Pt, 0, sb, R.st));
+  // stage j: (A, column, weight of k_j in the sum, step to the next stage point)
+  const double half = 0.5 * dz;
+  for (int l = 1; l <= R.ns; ++l) {
+    const int c0 = 2 * (l - 1), c1 = 2 * l - 1, c2 = 2 * l;
+    const int cols[4] = {c0, c1, c1, c2};
+    const double w[4] = {1.0, 2.0, 2.0, 1.0};
+    const double step[4] = {half, half, dz, 0.0};
+    for (int j = 0; j < 4; ++j) {
+      gather(R, cols[j], R.split);
+      stage_product(C, R, j == 0 ? R.Q : Qt, KP, R.Qn, 1.0, 0.0);
+      launch_rk4_combine(R.Q, R.P, Qt, Pt, KP, SQ, SP, j, w[j], step[j], dz / 6, R.nang, R.n,
+                         R.ld, R.st);
+      R.launches += 1;
     }
-  C->stats[0] = (double)renorms;
-  C->stats[1] = (double)products;
-  C->stats[2] = ms;
-  C->stats[3] = (double)Pb.ncol;
-  C->stats[4] = prod_ms;
-  C->stats[5] = (double)launches;
-  C->stats[6] = (double)gj_launches;
-  if (h_status[0] & kStatusTimeout) throw CudaError("device wait timed out", TRHEPD_ETIMEOUT);
-  if (h_status[0] & (kStatusNonFinite | kStatusZeroPivot))
-    throw CudaError("non-finite value or zero pivot in the surface solve", TRHEPD_ENONFINITE);
+    renormalise(C, R, l, false);
+  }
+  finish_run(C, Pb, R);
+}
+
+
+// Batched FP64 product C = A B (+ C) over the angles; a zero stride shares the operand.
+void bgemm(const cd* A, long long sA, const cd* B, long long sB, cd* Cm, long long sC, int n,
+           int ld, int beta, int batch, cudaStream_t st) {
+  BatchedGemm g{A, B, Cm, n, n, n, ld, ld, ld, sA, sB, sC, cd{1.0, 0.0}, beta, batch, nullptr};
+  launch_zgemm_batched(g, st);
+}
+
+// Magnus integrators m2/m4/m6 (m2_int_spa, m4_int_spa, m6_int_spa;
+// surf_magnus.f90:114-339) batched over angles.  Each slice forms q and rp from
+// hyperbolic_exp4r/6r of the stage matrices (magnus.cu), then P += Q rp and
+// Q += P q as batched GEMMs; after a renormalisation Q = I enters those products
+// as the identity.  Plain FP64 only.
+void run_magnus(trhepd_context* C, trhepd_problem& Pb, int precision) {
+  if (precision != TRHEPD_FP64)
+    throw std::invalid_argument("the Magnus integrators (int_method 1-3) run in plain FP64 only");
+  const double dz = Pb.dz;
+  const Family fam = Pb.I.family;
+  RunState R;
+  begin_run(C, Pb, precision, 0, R);
+  const int n = R.n, nang = R.nang, ld = R.ld;
+  cudaStream_t st = R.st;
+  const size_t sb = R.sbytes, vb = (size_t)(R.kpad + 1) * ld * sizeof(cd);
+  const long long sa = (long long)n * ld;
+  cd* Qq = (cd*)C->rk[0].ensure(sb);
+  cd* RPN = (cd*)C->rk[1].ensure(sb);
+  cd* RP = (cd*)C->rk[2].ensure(sb);
+  cd* R2 = (cd*)C->rk[3].ensure(sb);
+  cd* T = (cd*)C->rk[4].ensure(sb);
+  cd* RNEW = (cd*)C->mg[0].ensure(sb);
+  cd* V1 = (cd*)C->mg[1].ensure(vb);
+  cd* V3 = (cd*)C->mg[2].ensure(vb);
+  cd* S = (cd*)C->mg[3].ensure(vb);
+  cd* D13 = (cd*)C->mg[4].ensure(vb);
+  cd* S13 = (cd*)C->mg[5].ensure(vb);
+  cd* Wm = (cd*)C->mg[6].ensure(vb);
+  cd* Wp = (cd*)C->mg[7].ensure(vb);
+  cd* M3s = (cd*)C->mg[8].ensure(vb);
+  CK(cudaMemsetAsync(RP, 0, sb, st));
+  const cd* D = R.D;
+  auto gather_into = [&](int col, cd* dst) {
+    launch_gather_stage(R.table + (size_t)col * R.nv, R.pair, n, R.kpad, ld, false, dst, st);
+    R.launches += 1;
+  };
+  auto update_state = [&]() {  // P += Q RPN; Q += P Qq
+    bgemm(R.Q, sa, RPN, sa, R.P, sa, n, ld, 1, nang, st);
+    bgemm(R.P, sa, Qq, sa, R.Q, sa, n, ld, 1, nang, st);
+    R.launches += 2;
+    R.products += 2;
+  };
+  for (int l = 1; l <= R.ns; ++l) {
+    if (fam == kMagnus2) {
+      gather_into(l - 1, R.V);
+      bgemm(R.V, 0, R.V, 0, S, 0, n, ld, 0, 1, st);
+      launch_magnus4_step(R.V, S, nullptr, nullptr, D, nang, n, ld, dz, dz, 0.0, 0.0, Qq, RPN, RP,
+                          st);
+      R.launches += 2;
+      update_state();
+    } else if (fam == kMagnus4) {
+      const double c0 = std::sqrt(15.0) / 36, c1 = 5.0 / 36;
+      gather_into(3 * l - 3, V1);
+      gather_into(3 * l - 2, R.V);
+      gather_into(3 * l - 1, V3);
+      bgemm(R.V, 0, R.V, 0, S, 0, n, ld, 0, 1, st);
+      launch_magnus4_step(R.V, S, V1, V3, D, nang, n, ld, dz, dz, c0, c1, Qq, RPN, RP, st);
+      R.launches += 2;
+      update_state();
+    } else {  // kMagnus6
+      const double c0 = std::sqrt(15.0) / 180, c1 = 1.0 / 18, c2 = 1.0 / 12960;
+      const double d0 = 4.0 / (3.0 * std::sqrt(15.0)), d1 = 1.0 / 6;
+      const double h = dz / 2, c0dz = c0 * dz;
+      gather_into(3 * l - 3, V1);
+      gather_into(3 * l - 2, R.V);
+      gather_into(3 * l - 1, V3);
+      launch_magnus6_shared(V1, R.V, V3, n, ld, d0, d1, D13, S13, Wm, Wp, st);
+      bgemm(D13, 0, D13, 0, M3s, 0, n, ld, 0, 1, st);
+      launch_magnus6_m3(M3s, S13, c2 * (dz * dz * dz), c1 * dz, n, ld, st);
+      R.launches += 3;
+      // first half step: exponent of m2 - d0 m1
+      bgemm(Wm, 0, Wm, 0, S, 0, n, ld, 0, 1, st);
+      launch_magnus_square(S, Wm, D, nang, n, ld, R2, st);
+      bgemm(R2, sa, Wm, 0, T, sa, n, ld, 0, nang, st);
+      launch_magnus6_exp(Wm, D, R2, T, nang, n, ld, h, RP, D13, M3s, c0dz, Qq, RPN, RNEW, st);
+      R.launches += 4;
+      update_state();
+      // second half step: exponent of m2 + d0 m1, rp = r(first) + r(second)
+      bgemm(Wp, 0, Wp, 0, S, 0, n, ld, 0, 1, st);
+      launch_magnus_square(S, Wp, D, nang, n, ld, R2, st);
+      bgemm(R2, sa, Wp, 0, T, sa, n, ld, 0, nang, st);
+      launch_magnus6_exp(Wp, D, R2, T, nang, n, ld, h, RNEW, nullptr, nullptr, 0.0, Qq, RPN, RNEW,
+                         st);
+      R.launches += 4;
+      update_state();
+      launch_magnus6_carry(RNEW, D13, M3s, c0dz, nang, n, ld, RP, st);
+      R.launches += 1;
+    }
+    renormalise(C, R, l, false);
+  }
+  launch_add(R.P, RP, nang, n, ld, st);  // P += rp
+  R.launches += 1;
+  finish_run(C, Pb, R);
+}
+
+void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
+  switch (Pb.I.family) {
+    case kRkn: run_rkn(C, Pb, precision); break;
+    case kLeapfrog: run_lf(C, Pb, precision); break;
+    case kRk4: run_rk4(C, Pb, precision); break;
+    case kMagnus2:
+    case kMagnus4:
+    case kMagnus6: run_magnus(C, Pb, precision); break;
+  }
 }
 
 void fetch(trhepd_context* C, trhepd_problem& Pb, double* f2, double* angle_deg) {
@@ -923,6 +1195,11 @@ int trhepd_set_option(trhepd_context* c, int option, double value) {
       return TRHEPD_OK;
     case TRHEPD_OPT_PROFILE:
       c->profile = value != 0.0;
+      return TRHEPD_OK;
+    case TRHEPD_OPT_SPLIT_KERNEL:
+      if (value != kSplitPersistent && value != kSplitPerTile)
+        return fail(c, TRHEPD_EINVAL, "split kernel must be 0 (persistent) or 1 (per tile)");
+      c->split_variant = (int)value;
       return TRHEPD_OK;
   }
   return fail(c, TRHEPD_EINVAL, "unknown option");

@@ -28,6 +28,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -209,18 +210,27 @@ __global__ void k_slice_rows(const cd* __restrict__ Q, int rows, int n, int ld, 
   }
 }
 
-// Column exponents of Voff (thread per complex column).
-__global__ void k_col_exponents(const cd* __restrict__ V, int n, int ld, int* __restrict__ fcol) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
+// Column exponents of Voff: 32 columns per block, the 8 warps split the rows
+// (lanes read consecutive columns), then a shared-memory maximum.
+__global__ void __launch_bounds__(256) k_col_exponents(const cd* __restrict__ V, int n, int ld,
+                                                       int* __restrict__ fcol) {
+  __shared__ double red[8][33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int j = blockIdx.x * 32 + lane;
   double m = 0.0;
-  for (int k = 0; k < n; ++k) {
-    cd v = V[(size_t)k * ld + j];
-    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  if (j < n)
+    for (int k = w; k < n; k += 8) {
+      cd v = V[(size_t)k * ld + j];
+      m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    }
+  red[w][lane] = m;
+  __syncthreads();
+  if (w == 0 && j < n) {
+    for (int q = 1; q < 8; ++q) m = fmax(m, red[q][lane]);
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);
+    fcol[j] = e;
   }
-  int e = 0;
-  if (m > 0.0) frexp(m, &e);
-  fcol[j] = e;
 }
 
 // B^T slices: row 2j (Re-out) = [Vr(k,j), -Vi(k,j)]_k, row 2j+1 (Im-out) = [Vi, Vr]_k.
@@ -248,6 +258,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     k_split_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  EpiArgs ep, int nkb) {
   constexpr int STAGES = stages_for(S);
+  // an earlier launch gave up on a wait: skip the work, the host reports it
+  if (*(volatile unsigned*)ep.status & kStatusTimeout) return;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -403,6 +415,303 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
+// ------------------------------------------------------------ persistent form
+// One CTA per SM walks the tiles (static stride) with the mainloop and the three
+// accumulators of the per-tile form (s+t = 0, 1, >= 2; 384 TMEM columns).  Eight
+// epilogue warps (two per TMEM lane quadrant, one per 32-column half) drain a
+// finished tile with 16x256b TMEM loads, which hand each lane complex values in
+// column-coalesced position (rows t/4 and t/4 + 8 of a 16-row block, complex
+// column t%4 of a 4-column group), keep them in registers as scaled FP64 and give
+// the TMEM back at once; the MMAs of the next tile then run while the same warps
+// perform the HBM-bound RKN update from registers.  The register file is split
+// with setmaxnreg: the control warpgroup (TMA, MMA, two idle warps) drops to
+// P_REG_CTRL, the two epilogue warpgroups rise to P_REG_EPI.
+constexpr int P_THREADS = 384;   // warps 0 TMA, 1 MMA, 2-3 idle, 4-11 epilogue
+constexpr int P_EPI_WARPS = 8;
+constexpr int P_REG_LAUNCH = 168;  // registers per thread the launch must provide
+constexpr int P_REG_CTRL = 40;
+constexpr int P_REG_EPI = 232;
+static_assert(128 * P_REG_CTRL + 256 * P_REG_EPI <= P_THREADS * P_REG_LAUNCH,
+              "setmaxnreg split exceeds the launch's registers");
+__host__ __device__ constexpr int pstages_for(int S) { return stages_for(S); }
+inline size_t psmem_bytes(int S) { return smem_bytes(S); }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ int ld_volatile(const int* p) { return *(const volatile int*)p; }
+// 2^e as a double: exact bit construction in the normal range, ldexp outside it.
+__device__ __forceinline__ double pow2(int e) {
+  return (e > -1022 && e < 1023) ? __longlong_as_double((long long)(e + 1023) << 52)
+                                 : ldexp(1.0, e);
+}
+// 16 TMEM lanes x 256 bits: r0, r1 = lane t/4, 32-bit columns 2(t%4), 2(t%4)+1;
+// r2, r3 = the same columns of lane t/4 + 8.
+__device__ __forceinline__ void tmem_ld_16x256(uint32_t taddr, uint32_t* v) {
+  asm volatile("tcgen05.ld.sync.aligned.16x256b.x1.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+               : "r"(taddr));
+}
+// Named barrier of the epilogue warps returning whether any thread passed
+// fail != 0, so that all of them take the same branch afterwards.
+__device__ __forceinline__ bool epi_any(int fail) {
+  uint32_t any;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.s32 q, %1, 0;\n\t"
+      "bar.red.or.pred p, 1, %2, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(any)
+      : "r"(fail), "n"(32 * P_EPI_WARPS)
+      : "memory");
+  return any != 0;
+}
+
+template <int S>
+__global__ void __launch_bounds__(P_THREADS, 1)
+    k_split_gemm_p(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   EpiArgs ep, int nkb, int tiles_n, int tiles) {
+  constexpr int STAGES = pstages_for(S);
+  // an earlier launch gave up on a wait: skip the work, the host reports it
+  if (*(volatile unsigned*)ep.status & kStatusTimeout) return;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], tfull, tempty, drain_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh, issued_sh, consumed_sh;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t sbytes = stage_bytes(S);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&tfull, 1);
+    mbar_init(&tempty, P_EPI_WARPS);
+    mbar_init(&drain_bar, 1);
+    abort_sh = 0;
+    issued_sh = 0;
+    consumed_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_sh)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+
+  if (warp < 4) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(P_REG_CTRL));
+  if (warp == 0) {
+    // ---------------- TMA producer
+    if (lane == 0) {
+      int g = 0;
+      bool stop = false;
+      for (int tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x) {
+        const int m0 = (tile / tiles_n) * BM, n0 = (tile % tiles_n) * NT;
+        for (int kb = 0; kb < nkb; ++kb, ++g) {
+          const int st = g % STAGES, round = g / STAGES;
+          if (round > 0 && !mbar_wait(&empty_bar[st], (round - 1) & 1)) {
+            atomicOr(ep.status, kStatusTimeout);
+            abort_sh = 1;
+            stop = true;
+            break;
+          }
+          if (ld_volatile(&abort_sh)) {
+            stop = true;
+            break;
+          }
+          unsigned char* sa = smem + st * sbytes;
+          unsigned char* sb = sa + S * A_SLICE_BYTES;
+          mbar_expect_tx(&full_bar[st], (uint32_t)sbytes);
+#pragma unroll
+          for (int s = 0; s < S; ++s) {
+            tma_load_3d(&tmA, &full_bar[st], sa + s * A_SLICE_BYTES, kb * BK, m0, s);
+            tma_load_3d(&tmB, &full_bar[st], sb + s * B_SLICE_BYTES, kb * BK, n0, s);
+          }
+        }
+      }
+      issued_sh = g;
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = instr_desc();
+      int g = 0, it = 0;
+      bool stop = false;
+      for (int tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x, ++it) {
+        // the accumulators of the previous tile must have been drained
+        if (it > 0 && !mbar_wait(&tempty, (it - 1) & 1)) {
+          atomicOr(ep.status, kStatusTimeout);
+          abort_sh = 1;
+          break;
+        }
+        tc_fence_after();
+        bool started[NACC] = {false, false, false};
+        for (int kb = 0; kb < nkb; ++kb, ++g) {
+          const int st = g % STAGES, round = g / STAGES;
+          if (!mbar_wait(&full_bar[st], round & 1)) {
+            atomicOr(ep.status, kStatusTimeout);
+            abort_sh = 1;
+            stop = true;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(smem + st * sbytes);
+          const uint32_t sb = sa + S * A_SLICE_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+#pragma unroll
+              for (int t = 0; t < S - s; ++t) {
+                const int acc = (s + t < 2) ? s + t : 2;
+                const uint64_t ad = sw64_desc(sa + s * A_SLICE_BYTES + kk * 32);
+                const uint64_t bd = sw64_desc(sb + t * B_SLICE_BYTES + kk * 32);
+                tc_mma(tmem + acc * NT, ad, bd, idesc, started[acc] ? 1u : 0u);
+                started[acc] = true;
+              }
+            }
+          }
+          tc_commit(&empty_bar[st]);
+        }
+        if (stop) break;
+        tc_commit(&tfull);
+      }
+      consumed_sh = g;
+      // no MMA may still be running when the TMEM is released
+      tc_commit(&drain_bar);
+      if (!mbar_wait(&drain_bar, 0)) atomicOr(ep.status, kStatusTimeout);
+    }
+  }
+  } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(P_REG_EPI));
+    // ---------------- epilogue warps 4..11
+    const int q4 = warp & 3;                 // TMEM lane quadrant
+    const int half = (warp - 4) >> 2;        // 32-complex-column half of the tile
+    const int t0 = lane & 3, t1 = lane >> 2;
+    const cd vd = ep.V[(size_t)ep.kpad * ep.ld];
+    int it = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
+      const int m0 = (tile / tiles_n) * BM + q4 * 32;          // first row of this quadrant
+      const int jh = (tile % tiles_n) * NC + half * (NC / 2);  // first complex column
+      // this lane's rows m0 + 16h + 8u + t1 and columns jh + 4g + t0
+      int er[2][2], ra[2][2], ri[2][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int r = m0 + 16 * h + 8 * u + t1;
+          er[h][u] = 0;
+          ra[h][u] = 0;
+          ri[h][u] = 0;
+          if (r < ep.rows) {
+            er[h][u] = ep.erow[r];
+            ra[h][u] = r / ep.n;
+            ri[h][u] = r - ra[h][u] * ep.n;
+          }
+        }
+      int fc[8];
+#pragma unroll
+      for (int g = 0; g < 8; ++g) {
+        const int j = jh + 4 * g + t0;
+        fc[g] = (j < ep.n) ? ep.fcol[j] : 0;
+      }
+      const bool ok = mbar_wait(&tfull, it & 1);
+      if (epi_any(!ok)) {  // uniform across the epilogue warps
+        if (!ok) atomicOr(ep.status, kStatusTimeout);
+        abort_sh = 1;
+        break;
+      }
+      tc_fence_after();
+      // drain: (acc2 + acc1) + acc0 in FP64 (the order of the per-tile form),
+      // scaled exactly by 2^(e_r + f_j - 14)
+      cd vals[8][2][2];
+#pragma unroll
+      for (int g = 0; g < 8; ++g)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t taddr = tmem + ((uint32_t)(q4 * 32 + 16 * h) << 16) +
+                                 (uint32_t)(2 * (half * (NC / 2) + 4 * g));
+          uint32_t a2[4], a1[4], a0[4];
+          tmem_ld_16x256(taddr + 2 * NT, a2);
+          tmem_ld_16x256(taddr + 1 * NT, a1);
+          tmem_ld_16x256(taddr + 0 * NT, a0);
+          tmem_wait_ld();
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const double re = (double)__uint_as_float(a2[2 * u]) +
+                              (double)__uint_as_float(a1[2 * u]) +
+                              (double)__uint_as_float(a0[2 * u]);
+            const double im = (double)__uint_as_float(a2[2 * u + 1]) +
+                              (double)__uint_as_float(a1[2 * u + 1]) +
+                              (double)__uint_as_float(a0[2 * u + 1]);
+            const double sc = pow2(er[h][u] + fc[g] - 14);
+            vals[g][h][u] = cd{re * sc, im * sc};
+          }
+        }
+      // the accumulators are in registers: let the next tile's MMAs start
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty);
+      // RKN update from registers; each warp access covers 8 rows x 4 columns
+#pragma unroll
+      for (int g = 0; g < 8; ++g) {
+        const int j = jh + 4 * g + t0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          cd qv[2], pv[2], qd[2], vv[2], dv[2];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int r = m0 + 16 * h + 8 * u + t1;
+            if (r < ep.rows && j < ep.n) {
+              const size_t ro = (size_t)r * ep.ld;
+              qv[u] = ep.Q[ro + j];
+              pv[u] = ep.P[ro + j];
+              qd[u] = ep.Q[ro + ri[h][u]];
+              vv[u] = ep.V[(size_t)ri[h][u] * ep.ld + j];
+              dv[u] = ep.D[(size_t)ra[h][u] * ep.ld + j];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int r = m0 + 16 * h + 8 * u + t1;
+            if (r < ep.rows && j < ep.n) {
+              const size_t ro = (size_t)r * ep.ld;
+              const cd acc = vals[g][h][u] + qd[u] * vv[u] + qv[u] * (dv[u] + vd);
+              const cd p = pv[u] + ep.cb * acc;
+              ep.P[ro + j] = p;
+              ep.Qo[ro + j] = qv[u] + ep.ca * p;
+            }
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // bulk copies issued but never consumed (only after a timeout) must land
+    // before the CTA exits
+    for (int g = consumed_sh; g < issued_sh; ++g)
+      if (!mbar_wait(&full_bar[g % STAGES], (g / STAGES) & 1)) break;
+  }
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS));
+  }
+}
+
 }  // namespace split
 
 // ============================================================ host side
@@ -455,27 +764,36 @@ EncodeTiled encoder() {
   return fn;
 }
 
-// 3-D map over [S][rows][kr] BF16 with a (32 x 128 x 1) box and 64-byte swizzle.
-CUtensorMap make_map(void* base, int kr, int rows, int S) {
+// 3-D map over [S][rows][kr] BF16 with a (bk x 128 x 1) box: bk = 32 with 64-byte
+// swizzle (both kernel forms) or bk = 16 with 32-byte swizzle.
+CUtensorMap make_map(void* base, int kr, int rows, int S, int bk = split::BK) {
   CUtensorMap m;
   cuuint64_t dims[3] = {(cuuint64_t)kr, (cuuint64_t)rows, (cuuint64_t)S};
   cuuint64_t strides[2] = {(cuuint64_t)kr * 2, (cuuint64_t)kr * 2 * rows};
-  cuuint32_t box[3] = {split::BK, split::BM, 1};
+  cuuint32_t box[3] = {(cuuint32_t)bk, split::BM, 1};
   cuuint32_t estr[3] = {1, 1, 1};
+  const CUtensorMapSwizzle sw = (bk == 32) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
   CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
   return m;
 }
 
+int sm_count() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 148;
+}
+
 template <int S>
 void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
-               int nang, int n, int ld, double cb, double ca, cudaStream_t st) {
+               int nang, int n, int ld, double cb, double ca, int variant, cudaStream_t st) {
   Carve c = carve(w.base, nang, n, S);
   const int kr = 2 * c.kc;
   // slices of the shared potential matrix (one set for every angle)
-  split::k_col_exponents<<<ceil_div(n, 128), 128, 0, st>>>(V, n, ld, c.fcol);
+  split::k_col_exponents<<<ceil_div(n, 32), 256, 0, st>>>(V, n, ld, c.fcol);
   {
     dim3 grid(ceil_div(c.kc, 128), n);
     split::k_slice_cols<S><<<grid, 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, c.B);
@@ -485,15 +803,38 @@ void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V,
   CUtensorMap ta = make_map(c.A, kr, c.rows, S);
   CUtensorMap tb = make_map(c.B, kr, c.nrows, S);
   split::EpiArgs ep{Q, P, Qo, V, D, c.erow, c.fcol, w.status, c.rows, n, ld, c.kc, S, cb, ca};
-  const size_t smem = split::smem_bytes(S);
-  static bool attr[6] = {false, false, false, false, false, false};
-  if (!attr[S]) {
-    cudaFuncSetAttribute(split::k_split_gemm<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    attr[S] = true;
+  const int tiles_n = c.nrows / split::NT, tiles_m = ceil_div(c.rows, split::BM);
+  if (variant == kSplitPersistent) {
+    const size_t smem = split::psmem_bytes(S);
+    static bool attr[6] = {false, false, false, false, false, false};
+    if (!attr[S]) {
+      // setmaxnreg redistributes the registers the block was launched with: the
+      // kernel must have been built with the count the split assumes
+      cudaFuncAttributes fa{};
+      if (cudaFuncGetAttributes(&fa, split::k_split_gemm_p<S>) != cudaSuccess ||
+          fa.numRegs < split::P_REG_LAUNCH)
+        throw std::runtime_error("persistent split kernel built with " +
+                                 std::to_string(fa.numRegs) + " registers per thread, needs " +
+                                 std::to_string(split::P_REG_LAUNCH));
+      cudaFuncSetAttribute(split::k_split_gemm_p<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      attr[S] = true;
+    }
+    const int tiles = tiles_n * tiles_m;
+    const int grid = std::min(tiles, sm_count());
+    split::k_split_gemm_p<S><<<grid, split::P_THREADS, smem, st>>>(ta, tb, ep, kr / split::BK,
+                                                                   tiles_n, tiles);
+  } else {
+    const size_t smem = split::smem_bytes(S);
+    static bool attr[6] = {false, false, false, false, false, false};
+    if (!attr[S]) {
+      cudaFuncSetAttribute(split::k_split_gemm<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      attr[S] = true;
+    }
+    dim3 grid(tiles_n, tiles_m);
+    split::k_split_gemm<S><<<grid, split::THREADS, smem, st>>>(ta, tb, ep, kr / split::BK);
   }
-  dim3 grid(c.nrows / split::NT, ceil_div(c.rows, split::BM));
-  split::k_split_gemm<S><<<grid, split::THREADS, smem, st>>>(ta, tb, ep, kr / split::BK);
 }
 
 }  // namespace
@@ -517,16 +858,19 @@ SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, un
 }
 
 int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
-                int nang, int n, int ld, double cb, double ca, int slices, cudaStream_t st) {
+                int nang, int n, int ld, double cb, double ca, int slices, int variant,
+                cudaStream_t st) {
+  if (variant != kSplitPersistent && variant != kSplitPerTile)
+    throw std::invalid_argument("unknown split kernel variant");
   switch (slices) {
     case 3:
-      run_split<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, st);
+      run_split<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, variant, st);
       break;
     case 4:
-      run_split<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, st);
+      run_split<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, variant, st);
       break;
     case 5:
-      run_split<5>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, st);
+      run_split<5>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, variant, st);
       break;
     default:
       throw std::invalid_argument("split slices must be 3, 4 or 5");

@@ -17,9 +17,17 @@ size_t split_workspace_bytes(int nang, int n, int slices);
 SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, unsigned* status,
                                      cudaStream_t st);
 
+// Tensor-core kernel forms of the stage product.
+//   kSplitPersistent: one CTA per SM over all tiles; the accumulators of a tile
+//     are drained to registers and the FP64 update runs during the next tile's MMAs;
+//   kSplitPerTile: one CTA per tile, the epilogue after the tile's MMAs.
+// Both use three FP32 accumulators (slice pairs with s+t = 0, 1, >= 2).
+enum SplitVariant { kSplitPersistent = 0, kSplitPerTile = 1 };
+
 // P += cb*(Q V + Q o D_a) with the potential product from BF16 slices; Qo = Q + ca*P.
 // Returns the number of kernels launched.
 int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
-                 int nang, int n, int ld, double cb, double ca, int slices, cudaStream_t st);
+                int nang, int n, int ld, double cb, double ca, int slices, int variant,
+                cudaStream_t st);
 
 }  // namespace trhepd

@@ -21,6 +21,7 @@ OPT_RENORM_POLICY = 1
 OPT_RENORM_TAU = 2
 OPT_SPLIT_SLICES = 3
 OPT_PROFILE = 4
+OPT_SPLIT_KERNEL = 5
 
 # every symbol include/trhepd_b200.h declares
 EXPORTS = [

@@ -205,9 +205,11 @@ def summarize(stream: list[Request], wall: float) -> dict:
 
 
 def isolated_times(server: Server, cases: list[tuple[int, int]], reps: int = 1) -> dict:
-    """Latency of each (N, angle grid) request solved alone on an idle server."""
+    """Latency of each (N, angle grid) request solved alone on an idle server
+    (best of `reps`; the inputs of the base structure are prepared beforehand)."""
     out = {}
     for n, g in cases:
+        server._bulk(n, g)
         best = None
         for k in range(reps):
             r = Request(rid=10**9 + len(out) * 10 + k, n=n, n_angles=g, sigma=0.1, seed=k)
@@ -215,7 +217,26 @@ def isolated_times(server: Server, cases: list[tuple[int, int]], reps: int = 1) 
             r.arrival = t0 - server.t0
             server.submit(r)
             server.q.join()
+            if r.error is not None:
+                raise RuntimeError(f"isolated request N={n} grid={g}: {r.error}")
             dt = time.perf_counter() - t0
             best = dt if best is None else min(best, dt)
         out[(n, g)] = best
     return out
+
+
+def slowdowns(stream: list[Request], isolated: dict) -> dict:
+    """Latency in the mix over the isolated solve time of the same (N, grid)."""
+    ratios = np.array([r.latency / isolated[(r.n, r.n_angles)] for r in stream
+                       if r.error is None and r.finish > 0 and (r.n, r.n_angles) in isolated])
+    if not len(ratios):
+        return {"count": 0}
+    return {"count": int(len(ratios)), "p50": float(np.percentile(ratios, 50)),
+            "p99": float(np.percentile(ratios, 99)), "max": float(ratios.max())}
+
+
+def expected_busy_seconds(isolated: dict, mix=None, grids=GRIDS) -> float:
+    """Mean isolated solve time of one request drawn from the mix."""
+    mix = mix or DEFAULT_MIX
+    tot = sum(mix.values())
+    return sum(w / tot * np.mean([isolated[(n, g)] for g in grids]) for n, w in mix.items())

@@ -45,8 +45,7 @@ class SurfaceProblem:
     def potential_table(self, int_method: int | None = None):
         """Stage potential tables v, vi as (ncol, nv) complex arrays."""
         m = self.args.int_method if int_method is None else int_method
-        s = {5: 6, 6: 11}[m]
-        ncol = s * self.args.ns + 1
+        ncol = table_columns(m, self.args.ns)
         v = np.zeros((ncol, self.pot.nv), dtype=np.complex128)
         vi = np.zeros_like(v)
         nc = ctypes.c_int(0)
@@ -70,6 +69,16 @@ class SurfaceProblem:
             self.close()
         except Exception:
             pass
+
+
+def table_columns(int_method: int, ns: int) -> int:
+    """Stage-table columns of each integrator's init routine (surf_prkn.f90:174-197,
+    surf_magnus.f90:4-42, surf_rk.f90:4-25)."""
+    per = {1: (1, 0), 2: (3, 0), 3: (3, 0), 4: (1, 0), 5: (6, 1), 6: (11, 1), 7: (2, 1)}
+    if int_method not in per:
+        raise ValueError("the GPU path integrates int_method 1 to 7")
+    s, extra = per[int_method]
+    return s * ns + extra
 
 
 def potential_table(ctx: native.Context, bulkp, surf, dz2: float, int_method: int = 5):
