@@ -12,9 +12,13 @@
 //                                               s = sin(sqrt(H) dz)/sqrt(H).
 // C and s come from a degree-8 Taylor series in X = -H h^2 on h = dz / 2^m
 // (||X|| <= 1/4) followed by m double-angle steps C <- 2C^2 - I, s <- 2 s C:
-// batched complex GEMMs, no eigensolver.  Slices are chained in w-space and
-// converted once; then the layer recursion R <- (T12 + T11 R)(T22 + T21 R)^-1
-// with the reference's convergence exit (bulk.f90:95-119).
+// batched complex GEMMs, no eigensolver.  Each slice's propagator is converted
+// to mode space and the slices are chained there, as the reference chains its
+// slice transfer matrices (bulk.f90:67-79): chaining in w-space and converting
+// once would form the decaying blocks of strongly evanescent beams (e^{-kappa c},
+// ~1e-20 over a layer) as differences of ~1e20 entries.  Then the layer
+// recursion R <- (T12 + T11 R)(T22 + T21 R)^-1 with the reference's convergence
+// exit (bulk.f90:95-119).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -237,8 +241,8 @@ __global__ void k_bulk_build_e(const cd* __restrict__ C, const cd* __restrict__ 
   }
 }
 
-// T = S E S^-1 (see file header) and the unit-layer phase shift of columns j, j+n
-// (bulk.f90:83-93); padded beams use gamma = 1.
+// T = S E S^-1 (see file header), times the unit-layer phase shift of columns
+// j, j+n (bulk.f90:83-93) when `phase` is given; padded beams use gamma = 1.
 __global__ void k_bulk_similarity(const cd* __restrict__ E, const cd* __restrict__ gam,
                                   const cd* __restrict__ phase, const int* __restrict__ gsize,
                                   int ngr, int n, int ld2, int batch, cd* __restrict__ T) {
@@ -258,12 +262,30 @@ __global__ void k_bulk_similarity(const cd* __restrict__ E, const cd* __restrict
     cd A = gi * e11 - I * e21, B = gi * e12 - I * e22;
     cd Cc = gi * e11 + I * e21, D = gi * e12 + I * e22;
     cd ig = cdiv(cd{1.0, 0.0}, gj);
-    cd ph = (j < m) ? phase[b * n + j] : cd{1.0, 0.0};
+    cd ph = (phase && j < m) ? phase[b * n + j] : cd{1.0, 0.0};
     cd* Tb = T + b * 2 * n * ld2;
     Tb[(size_t)i * ld2 + j] = ph * (0.5 * (A * ig + I * B));
     Tb[(size_t)i * ld2 + n + j] = ph * (0.5 * (A * ig - I * B));
     Tb[(size_t)(n + i) * ld2 + j] = ph * (0.5 * (Cc * ig + I * D));
     Tb[(size_t)(n + i) * ld2 + n + j] = ph * (0.5 * (Cc * ig - I * D));
+  }
+}
+
+// Unit-layer phase shift (bulk.f90:83-93): columns j and j+n of T times ph_j.
+__global__ void k_bulk_phase_cols(cd* __restrict__ T, const cd* __restrict__ phase,
+                                  const int* __restrict__ gsize, int ngr, int n, int ld2,
+                                  int batch) {
+  size_t total = (size_t)batch * 2 * n * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    size_t b = e / ((size_t)2 * n * n);
+    int r = (int)(e % ((size_t)2 * n * n));
+    int i = r / n, j = r % n;
+    if (j >= gsize[b % ngr]) continue;
+    const cd ph = phase[b * n + j];
+    cd* Tb = T + b * 2 * n * ld2 + (size_t)i * ld2;
+    Tb[j] = ph * Tb[j];
+    Tb[n + j] = ph * Tb[n + j];
   }
 }
 
@@ -372,6 +394,11 @@ void launch_bulk_similarity(const cd* E, const cd* gam, const cd* phase, const i
                             int n, int ld2, int batch, cd* T, cudaStream_t st) {
   size_t total = (size_t)batch * n * n;
   k_bulk_similarity<<<grid_for(total), 256, 0, st>>>(E, gam, phase, gsize, ngr, n, ld2, batch, T);
+}
+void launch_bulk_phase_cols(cd* T, const cd* phase, const int* gsize, int ngr, int n, int ld2,
+                            int batch, cudaStream_t st) {
+  size_t total = (size_t)batch * 2 * n * n;
+  k_bulk_phase_cols<<<grid_for(total), 256, 0, st>>>(T, phase, gsize, ngr, n, ld2, batch);
 }
 void launch_bulk_layer_init(const cd* T, const int* active, int n, int ld, int ld2, int batch,
                             cd* t1, cd* t2, cudaStream_t st) {

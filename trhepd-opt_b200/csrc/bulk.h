@@ -34,6 +34,8 @@ void launch_bulk_build_e(const cd* C, const cd* S, const cd* Hs, int n, int ld, 
                          cd* E, cudaStream_t st);
 void launch_bulk_similarity(const cd* E, const cd* gam, const cd* phase, const int* gsize, int ngr,
                             int n, int ld2, int batch, cd* T, cudaStream_t st);
+void launch_bulk_phase_cols(cd* T, const cd* phase, const int* gsize, int ngr, int n, int ld2,
+                            int batch, cudaStream_t st);
 void launch_bulk_layer_init(const cd* T, const int* active, int n, int ld, int ld2, int batch,
                             cd* t1, cd* t2, cudaStream_t st);
 void launch_bulk_transpose_pair(const cd* t1, const cd* t2, const int* active, const int* gsize,

@@ -892,7 +892,7 @@ void bulk_solve(trhepd_context* C, BulkInputs& B, std::vector<std::vector<cd>>& 
   auto buf2 = [&](int k) { return (cd*)C->bk[k].ensure(nb2 * sizeof(cd)); };
   cd *H = buf1(0), *X = buf1(1), *X2 = buf1(2), *X3 = buf1(3), *X4 = buf1(4), *Cm = buf1(5);
   cd *Sm = buf1(6), *T1 = buf1(7), *T2 = buf1(8), *Hs = buf1(9);
-  cd *E = buf2(10), *Et = buf2(11), *En = buf2(12);
+  cd *E = buf2(10), *Et = buf2(11), *En = buf2(12), *Tl = buf2(18);
   if (nitem > 65535) throw std::invalid_argument("too many (angle, group) items for one bulk batch");
   // per-item matrices: n x n at ld (stride s1) or 2n x 2n at ld2 (stride s2)
   const long long s1 = (long long)n * ld, s2 = (long long)n2 * ld2;
@@ -943,14 +943,16 @@ void bulk_solve(trhepd_context* C, BulkInputs& B, std::vector<std::vector<cd>>& 
       launch_bulk_axpby(Sm, T2, 0.0, 2.0, 0.0, n, ld, nitem, st);
     }
     gemm1(H, Sm, Hs, 0, nullptr);
-    launch_bulk_build_e(Cm, Sm, Hs, n, ld, ld2, nitem, l == 0 ? Et : E, st);
-    if (l > 0) {  // E_tot <- E_l E_tot
-      gemm2(E, Et, En);
+    launch_bulk_build_e(Cm, Sm, Hs, n, ld, ld2, nitem, E, st);
+    // slice transfer matrix T_l = S E_l S^-1 (trmat), then T_tot <- T_l T_tot
+    launch_bulk_similarity(E, d_gam, nullptr, d_gsize, ngr, n, ld2, nitem, l == 0 ? Et : Tl, st);
+    if (l > 0) {
+      gemm2(Tl, Et, En);
       std::swap(Et, En);
     }
   }
-  cd* Tm = En;  // the free 2n buffer receives T = S E S^-1
-  launch_bulk_similarity(Et, d_gam, d_ph, d_gsize, ngr, n, ld2, nitem, Tm, st);
+  cd* Tm = Et;  // unit-layer transfer matrix
+  if (shifted) launch_bulk_phase_cols(Tm, d_ph, d_gsize, ngr, n, ld2, nitem, st);
   // layer recursion with the convergence exit
   std::vector<int> act(nitem, 1);
   int* d_act = upload(C->bk[13], act, st);
