@@ -5,13 +5,16 @@ Workload (default ``dense521``): synthetic 2x2 Si/Ge surface over a 4-atom
 bulk, N = 521 beams, 61 glancing angles (0.5..6.5 deg), 2004 slices of
 0.01 A, symplectic RKN-4 (int_method 5).  One step = one solve of all 61 angles.
 
-* ``value``: split-precision (BF16 slices on tcgen05) when available, else the
-  plain FP64 form, with inputs resident in HBM (trhepd_problem_solve), device
-  time from CUDA events on the library stream, max over ranks.
+* ``value``: the split-precision form (default: 4 signed 8-bit digit slices per
+  operand on tcgen05 kind::i8 with exact INT32 accumulation; ``--precision``
+  bf16 / fp64 select the other forms), inputs resident in HBM
+  (trhepd_problem_solve), device time from CUDA events on the library stream,
+  max over ranks.
 * ``e2e``: the same metric through the C ABI with host buffers
   (trhepd_srfref: uploads, stage-table build, solve, intensities back).
-* ``fp64``: the plain FP64 form of the same workload for comparison.
-* ``roofline``: the stage-product kernel, live event timing of every launch.
+* ``fp64``: the plain FP64 form of the same workload, its speed and the split
+  form's error against it; ``bf16_split``: the BF16-slice form beside it.
+* ``roofline``: the tensor-core stage kernel, live event timing of every launch.
 * ``cpu_baseline``: the CPU oracle (C++ restatement of the reference path,
   OpenMP over angles, OpenBLAS) on a bounded sample of the workload.
 
@@ -56,6 +59,9 @@ from trhepd_opt_b200 import build as tbuild  # noqa: E402
 from trhepd_opt_b200 import bulkfile, generator, native, surface  # noqa: E402
 
 METRIC = "angle-solves/s at N=521, split-precision vs FP64 on 1 B200; p50/p99 latency"
+# DRAM bytes (read + write) per launch of the tensor-core stage kernel from one ncu
+# capture (profiles/), keyed by (workload, form); absent entries report null.
+NCU_TRAFFIC: dict = {}
 WORKLOADS = {
     "dense521": ("dense521: N=521 beams, 61 glancing angles 0.5-6.5 deg, 20 A region in 0.01 A "
                  "slices (sp4 RKN), synthetic 2x2 Si/Ge surface over 4-atom bulk, seed 3",
@@ -137,28 +143,48 @@ def measured_peaks() -> dict:
     return {}
 
 
-def fp64_gemm_peak(device: int) -> float | None:
-    """cuBLAS DGEMM 8192^3 throughput (TFLOP/s), the FP64 tensor-core reference."""
+def library_gemm_peak(device: int, kind: str, seconds: float = 3.0) -> dict | None:
+    """Library GEMM 8192^3 throughput in T(FL)OP/s on this GPU: cuBLAS DGEMM (kind
+    "f64", the FP64 tensor-core reference) or cuBLASLt INT8 -> INT32 (kind "i8",
+    torch._int_mm).  "burst" is the best of 5 single launches, "sustained" the mean
+    over a back-to-back loop of `seconds`, the figure for kernels timed inside a
+    long solve."""
     try:
         import torch
         torch.cuda.set_device(device)
         n = 8192
-        a = torch.randn(n, n, dtype=torch.float64, device="cuda")
-        b = torch.randn(n, n, dtype=torch.float64, device="cuda")
-        for _ in range(2):
-            torch.matmul(a, b)
+        if kind == "f64":
+            a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+            b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+            op = lambda: torch.matmul(a, b)  # noqa: E731
+        else:
+            a = torch.randint(-128, 128, (n, n), dtype=torch.int8, device="cuda")
+            b = torch.randint(-128, 128, (n, n), dtype=torch.int8,
+                              device="cuda").t().contiguous().t()
+            op = lambda: torch._int_mm(a, b)  # noqa: E731
+        for _ in range(3):
+            op()
         torch.cuda.synchronize()
         best = 1e30
         for _ in range(5):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            torch.matmul(a, b)
+            op()
             e1.record()
             torch.cuda.synchronize()
             best = min(best, e0.elapsed_time(e1))
+        reps = max(3, int(seconds * 1e3 / best))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            op()
+        e1.record()
+        torch.cuda.synchronize()
+        mean = e0.elapsed_time(e1) / reps
         del a, b
         torch.cuda.empty_cache()
-        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+        w = 2.0 * n ** 3
+        return {"burst": w / (best * 1e-3) / 1e12, "sustained": w / (mean * 1e-3) / 1e12}
     except Exception:
         return None
 
@@ -246,9 +272,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dense521", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="auto", choices=["auto", "split", "fp64"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "int8", "bf16", "fp64"],
+                    help="auto: the INT8 split form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-bf16", action="store_true", help="skip the BF16 split comparison")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=40.0)
@@ -309,15 +337,11 @@ def main():
     rp = sp.resident()
     nang, n = rp.nangles, rp.nb
     ctx.set_option(native.OPT_RENORM_POLICY, 1)
-    prec = {"auto": native.SPLIT_BF16, "split": native.SPLIT_BF16,
+    prec = {"auto": native.SPLIT_INT8, "int8": native.SPLIT_INT8, "bf16": native.SPLIT_BF16,
             "fp64": native.FP64}[args.precision]
-    if prec == native.SPLIT_BF16:
-        try:
-            rp.solve(prec)
-        except native.TrhepdError:
-            if args.precision == "split":
-                raise
-            prec = native.FP64  # this build has no split form: report the FP64 form
+    split = prec != native.FP64
+    slices = 4
+    ctx.set_option(native.OPT_SPLIT_SLICES, slices)
 
     def solve_ms(p):
         rp.solve(p)
@@ -347,42 +371,79 @@ def main():
     ms_per_step = max_ms / args.steps
     _, f2_main = rp.fetch()
 
-    # ---- roofline of the stage-product kernel (one profiled solve)
+    # ---- roofline of the tensor-core stage kernel (one profiled solve): CUDA events
+    # around every launch of that kernel on the library stream
     ctx.set_option(native.OPT_PROFILE, 1)
     stp = solve_ms(prec)
     ctx.set_option(native.OPT_PROFILE, 0)
-    avg_ms = stp["stage_kernel_ms"] / max(stp["stage_products"], 1)
-    flops_per_launch = 8.0 * nang * n ** 3  # complex N x N x N product per angle
-    achieved = flops_per_launch / (avg_ms * 1e-3) / 1e12
+    nprod = max(stp["stage_products"], 1)
+    tensor_ms = stp["tensor_kernel_ms"] / nprod
+    stage_ms = stp["stage_kernel_ms"] / nprod
+    fp64_equiv = 8.0 * nang * n ** 3  # complex N x N x N product per angle
+    pairs = slices * (slices + 1) // 2 if split else 1
+    issued = pairs * fp64_equiv       # slice-pair GEMM work of one launch
+    achieved = issued / (tensor_ms * 1e-3) / 1e12
     peaks = measured_peaks()
-    if prec == native.SPLIT_BF16:
+    f64_peak = library_gemm_peak(local, "f64") if rank == 0 else None
+    if prec == native.SPLIT_INT8:
+        pk = library_gemm_peak(local, "i8") if rank == 0 else None
+        peak = pk["sustained"] if pk else None
+        peak_src = ("cuBLASLt INT8 GEMM 8192^3 (torch._int_mm) measured in this run, "
+                    "sustained over a 3 s loop")
+        kernel, unit = "k_split_gemm_i8 (tcgen05 kind::i8, INT32 accumulators)", "TOP/s"
+    elif prec == native.SPLIT_BF16:
+        pk = None
         peak = peaks.get("bf16_tflops_sustained") or 1400.0
-        peak_src = ("MEASURED_PEAKS.json bf16_tflops_sustained" if peaks else
+        peak_src = ("MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if peaks else
                     "fallback 1.4 PFLOP/s sustained")
+        kernel, unit = "k_split_gemm_p (tcgen05 kind::f16, FP32 accumulators)", "TFLOP/s"
     else:
-        peak = fp64_gemm_peak(local) if rank == 0 else None
-        peak_src = "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor peak)"
-    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": (achieved / peak) if peak else None, "traffic": None,
-            "kernel": "stage product (split BF16 tcgen05)" if prec == native.SPLIT_BF16
-            else "k_stage_gemm_f64 (FP64 DMMA)",
-            "peak_source": peak_src, "avg_launch_ms": avg_ms,
-            "flops_per_launch": flops_per_launch,
-            "note": "algorithmic FP64-equivalent flops 8*nangles*N^3 per stage product"}
+        pk = None
+        peak = f64_peak["sustained"] if f64_peak else None
+        peak_src = "cuBLAS DGEMM 8192^3 measured in this run, sustained over a 3 s loop"
+        kernel, unit = "k_stage_gemm_f64 (FP64 DMMA)", "TFLOP/s"
+    fp64_equiv_tflops = fp64_equiv / (tensor_ms * 1e-3) / 1e12
+    form = args.precision if args.precision != "auto" else "int8"
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": unit,
+            "frac": (achieved / peak) if peak else None,
+            "traffic": NCU_TRAFFIC.get((args.workload, form)),
+            "kernel": kernel, "peak_source": peak_src, "library_peak": pk,
+            "avg_launch_ms": tensor_ms, "stage_product_ms": stage_ms, "ops_per_launch": issued,
+            "slice_pairs": pairs, "fp64_equivalent_tflops": fp64_equiv_tflops,
+            "fp64_library_peak_tflops": f64_peak,
+            "frac_of_fp64_peak": (fp64_equiv_tflops / f64_peak["sustained"]) if f64_peak else None,
+            "note": "ops per launch = slice pairs x 8*nangles*N^3 (complex N^3 as a real "
+                    "(nangles*N) x 2N x 2N product per slice pair); stage_product_ms adds "
+                    "the slicing and exponent kernels of the same stage"}
 
-    # ---- FP64 comparison
+    # ---- comparison forms on the same resident problem
+    def compare(p):
+        solve_ms(p)
+        st = solve_ms(p)
+        _, f2_ref = rp.fetch()
+        return st, f2_ref
+
+    def errors(got, ref):
+        rowmax = np.maximum(np.abs(ref).max(axis=1, keepdims=True), 1e-300)
+        d = np.abs(got - ref)
+        big = np.abs(ref) >= 1e-3 * rowmax
+        return {"max_err_vs_rowmax": float((d / rowmax).max()),
+                "max_rel_err_spots_ge_1e-3_rowmax":
+                    float((d / np.where(big, np.abs(ref), np.inf)).max())}
+
     fp64 = None
-    if prec == native.SPLIT_BF16 and not args.no_fp64:
-        solve_ms(native.FP64)
-        st = solve_ms(native.FP64)
-        _, f2_64 = rp.fetch()
-        rowmax = np.maximum(np.abs(f2_64).max(axis=1, keepdims=True), 1e-300)
-        d = np.abs(f2_main - f2_64)
-        big = np.abs(f2_64) >= 1e-3 * rowmax
+    f2_64 = None
+    if split and not args.no_fp64:
+        st, f2_64 = compare(native.FP64)
         fp64 = {"value": nang / (st["device_ms"] / 1e3), "ms_per_step": st["device_ms"],
-                "split_speedup": (st["device_ms"] / ms_per_step),
-                "split_max_err_vs_rowmax": float((d / rowmax).max()),
-                "split_max_rel_err_spots_ge_1e-3_rowmax": float((d / np.where(big, np.abs(f2_64), np.inf)).max())}
+                "split_speedup": (st["device_ms"] / ms_per_step)}
+        fp64.update({"split_" + k: v for k, v in errors(f2_main, f2_64).items()})
+    bf16 = None
+    if prec == native.SPLIT_INT8 and not args.no_bf16:
+        st, f2_b = compare(native.SPLIT_BF16)
+        bf16 = {"value": nang / (st["device_ms"] / 1e3), "ms_per_step": st["device_ms"]}
+        if f2_64 is not None:
+            bf16.update(errors(f2_b, f2_64))
 
     # ---- end to end through the C ABI with host buffers
     e2e = None
@@ -414,7 +475,7 @@ def main():
 
     serve = None
     if rank == 0 and ws == 1 and not args.no_serve:
-        serve = {"split" if prec == native.SPLIT_BF16 else "fp64":
+        serve = {"split" if split else "fp64":
                  serve_leg(local, args.serve_seconds, args.serve_load, prec)}
         if args.serve_fp64 and prec != native.FP64:
             serve["fp64"] = serve_leg(local, args.serve_seconds, args.serve_load, native.FP64)
@@ -423,15 +484,20 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "angle-solves/s", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "bf16x4-split/f64" if prec == native.SPLIT_BF16 else "f64",
+                "dtype": {native.SPLIT_INT8: "i8x4-split/f64",
+                          native.SPLIT_BF16: "bf16x4-split/f64", native.FP64: "f64"}[prec],
                 "data": "synthetic",
                 "config": {"workload": desc, "nb": n, "nangles": nang, "slices": rp.ns,
-                           "precision": "split-bf16" if prec == native.SPLIT_BF16 else "fp64",
+                           "precision": {native.SPLIT_INT8: "split-int8",
+                                         native.SPLIT_BF16: "split-bf16",
+                                         native.FP64: "fp64"}[prec],
+                           "split_slices": slices if split else None,
                            "renormalisation": "growth bound ln(1e3)",
                            "bulk_boundary": "non-reflecting bulk records (f = 0)",
                            "l2": "inputs larger than L2 (state + stage table > 1 GB)",
                            "parallelism": f"replicas x{ws}"},
-                "roofline": roof, "fp64": fp64, "e2e": e2e, "cpu_baseline": cpu,
+                "roofline": roof, "fp64": fp64, "bf16_split": bf16, "e2e": e2e,
+                "cpu_baseline": cpu,
                 "gpu_launches": launches, "clocks": clk, "wall_seconds_timed": t_wall,
                 "serving": serve}
         print(json.dumps(line), flush=True)

@@ -35,18 +35,26 @@ enum trhepd_status {
 /* precision forms of the surface solve */
 enum trhepd_precision {
   TRHEPD_FP64 = 0,        /* all-FP64 (DMMA) */
-  TRHEPD_SPLIT_BF16 = 1   /* stage products from BF16 slices on tcgen05, FP64 elsewhere */
+  TRHEPD_SPLIT_BF16 = 1,  /* stage products from BF16 slices on tcgen05 (FP32 accumulators),
+                             FP64 elsewhere */
+  TRHEPD_SPLIT_INT8 = 2   /* stage products from signed 8-bit digit slices on tcgen05
+                             (exact INT32 accumulators, 3 or 4 slices), FP64 elsewhere */
 };
 
 /* options (trhepd_set_option) */
 enum trhepd_option {
   TRHEPD_OPT_RENORM_POLICY = 1, /* 0: Gershgorin test > 1e3 per angle and slice (reference)
-                                   1: growth bound, uniform schedule (see DESIGN) */
+                                   1: growth bound: every floor(tau / ((kappa_max + 1) dz))
+                                      slices, kappa_max the largest evanescent decay constant */
   TRHEPD_OPT_RENORM_TAU = 2,    /* growth bound ln(cond) between renormalisations (policy 1) */
-  TRHEPD_OPT_SPLIT_SLICES = 3,  /* BF16 slices per operand in the split form (3..5) */
+  TRHEPD_OPT_SPLIT_SLICES = 3,  /* slices per operand in the split forms (BF16 3..5, INT8 3..4) */
   TRHEPD_OPT_PROFILE = 4,       /* nonzero: time every stage-product launch with CUDA events */
-  TRHEPD_OPT_SPLIT_KERNEL = 5   /* split-form kernel: 0 persistent, two accumulators, epilogue
-                                   overlapped (default); 1 one CTA per tile, three accumulators */
+  TRHEPD_OPT_SPLIT_KERNEL = 5,  /* BF16 split kernel: 0 persistent, one CTA per SM, epilogue of
+                                   a tile overlapped with the next tile's MMAs (default);
+                                   1 one CTA per tile */
+  TRHEPD_OPT_GRAPHS = 6         /* nonzero (default): a resident problem's solve is captured
+                                   into a CUDA graph on its second solve with the same
+                                   options and replayed afterwards; 0: launch directly */
 };
 
 typedef struct trhepd_context trhepd_context;
@@ -58,7 +66,9 @@ int trhepd_set_option(trhepd_context* ctx, int option, double value);
 /* counters of the last solve: out[0] renormalisations, out[1] stage products,
    out[2] device milliseconds of the solve, out[3] stage columns, out[4] summed
    device milliseconds of the stage-product kernels (TRHEPD_OPT_PROFILE only),
-   out[5] kernels launched, out[6] of which renormalisation kernels */
+   out[5] kernels launched, out[6] of which renormalisation kernels, out[7] summed
+   device milliseconds of the tensor-core kernel alone inside the stage products
+   (TRHEPD_OPT_PROFILE only) */
 int trhepd_last_stats(const trhepd_context* ctx, double* out, int n);
 
 /*

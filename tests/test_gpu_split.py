@@ -1,5 +1,5 @@
-"""Split-precision form (BF16 slices on tcgen05, FP64 elsewhere) against the
-plain FP64 form and the oracle.  Target: every spot within 1e-6 of its row
+"""Split-precision forms (BF16 or INT8 digit slices on tcgen05, FP64 elsewhere)
+against the plain FP64 form and the oracle.  Target: every spot within 1e-6 of its row
 maximum and within 1e-5 relative on spots >= 1e-3 of the row maximum, with 4
 slices.  (At 2000 chained slices the FP64 result itself moves by ~4e-7 relative
 on weak spots when only the renormalisation points change, so weaker spots are
@@ -32,9 +32,13 @@ def _resident(ctx, tmp_path, s):
     return sp, sp.resident()
 
 
-@pytest.mark.parametrize("variant", [0, 1], ids=["persistent", "per_tile"])
+# (precision form, BF16 kernel variant)
+FORMS = {"persistent": (1, 0), "per_tile": (1, 1), "int8": (2, 0)}
+
+
+@pytest.mark.parametrize("form", sorted(FORMS))
 @pytest.mark.parametrize("case", ["small23", "dense95", "dense200"])
-def test_split_matches_fp64(ctx, tmp_path, case, variant):
+def test_split_matches_fp64(ctx, tmp_path, case, form):
     from trhepd_opt_b200 import generator, native
     if case == "small23":
         s = generator.small23()
@@ -45,10 +49,11 @@ def test_split_matches_fp64(ctx, tmp_path, case, variant):
     sp, rp = _resident(ctx, tmp_path, s)
     rp.solve(native.FP64)
     _, ref = rp.fetch()
+    precision, variant = FORMS[form]
     ctx.set_option(native.OPT_SPLIT_SLICES, 4)
     ctx.set_option(native.OPT_SPLIT_KERNEL, variant)
     try:
-        rp.solve(native.SPLIT_BF16)
+        rp.solve(precision)
         _, got = rp.fetch()
     finally:
         ctx.set_option(native.OPT_SPLIT_KERNEL, 0)
@@ -58,34 +63,52 @@ def test_split_matches_fp64(ctx, tmp_path, case, variant):
     assert rel_big <= 1e-5, rel_big
 
 
-def test_split_against_reference_output(ctx, golden):
-    """The split form on the reference's own N=47 case at 0.22 A slices."""
+@pytest.mark.parametrize("precision", [1, 2], ids=["bf16", "int8"])
+def test_split_against_reference_output(ctx, golden, precision):
+    """The split forms on the reference's own N=47 case at 0.22 A slices."""
     from trhepd_opt_b200 import native
     d = golden / "test47"
     ref = np.load(d / "perf-5-0.22.npz")
     ctx.set_option(native.OPT_SPLIT_SLICES, 4)
-    f2, _ = ctx.surf_run(d / "bulkP.b", d / "surf.txt", 0.22, 5, native.SPLIT_BF16)
+    f2, _ = ctx.surf_run(d / "bulkP.b", d / "surf.txt", 0.22, 5, precision)
     abs_err, _ = spot_errors(f2, ref["f2"])
     assert abs_err <= 1e-6, abs_err
 
 
-def test_more_slices_is_more_accurate(ctx, tmp_path):
+@pytest.mark.parametrize("precision,slices", [(1, (3, 4, 5)), (2, (3, 4))],
+                         ids=["bf16", "int8"])
+def test_more_slices_is_more_accurate(ctx, tmp_path, precision, slices):
     from trhepd_opt_b200 import generator, native
     sp, rp = _resident(ctx, tmp_path, generator.small23())
     rp.solve(native.FP64)
     _, ref = rp.fetch()
     errs = []
-    for S in (3, 4, 5):
+    for S in slices:
         ctx.set_option(native.OPT_SPLIT_SLICES, S)
-        rp.solve(native.SPLIT_BF16)
+        rp.solve(precision)
         _, got = rp.fetch()
         errs.append(spot_errors(got, ref)[0])
     ctx.set_option(native.OPT_SPLIT_SLICES, 4)
-    assert errs[0] > errs[1] > errs[2], errs
+    assert all(a > b for a, b in zip(errs, errs[1:])), errs
 
 
+def test_int8_rejects_five_slices(ctx, tmp_path):
+    """Five INT8 levels would need 640 tensor-memory columns: a clear error, and
+    the context stays usable."""
+    from trhepd_opt_b200 import generator, native
+    sp, rp = _resident(ctx, tmp_path, generator.small23())
+    ctx.set_option(native.OPT_SPLIT_SLICES, 5)
+    try:
+        with pytest.raises(native.TrhepdError):
+            rp.solve(native.SPLIT_INT8)
+    finally:
+        ctx.set_option(native.OPT_SPLIT_SLICES, 4)
+    rp.solve(native.SPLIT_INT8)
+
+
+@pytest.mark.parametrize("precision", [1, 2], ids=["bf16", "int8"])
 @pytest.mark.parametrize("method", [4, 7])
-def test_split_other_integrators(ctx, tmp_path, method):
+def test_split_other_integrators(ctx, tmp_path, method, precision):
     """The leapfrog and RK4 paths take the same split stage product."""
     from trhepd_opt_b200 import generator, native
     s = generator.small23()
@@ -94,7 +117,7 @@ def test_split_other_integrators(ctx, tmp_path, method):
     rp.solve(native.FP64)
     _, ref = rp.fetch()
     ctx.set_option(native.OPT_SPLIT_SLICES, 4)
-    rp.solve(native.SPLIT_BF16)
+    rp.solve(precision)
     _, got = rp.fetch()
     abs_err, _ = spot_errors(got, ref)
     assert abs_err <= 1e-6, abs_err

@@ -168,6 +168,7 @@ struct trhepd_context {
   int split_slices = 4;
   int split_variant = kSplitPersistent;
   int profile = 0;               // 1: time every stage-product launch with events
+  int graphs = 1;                // 1: replay resident solves from a captured CUDA graph
   double stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<cudaEvent_t> evpool;
   // device buffers (grown on demand, reused across calls)
@@ -180,6 +181,10 @@ struct trhepd_context {
 };
 
 namespace {
+
+bool valid_precision(int p) {
+  return p == TRHEPD_FP64 || p == TRHEPD_SPLIT_BF16 || p == TRHEPD_SPLIT_INT8;
+}
 
 int fail(trhepd_context* ctx, int code, const std::string& msg) {
   if (ctx) ctx->err = msg;
@@ -258,6 +263,33 @@ struct SolveArgs {
 
 }  // namespace
 
+namespace {
+
+// Device buffers and counters of one integration of a resident problem.
+struct RunState {
+  int n = 0, ns = 0, nv = 0, nang = 0, ld = 0, kpad = 0;
+  bool split = false;
+  int split_variant = kSplitPersistent;
+  cudaStream_t st = nullptr;
+  const TableEntry* table = nullptr;
+  const int* pair = nullptr;
+  const cd* gam = nullptr;
+  const cd* D = nullptr;
+  size_t sbytes = 0;
+  cd *Q = nullptr, *Qn = nullptr, *P = nullptr, *V = nullptr;
+  int* flags = nullptr;
+  double* dval = nullptr;
+  void* gjs = nullptr;
+  unsigned* status = nullptr;
+  SplitWorkspace sw{};
+  int interval = 1;          // renormalisation interval of the growth-bound policy
+  long renorms = 0, products = 0, launches = 0, gj_launches = 0;
+  int gj_per = 0;
+  bool capturing = false;    // launches go into a CUDA graph: no events on the stream
+};
+
+}  // namespace
+
 // Device-resident problem: stage table, beam-pair map, bulk boundary, gammas.
 // Solving it reads only device memory; the result stays on the device until
 // fetched.
@@ -268,10 +300,22 @@ struct trhepd_problem {
   int ncol = 0;
   DevBuf table, pair, gam, D, F, wnsga2, f2;
   std::vector<double> angle_deg;
+  // CUDA graph of the whole solve, valid for `graph_key` and the context buffers
+  // in `graph_sig`; `last_sig` holds the buffers of the last uncaptured solve.
+  cudaGraphExec_t graph = nullptr;
+  std::vector<double> graph_key;
+  std::vector<void*> graph_sig, last_sig;
+  RunState graph_run;
+  void drop_graph() {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+    graph_sig.clear();
+  }
   size_t bytes() const {
     return table.n + pair.n + gam.n + D.n + F.n + wnsga2.n + f2.n;
   }
   void release() {
+    drop_graph();
     for (DevBuf* b : {&table, &pair, &gam, &D, &F, &wnsga2, &f2}) b->release();
   }
 };
@@ -382,26 +426,6 @@ void prepare(trhepd_context* C, const SolveArgs& A, trhepd_problem& Pb) {
   Pb.f2.ensure((size_t)nang * n * sizeof(double));
 }
 
-// Device buffers and counters of one integration of a resident problem.
-struct RunState {
-  int n = 0, ns = 0, nv = 0, nang = 0, ld = 0, kpad = 0;
-  bool split = false;
-  cudaStream_t st = nullptr;
-  const TableEntry* table = nullptr;
-  const int* pair = nullptr;
-  const cd* gam = nullptr;
-  const cd* D = nullptr;
-  size_t sbytes = 0;
-  cd *Q = nullptr, *Qn = nullptr, *P = nullptr, *V = nullptr;
-  int* flags = nullptr;
-  double* dval = nullptr;
-  void* gjs = nullptr;
-  unsigned* status = nullptr;
-  SplitWorkspace sw{};
-  int interval = 1;          // renormalisation interval of the growth-bound policy
-  long renorms = 0, products = 0, launches = 0, gj_launches = 0;
-  int gj_per = 0;
-};
 
 // Buffers, the boundary transform invstransh (matcomp.f90:140-172) and the
 // renormalisation schedule; Q = I and P = P0 afterwards.
@@ -428,19 +452,22 @@ void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_m
   R.dval = (double*)C->dval.ensure(std::max(nang, 4) * sizeof(double));
   R.gjs = C->gj.ensure(gj_scratch_bytes(nang, n));
   R.status = (unsigned*)C->status.ensure(16);
-  R.split = precision == TRHEPD_SPLIT_BF16;
+  R.split = precision == TRHEPD_SPLIT_BF16 || precision == TRHEPD_SPLIT_INT8;
+  R.split_variant = (precision == TRHEPD_SPLIT_INT8) ? kSplitInt8 : C->split_variant;
+  if (precision == TRHEPD_SPLIT_INT8 && C->split_slices > 4)
+    throw std::invalid_argument("the INT8 split form takes 3 or 4 slices");
   if (R.split)
     R.sw = split_workspace_carve(C->split.ensure(split_workspace_bytes(nang, n, C->split_slices)),
                                  nang, n, C->split_slices, R.status, st);
   R.gj_per = 2 * ceil_div(n, 16);
-  if (C->profile && (int)C->evpool.size() < 2 * nprod_max) {
-    while ((int)C->evpool.size() < 2 * nprod_max) {
+  if (C->profile && (int)C->evpool.size() < 4 * nprod_max) {
+    while ((int)C->evpool.size() < 4 * nprod_max) {
       cudaEvent_t e;
       CK(cudaEventCreate(&e));
       C->evpool.push_back(e);
     }
   }
-  CK(cudaEventRecord(C->ev0, st));
+  if (!R.capturing) CK(cudaEventRecord(C->ev0, st));
   CK(cudaMemsetAsync(R.status, 0, 16, st));
   CK(cudaMemsetAsync(R.Q, 0, R.sbytes, st));
   CK(cudaMemsetAsync(R.Qn, 0, R.sbytes, st));
@@ -467,15 +494,18 @@ void gather(RunState& R, int col, bool drop_diag) {
 // P += cb (Q M), Qo = Q + ca P with M from R.V (gathered for the chosen form).
 void stage_product(trhepd_context* C, RunState& R, const cd* Q, cd* P, cd* Qo, double cb,
                    double ca) {
-  if (C->profile) CK(cudaEventRecord(C->evpool[2 * R.products], R.st));
+  const cudaEvent_t* ev = C->profile ? &C->evpool[4 * R.products] : nullptr;
+  if (ev) CK(cudaEventRecord(ev[0], R.st));
   if (R.split) {
     R.launches += split_stage(R.sw, Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, cb, ca,
-                              C->split_slices, C->split_variant, R.st);
+                              C->split_slices, R.split_variant, ev ? ev + 1 : nullptr, R.st);
   } else {
+    if (ev) CK(cudaEventRecord(ev[1], R.st));
     launch_stage_gemm_f64(Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, R.kpad, cb, ca, R.st);
+    if (ev) CK(cudaEventRecord(ev[2], R.st));
     R.launches += 1;
   }
-  if (C->profile) CK(cudaEventRecord(C->evpool[2 * R.products + 1], R.st));
+  if (ev) CK(cudaEventRecord(ev[3], R.st));
   ++R.products;
 }
 
@@ -500,9 +530,8 @@ void renormalise(trhepd_context* C, RunState& R, int l, bool every_slice) {
   }
 }
 
-// stransh (matcomp.f90:174-196), the intensities (surflf.f90:142-151) and the
-// status and timing of the whole run.
-void finish_run(trhepd_context* C, trhepd_problem& Pb, RunState& R) {
+// stransh (matcomp.f90:174-196) and the intensities (surflf.f90:142-151).
+void finish_device(trhepd_context* C, trhepd_problem& Pb, RunState& R) {
   cudaStream_t st = R.st;
   const int n = R.n, nang = R.nang, ld = R.ld;
   launch_stransh_build(R.Q, R.P, R.gam, nang, n, ld, st);
@@ -511,19 +540,27 @@ void finish_run(trhepd_context* C, trhepd_problem& Pb, RunState& R) {
   launch_intensities(R.P, R.gam, Pb.wnsga2.as<double>(), nang, n, ld, Pb.nb0,
                      Pb.f2.as<double>(), st);
   R.launches += 3 + R.gj_per;
-  CK(cudaEventRecord(C->ev1, st));
+  if (!R.capturing) CK(cudaEventRecord(C->ev1, st));
+  CK(cudaGetLastError());
+}
+
+// Status and timing of a finished run (after its launches or its graph).
+void finish_host(trhepd_context* C, trhepd_problem& Pb, RunState& R) {
+  cudaStream_t st = R.st;
   CK(cudaGetLastError());
   unsigned h_status[4];
   CK(cudaMemcpyAsync(h_status, R.status, 16, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   float ms = 0;
   cudaEventElapsedTime(&ms, C->ev0, C->ev1);
-  double prod_ms = 0.0;
+  double prod_ms = 0.0, tensor_ms = 0.0;
   if (C->profile)
     for (long p = 0; p < R.products; ++p) {
-      float e = 0;
-      cudaEventElapsedTime(&e, C->evpool[2 * p], C->evpool[2 * p + 1]);
+      float e = 0, t = 0;
+      cudaEventElapsedTime(&e, C->evpool[4 * p], C->evpool[4 * p + 3]);
+      cudaEventElapsedTime(&t, C->evpool[4 * p + 1], C->evpool[4 * p + 2]);
       prod_ms += e;
+      tensor_ms += t;
     }
   C->stats[0] = (double)R.renorms;
   C->stats[1] = (double)R.products;
@@ -532,16 +569,16 @@ void finish_run(trhepd_context* C, trhepd_problem& Pb, RunState& R) {
   C->stats[4] = prod_ms;
   C->stats[5] = (double)R.launches;
   C->stats[6] = (double)R.gj_launches;
+  C->stats[7] = tensor_ms;
   if (h_status[0] & kStatusTimeout) throw CudaError("device wait timed out", TRHEPD_ETIMEOUT);
   if (h_status[0] & (kStatusNonFinite | kStatusZeroPivot))
     throw CudaError("non-finite value or zero pivot in the surface solve", TRHEPD_ENONFINITE);
 }
 
 // Symplectic RKN (hp_int_spa, surf_prkn.f90:278-330) batched over angles.
-void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision) {
+void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
   const Integrator& I = Pb.I;
   const double dz = Pb.dz;
-  RunState R;
   begin_run(C, Pb, precision, I.s * Pb.ns, R);
   const bool every_slice = (Pb.n == 1 && Pb.int_method == 6);  // hp_int_spa1d renormalises each slice
   for (int l = 1; l <= R.ns; ++l) {
@@ -569,16 +606,15 @@ void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision) {
   gather(R, I.s * R.ns, false);
   launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, I.bab[0] * dz, 0.0, R.st);
   R.launches += 1;
-  finish_run(C, Pb, R);
+  finish_device(C, Pb, R);
 }
 
 // Stormer-Verlet leapfrog (lf_int_spa, surf_magnus.f90:46-110) batched over
 // angles: Q = I + dz/2 P, then per slice P += dz Q M(l), Q += dz P (dz/2 on the
 // last slice).  A renormalised Q = I enters the next product as the identity,
 // which gives the reference's Q = I shortcut exactly.
-void run_lf(trhepd_context* C, trhepd_problem& Pb, int precision) {
+void run_lf(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
   const double dz = Pb.dz;
-  RunState R;
   begin_run(C, Pb, precision, Pb.ns, R);
   gather(R, 0, false);  // any finite stage matrix: cb = 0 below
   launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, 0.0, 0.5 * dz, R.st);
@@ -590,15 +626,14 @@ void run_lf(trhepd_context* C, trhepd_problem& Pb, int precision) {
     std::swap(R.Q, R.Qn);
     renormalise(C, R, l, false);
   }
-  finish_run(C, Pb, R);
+  finish_device(C, Pb, R);
 }
 
 // Classical RK4 on [Q | P] (rk4_int, surf_rk.f90:27-91) batched over angles:
 // k = (P', Q' M) at the stage points, each product Q' M formed by the stage
 // kernel into a zeroed buffer (cb = 1, ca = 0).
-void run_rk4(trhepd_context* C, trhepd_problem& Pb, int precision) {
+void run_rk4(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
   const double dz = Pb.dz;
-  RunState R;
   begin_run(C, Pb, precision, 4 * Pb.ns, R);
   const size_t sb = R.sbytes;
   cd* Qt = (cd*)C->rk[0].ensure(sb);
@@ -625,7 +660,7 @@ void run_rk4(trhepd_context* C, trhepd_problem& Pb, int precision) {
     }
     renormalise(C, R, l, false);
   }
-  finish_run(C, Pb, R);
+  finish_device(C, Pb, R);
 }
 
 
@@ -641,12 +676,11 @@ void bgemm(const cd* A, long long sA, const cd* B, long long sB, cd* Cm, long lo
 // hyperbolic_exp4r/6r of the stage matrices (magnus.cu), then P += Q rp and
 // Q += P q as batched GEMMs; after a renormalisation Q = I enters those products
 // as the identity.  Plain FP64 only.
-void run_magnus(trhepd_context* C, trhepd_problem& Pb, int precision) {
+void run_magnus(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
   if (precision != TRHEPD_FP64)
     throw std::invalid_argument("the Magnus integrators (int_method 1-3) run in plain FP64 only");
   const double dz = Pb.dz;
   const Family fam = Pb.I.family;
-  RunState R;
   begin_run(C, Pb, precision, 0, R);
   const int n = R.n, nang = R.nang, ld = R.ld;
   cudaStream_t st = R.st;
@@ -728,18 +762,84 @@ void run_magnus(trhepd_context* C, trhepd_problem& Pb, int precision) {
   }
   launch_add(R.P, RP, nang, n, ld, st);  // P += rp
   R.launches += 1;
-  finish_run(C, Pb, R);
+  finish_device(C, Pb, R);
 }
 
-void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
+// Every launch of one solve, in stream order, without host synchronisation.
+void run_device(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
   switch (Pb.I.family) {
-    case kRkn: run_rkn(C, Pb, precision); break;
-    case kLeapfrog: run_lf(C, Pb, precision); break;
-    case kRk4: run_rk4(C, Pb, precision); break;
+    case kRkn: run_rkn(C, Pb, precision, R); break;
+    case kLeapfrog: run_lf(C, Pb, precision, R); break;
+    case kRk4: run_rk4(C, Pb, precision, R); break;
     case kMagnus2:
     case kMagnus4:
-    case kMagnus6: run_magnus(C, Pb, precision); break;
+    case kMagnus6: run_magnus(C, Pb, precision, R); break;
   }
+}
+
+// The context buffers a solve's launches address; a graph stays valid while they do.
+std::vector<void*> buffer_signature(const trhepd_context* C) {
+  std::vector<void*> s = {C->Q0.p, C->Q1.p, C->P.p, C->V.p, C->flags.p, C->dval.p,
+                          C->gj.p, C->status.p, C->split.p};
+  for (const DevBuf& b : C->rk) s.push_back(b.p);
+  for (const DevBuf& b : C->mg) s.push_back(b.p);
+  return s;
+}
+
+// Solve a resident problem.  The launch sequence of a solve depends only on the
+// problem and the options, so after one uncaptured solve has sized the buffers,
+// the next one is captured into a CUDA graph and later solves replay it (one
+// launch instead of thousands; changed options, precision or reallocated buffers
+// force a new capture).  Profiling runs and TRHEPD_OPT_GRAPHS = 0 launch directly.
+void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
+  const std::vector<double> key = {(double)precision, (double)C->split_slices,
+                                   (double)C->split_variant, (double)C->renorm_policy,
+                                   C->renorm_tau};
+  if (!C->graphs || C->profile) {
+    Pb.drop_graph();
+    RunState R;
+    run_device(C, Pb, precision, R);
+    finish_host(C, Pb, R);
+    return;
+  }
+  const std::vector<void*> sig = buffer_signature(C);
+  if (!Pb.graph || Pb.graph_key != key || Pb.graph_sig != sig) {
+    Pb.drop_graph();
+    if (Pb.last_sig != sig || Pb.graph_key != key) {
+      // buffers may grow on this solve: run it directly, capture the next one
+      RunState R;
+      Pb.graph_key = key;
+      run_device(C, Pb, precision, R);
+      Pb.last_sig = buffer_signature(C);
+      finish_host(C, Pb, R);
+      return;
+    }
+    RunState R;
+    R.capturing = true;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(C->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      run_device(C, Pb, precision, R);
+    } catch (...) {
+      cudaStreamEndCapture(C->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      throw;
+    }
+    CK(cudaStreamEndCapture(C->stream, &g));
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    Pb.graph = ex;
+    Pb.graph_sig = sig;
+    Pb.graph_run = R;
+  }
+  RunState R = Pb.graph_run;
+  CK(cudaEventRecord(C->ev0, C->stream));
+  CK(cudaGraphLaunch(Pb.graph, C->stream));
+  CK(cudaEventRecord(C->ev1, C->stream));
+  finish_host(C, Pb, R);
 }
 
 void fetch(trhepd_context* C, trhepd_problem& Pb, double* f2, double* angle_deg) {
@@ -1203,6 +1303,9 @@ int trhepd_set_option(trhepd_context* c, int option, double value) {
         return fail(c, TRHEPD_EINVAL, "split kernel must be 0 (persistent) or 1 (per tile)");
       c->split_variant = (int)value;
       return TRHEPD_OK;
+    case TRHEPD_OPT_GRAPHS:
+      c->graphs = value != 0.0;
+      return TRHEPD_OK;
   }
   return fail(c, TRHEPD_EINVAL, "unknown option");
 }
@@ -1279,7 +1382,7 @@ int trhepd_srfref(trhepd_context* ctx, const trhepd_pot_state* pot, int nb, int 
     if (!pot || !iv || !nbg || !iord || !ih || !ik || !t1_records || !f2)
       throw std::invalid_argument("null argument");
     if (naz < 1 || ng < 1 || ngr < 1) throw std::invalid_argument("naz, ng, ngr must be >= 1");
-    if (precision != TRHEPD_FP64 && precision != TRHEPD_SPLIT_BF16)
+    if (!valid_precision(precision))
       throw std::invalid_argument("unknown precision form");
     SolveArgs a{pot, nb, ns, iv, dz, ngr, nbg, iord, ih, ik, wn, ghx, ghy, gky,
                 azi, daz, gi, dg, naz, ng, int_method, t1_records};
@@ -1314,7 +1417,7 @@ int trhepd_problem_create(trhepd_context* ctx, const trhepd_pot_state* pot,
 int trhepd_problem_solve(trhepd_context* ctx, trhepd_problem* pb, int precision) {
   return guarded(ctx, [&] {
     if (!pb) throw std::invalid_argument("null problem");
-    if (precision != TRHEPD_FP64 && precision != TRHEPD_SPLIT_BF16)
+    if (!valid_precision(precision))
       throw std::invalid_argument("unknown precision form");
     run(ctx, *pb, precision);
   });
@@ -1415,6 +1518,7 @@ int trhepd_surf_run(trhepd_context* ctx, const char* bulkp, const char* surf, do
                     int* dims) {
   return guarded(ctx, [&] {
     if (!bulkp || !surf || !(dz2 > 0)) throw std::invalid_argument("bad arguments");
+    if (!valid_precision(precision)) throw std::invalid_argument("unknown precision form");
     SurfaceInputs S;
     load_surface_inputs(bulkp, surf, dz2, int_method, S);
     structure_factors(ctx, S);

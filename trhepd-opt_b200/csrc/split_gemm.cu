@@ -50,6 +50,7 @@ constexpr int A_SLICE_BYTES = BM * BK * 2;
 constexpr int B_SLICE_BYTES = NT * BK * 2;
 constexpr int EPI_STRIDE = NC + 1;    // complex elements per staged row (odd: conflict-free)
 constexpr uint64_t kWaitNs = 2000000000ull;  // bounded waits give up after ~2 s
+constexpr double kDigitHeadroom = 1.0 + 1.0 / 128;  // INT8 exponents: |d_0| <= 127
 
 __host__ __device__ constexpr int stages_for(int S) { return S <= 4 ? 3 : 2; }
 __host__ __device__ constexpr size_t stage_bytes(int S) {
@@ -211,9 +212,10 @@ __global__ void k_slice_rows(const cd* __restrict__ Q, int rows, int n, int ld, 
 }
 
 // Column exponents of Voff: 32 columns per block, the 8 warps split the rows
-// (lanes read consecutive columns), then a shared-memory maximum.
+// (lanes read consecutive columns), then a shared-memory maximum; the exponent is
+// that of the maximum times `headroom` (1, or kDigitHeadroom for INT8 digits).
 __global__ void __launch_bounds__(256) k_col_exponents(const cd* __restrict__ V, int n, int ld,
-                                                       int* __restrict__ fcol) {
+                                                       double headroom, int* __restrict__ fcol) {
   __shared__ double red[8][33];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int j = blockIdx.x * 32 + lane;
@@ -228,7 +230,7 @@ __global__ void __launch_bounds__(256) k_col_exponents(const cd* __restrict__ V,
   if (w == 0 && j < n) {
     for (int q = 1; q < 8; ++q) m = fmax(m, red[q][lane]);
     int e = 0;
-    if (m > 0.0) frexp(m, &e);
+    if (m > 0.0) frexp(m * headroom, &e);
     fcol[j] = e;
   }
 }
@@ -712,6 +714,359 @@ __global__ void __launch_bounds__(P_THREADS, 1)
   }
 }
 
+// ------------------------------------------------------------ INT8 form
+// The same stage product from signed 8-bit digits on kind::i8 with exact INT32
+// accumulation (twice the BF16 MMA rate).  A row (column) whose largest entry is m
+// gets the exponent e of m (1 + 2^-7), so |x| < 2^e (1 - 2^-8) for its entries;
+// each entry is rounded once to the integer
+//     X = rint(x 2^(7 - e + 8(S-1)))
+// and written in balanced base 256, X = sum_s d_s 256^(S-1-s), d_s in [-128, 127]
+// for s >= 1; the headroom keeps |d_0| <= 127.  So x = 2^(e-7) sum_s d_s 2^-8s up
+// to half a unit of the last digit.  The slice pairs with s + t = L go to INT32
+// accumulator L (L < S, S*128 TMEM columns); every sum is exact (|acc_L| <=
+// S * 2^14 * K, below 2^31 for K < 32768), and the epilogue forms
+// sum_L 2^-8L acc_L in FP64 and scales it by 2^(e_r + f_j - 14).
+namespace i8 {
+constexpr int BK = 64;                     // int8 k per pipeline stage (64-byte rows)
+constexpr int A_SLICE_BYTES = BM * BK;     // 8 KB
+constexpr int B_SLICE_BYTES = NT * BK;     // 8 KB
+__host__ __device__ constexpr int stages_for(int S) { return S <= 3 ? 4 : 3; }
+__host__ __device__ constexpr size_t stage_bytes(int S) {
+  return (size_t)S * (A_SLICE_BYTES + B_SLICE_BYTES);
+}
+inline size_t smem_bytes(int S) { return 1024 + stages_for(S) * stage_bytes(S); }
+}  // namespace i8
+
+// Instruction descriptor: S8 x S8 -> S32, both K-major, M = 128, N = NT.
+__host__ __device__ constexpr uint32_t instr_desc_i8() {
+  return (2u << 4)                      // D format S32
+         | (1u << 7) | (1u << 10)       // A, B format S8
+         | ((uint32_t)(NT >> 3) << 17)  // N
+         | ((uint32_t)(BM >> 4) << 24); // M
+}
+__device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// Balanced base-256 digits of rint(x 2^(7 - e + 8(S-1))), most significant first.
+template <int S>
+__device__ __forceinline__ void digits_i8(double x, int e, int* d) {
+  long long X = __double2ll_rn(ldexp(x, 7 - e + 8 * (S - 1)));
+#pragma unroll
+  for (int s = S - 1; s >= 1; --s) {
+    const int lo = (int)((X + 128) & 255) - 128;
+    d[s] = lo;
+    X = (X - lo) >> 8;
+  }
+  d[0] = (int)X;
+}
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
+  return (uint32_t)(a & 255) | ((uint32_t)(b & 255) << 8) | ((uint32_t)(c & 255) << 16) |
+         ((uint32_t)(d & 255) << 24);
+}
+__device__ __forceinline__ uint16_t pack2(int a, int b) {
+  return (uint16_t)((a & 255) | ((b & 255) << 8));
+}
+
+// One warp per stacked row: exponent of the off-diagonal row maximum, then the S
+// digit slices of the row, (Re, Im) interleaved; each lane writes two complex k.
+template <int S>
+__global__ void k_slice_rows_i8(const cd* __restrict__ Q, int rows, int n, int ld, int kr,
+                                uint32_t* __restrict__ A, int* __restrict__ erow) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= rows) return;
+  const int r = warp, i = r % n;
+  const cd* q = Q + (size_t)r * ld;
+  double m = 0.0;
+  for (int k = lane; k < n; k += 32)
+    if (k != i) m = fmax(m, fmax(fabs(q[k].x), fabs(q[k].y)));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  int e = 0;
+  if (m > 0.0) frexp(m * kDigitHeadroom, &e);
+  if (lane == 0) erow[r] = e;
+  const int kw = kr / 4;      // 32-bit words per slice row (two complex k each)
+  for (int w = lane; w < kw; w += 32) {
+    const int k0 = 2 * w, k1 = 2 * w + 1;
+    const cd v0 = (k0 < n && k0 != i) ? q[k0] : cd{0.0, 0.0};
+    const cd v1 = (k1 < n && k1 != i) ? q[k1] : cd{0.0, 0.0};
+    int a[S], b[S], c[S], d[S];
+    digits_i8<S>(v0.x, e, a);
+    digits_i8<S>(v0.y, e, b);
+    digits_i8<S>(v1.x, e, c);
+    digits_i8<S>(v1.y, e, d);
+#pragma unroll
+    for (int s = 0; s < S; ++s) A[((size_t)s * rows + r) * kw + w] = pack4(a[s], b[s], c[s], d[s]);
+  }
+}
+
+// B^T digit slices: row 2j (Re-out) = [Vr(k,j), -Vi(k,j)]_k, row 2j+1 (Im-out) =
+// [Vi, Vr]_k; -Vi gets its own digits (negating digits could leave 128).
+template <int S>
+__global__ void k_slice_cols_i8(const cd* __restrict__ V, int n, int ld, int kc, int nrows,
+                                const int* __restrict__ fcol, uint16_t* __restrict__ B) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (k >= kc || j >= n) return;
+  const cd v = (k < n) ? V[(size_t)k * ld + j] : cd{0.0, 0.0};
+  const int e = fcol[j];
+  int dr[S], di[S], dn[S];
+  digits_i8<S>(v.x, e, dr);
+  digits_i8<S>(v.y, e, di);
+  digits_i8<S>(-v.y, e, dn);
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    B[((size_t)s * nrows + 2 * j) * kc + k] = pack2(dr[s], dn[s]);
+    B[((size_t)s * nrows + 2 * j + 1) * kc + k] = pack2(di[s], dr[s]);
+  }
+}
+
+// Persistent INT8 stage product: the warp roles, barriers, register split and the
+// register-held drain of k_split_gemm_p, with S INT32 accumulators.
+template <int S>
+__global__ void __launch_bounds__(P_THREADS, 1)
+    k_split_gemm_i8(const __grid_constant__ CUtensorMap tmA,
+                    const __grid_constant__ CUtensorMap tmB, EpiArgs ep, int nkb, int tiles_n,
+                    int tiles) {
+  static_assert(S * NT <= TMEM_COLS, "INT8 levels exceed the tensor memory");
+  constexpr int STAGES = i8::stages_for(S);
+  if (*(volatile unsigned*)ep.status & kStatusTimeout) return;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], tfull, tempty, drain_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh, issued_sh, consumed_sh;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t sbytes = i8::stage_bytes(S);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&tfull, 1);
+    mbar_init(&tempty, P_EPI_WARPS);
+    mbar_init(&drain_bar, 1);
+    abort_sh = 0;
+    issued_sh = 0;
+    consumed_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_sh)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+
+  if (warp < 4) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(P_REG_CTRL));
+    if (warp == 0) {
+      // ---------------- TMA producer
+      if (lane == 0) {
+        int g = 0;
+        bool stop = false;
+        for (int tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x) {
+          const int m0 = (tile / tiles_n) * BM, n0 = (tile % tiles_n) * NT;
+          for (int kb = 0; kb < nkb; ++kb, ++g) {
+            const int st = g % STAGES, round = g / STAGES;
+            if (round > 0 && !mbar_wait(&empty_bar[st], (round - 1) & 1)) {
+              atomicOr(ep.status, kStatusTimeout);
+              abort_sh = 1;
+              stop = true;
+              break;
+            }
+            if (ld_volatile(&abort_sh)) {
+              stop = true;
+              break;
+            }
+            unsigned char* sa = smem + st * sbytes;
+            unsigned char* sb = sa + S * i8::A_SLICE_BYTES;
+            mbar_expect_tx(&full_bar[st], (uint32_t)sbytes);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+              tma_load_3d(&tmA, &full_bar[st], sa + s * i8::A_SLICE_BYTES, kb * i8::BK, m0, s);
+              tma_load_3d(&tmB, &full_bar[st], sb + s * i8::B_SLICE_BYTES, kb * i8::BK, n0, s);
+            }
+          }
+        }
+        issued_sh = g;
+      }
+    } else if (warp == 1) {
+      // ---------------- MMA issuer
+      if (lane == 0) {
+        const uint32_t idesc = instr_desc_i8();
+        int g = 0, it = 0;
+        bool stop = false;
+        for (int tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x, ++it) {
+          if (it > 0 && !mbar_wait(&tempty, (it - 1) & 1)) {
+            atomicOr(ep.status, kStatusTimeout);
+            abort_sh = 1;
+            break;
+          }
+          tc_fence_after();
+          bool started[S];
+#pragma unroll
+          for (int L = 0; L < S; ++L) started[L] = false;
+          for (int kb = 0; kb < nkb; ++kb, ++g) {
+            const int st = g % STAGES, round = g / STAGES;
+            if (!mbar_wait(&full_bar[st], round & 1)) {
+              atomicOr(ep.status, kStatusTimeout);
+              abort_sh = 1;
+              stop = true;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t sa = smem_u32(smem + st * sbytes);
+            const uint32_t sb = sa + S * i8::A_SLICE_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < i8::BK / 32; ++kk) {
+#pragma unroll
+              for (int s = 0; s < S; ++s) {
+#pragma unroll
+                for (int t = 0; t < S - s; ++t) {
+                  const int L = s + t;
+                  const uint64_t ad = sw64_desc(sa + s * i8::A_SLICE_BYTES + kk * 32);
+                  const uint64_t bd = sw64_desc(sb + t * i8::B_SLICE_BYTES + kk * 32);
+                  tc_mma_i8(tmem + L * NT, ad, bd, idesc, started[L] ? 1u : 0u);
+                  started[L] = true;
+                }
+              }
+            }
+            tc_commit(&empty_bar[st]);
+          }
+          if (stop) break;
+          tc_commit(&tfull);
+        }
+        consumed_sh = g;
+        tc_commit(&drain_bar);
+        if (!mbar_wait(&drain_bar, 0)) atomicOr(ep.status, kStatusTimeout);
+      }
+    }
+  } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(P_REG_EPI));
+    // ---------------- epilogue warps 4..11
+    const int q4 = warp & 3;
+    const int half = (warp - 4) >> 2;
+    const int t0 = lane & 3, t1 = lane >> 2;
+    const cd vd = ep.V[(size_t)ep.kpad * ep.ld];
+    int it = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
+      const int m0 = (tile / tiles_n) * BM + q4 * 32;
+      const int jh = (tile % tiles_n) * NC + half * (NC / 2);
+      int er[2][2], ra[2][2], ri[2][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int r = m0 + 16 * h + 8 * u + t1;
+          er[h][u] = 0;
+          ra[h][u] = 0;
+          ri[h][u] = 0;
+          if (r < ep.rows) {
+            er[h][u] = ep.erow[r];
+            ra[h][u] = r / ep.n;
+            ri[h][u] = r - ra[h][u] * ep.n;
+          }
+        }
+      int fc[8];
+#pragma unroll
+      for (int g = 0; g < 8; ++g) {
+        const int j = jh + 4 * g + t0;
+        fc[g] = (j < ep.n) ? ep.fcol[j] : 0;
+      }
+      const bool ok = mbar_wait(&tfull, it & 1);
+      if (epi_any(!ok)) {
+        if (!ok) atomicOr(ep.status, kStatusTimeout);
+        abort_sh = 1;
+        break;
+      }
+      tc_fence_after();
+      cd vals[8][2][2];
+#pragma unroll
+      for (int g = 0; g < 8; ++g)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t taddr = tmem + ((uint32_t)(q4 * 32 + 16 * h) << 16) +
+                                 (uint32_t)(2 * (half * (NC / 2) + 4 * g));
+          uint32_t a[S][4];
+#pragma unroll
+          for (int L = 0; L < S; ++L) tmem_ld_16x256(taddr + L * NT, a[L]);
+          tmem_wait_ld();
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            double re = (double)(int)a[S - 1][2 * u], im = (double)(int)a[S - 1][2 * u + 1];
+#pragma unroll
+            for (int L = S - 2; L >= 0; --L) {
+              re = fma(re, 0.00390625, (double)(int)a[L][2 * u]);
+              im = fma(im, 0.00390625, (double)(int)a[L][2 * u + 1]);
+            }
+            const double sc = pow2(er[h][u] + fc[g] - 14);
+            vals[g][h][u] = cd{re * sc, im * sc};
+          }
+        }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty);
+#pragma unroll
+      for (int g = 0; g < 8; ++g) {
+        const int j = jh + 4 * g + t0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          cd qv[2], pv[2], qd[2], vv[2], dv[2];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int r = m0 + 16 * h + 8 * u + t1;
+            if (r < ep.rows && j < ep.n) {
+              const size_t ro = (size_t)r * ep.ld;
+              qv[u] = ep.Q[ro + j];
+              pv[u] = ep.P[ro + j];
+              qd[u] = ep.Q[ro + ri[h][u]];
+              vv[u] = ep.V[(size_t)ri[h][u] * ep.ld + j];
+              dv[u] = ep.D[(size_t)ra[h][u] * ep.ld + j];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int r = m0 + 16 * h + 8 * u + t1;
+            if (r < ep.rows && j < ep.n) {
+              const size_t ro = (size_t)r * ep.ld;
+              const cd acc = vals[g][h][u] + qd[u] * vv[u] + qv[u] * (dv[u] + vd);
+              const cd p = pv[u] + ep.cb * acc;
+              ep.P[ro + j] = p;
+              ep.Qo[ro + j] = qv[u] + ep.ca * p;
+            }
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int g = consumed_sh; g < issued_sh; ++g)
+      if (!mbar_wait(&full_bar[g % STAGES], (g / STAGES) & 1)) break;
+  }
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS));
+  }
+}
+
 }  // namespace split
 
 // ============================================================ host side
@@ -727,7 +1082,9 @@ struct Carve {
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
-Carve carve(void* base, int nang, int n, int S) {
+// Workspace layout: A slices, B^T slices (`cbytes` bytes per complex entry: 4 for
+// BF16 pairs, 2 for INT8 pairs), row and column exponents.
+Carve carve(void* base, int nang, int n, int S, int cbytes = 4) {
   Carve c;
   c.rows = nang * n;
   c.kc = round_up(n, 16);                 // complex k (= ld of the state)
@@ -736,9 +1093,9 @@ Carve carve(void* base, int nang, int n, int S) {
   char* p = reinterpret_cast<char*>(base);
   size_t o = 0;
   c.A = reinterpret_cast<__nv_bfloat162*>(p + o);
-  o = align256(o + (size_t)S * c.rows * c.kc * sizeof(__nv_bfloat162));
+  o = align256(o + (size_t)S * c.rows * c.kc * cbytes);
   c.B = reinterpret_cast<__nv_bfloat162*>(p + o);
-  o = align256(o + (size_t)S * c.nrows * c.kc * sizeof(__nv_bfloat162));
+  o = align256(o + (size_t)S * c.nrows * c.kc * cbytes);
   c.erow = reinterpret_cast<int*>(p + o);
   o = align256(o + (size_t)c.rows * sizeof(int));
   c.fcol = reinterpret_cast<int*>(p + o);
@@ -764,17 +1121,18 @@ EncodeTiled encoder() {
   return fn;
 }
 
-// 3-D map over [S][rows][kr] BF16 with a (bk x 128 x 1) box: bk = 32 with 64-byte
-// swizzle (both kernel forms) or bk = 16 with 32-byte swizzle.
-CUtensorMap make_map(void* base, int kr, int rows, int S, int bk = split::BK) {
+// 3-D map over [S][rows][kr] elements of `esize` bytes (BF16 or INT8) with a
+// (64 bytes x 128 x 1) box and 64-byte swizzle; out-of-range boxes read zeros.
+CUtensorMap make_map(void* base, int kr, int rows, int S, int esize = 2) {
   CUtensorMap m;
   cuuint64_t dims[3] = {(cuuint64_t)kr, (cuuint64_t)rows, (cuuint64_t)S};
-  cuuint64_t strides[2] = {(cuuint64_t)kr * 2, (cuuint64_t)kr * 2 * rows};
-  cuuint32_t box[3] = {(cuuint32_t)bk, split::BM, 1};
+  cuuint64_t strides[2] = {(cuuint64_t)kr * esize, (cuuint64_t)kr * esize * rows};
+  cuuint32_t box[3] = {(cuuint32_t)(64 / esize), split::BM, 1};
   cuuint32_t estr[3] = {1, 1, 1};
-  const CUtensorMapSwizzle sw = (bk == 32) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
-  CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+  const CUtensorMapDataType dt =
+      (esize == 2) ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+  CUresult r = encoder()(&m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
   return m;
@@ -789,11 +1147,12 @@ int sm_count() {
 
 template <int S>
 void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
-               int nang, int n, int ld, double cb, double ca, int variant, cudaStream_t st) {
+               int nang, int n, int ld, double cb, double ca, int variant, const cudaEvent_t* ev,
+               cudaStream_t st) {
   Carve c = carve(w.base, nang, n, S);
   const int kr = 2 * c.kc;
   // slices of the shared potential matrix (one set for every angle)
-  split::k_col_exponents<<<ceil_div(n, 32), 256, 0, st>>>(V, n, ld, c.fcol);
+  split::k_col_exponents<<<ceil_div(n, 32), 256, 0, st>>>(V, n, ld, 1.0, c.fcol);
   {
     dim3 grid(ceil_div(c.kc, 128), n);
     split::k_slice_cols<S><<<grid, 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, c.B);
@@ -822,8 +1181,10 @@ void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V,
     }
     const int tiles = tiles_n * tiles_m;
     const int grid = std::min(tiles, sm_count());
+    if (ev) cudaEventRecord(ev[0], st);
     split::k_split_gemm_p<S><<<grid, split::P_THREADS, smem, st>>>(ta, tb, ep, kr / split::BK,
                                                                    tiles_n, tiles);
+    if (ev) cudaEventRecord(ev[1], st);
   } else {
     const size_t smem = split::smem_bytes(S);
     static bool attr[6] = {false, false, false, false, false, false};
@@ -833,8 +1194,50 @@ void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V,
       attr[S] = true;
     }
     dim3 grid(tiles_n, tiles_m);
+    if (ev) cudaEventRecord(ev[0], st);
     split::k_split_gemm<S><<<grid, split::THREADS, smem, st>>>(ta, tb, ep, kr / split::BK);
+    if (ev) cudaEventRecord(ev[1], st);
   }
+}
+
+template <int S>
+void run_split_i8(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
+                  int nang, int n, int ld, double cb, double ca, const cudaEvent_t* ev,
+                  cudaStream_t st) {
+  Carve c = carve(w.base, nang, n, S, 2);
+  const int kr = 2 * c.kc;
+  uint16_t* B = reinterpret_cast<uint16_t*>(c.B);
+  uint32_t* A = reinterpret_cast<uint32_t*>(c.A);
+  split::k_col_exponents<<<ceil_div(n, 32), 256, 0, st>>>(V, n, ld, split::kDigitHeadroom,
+                                                          c.fcol);
+  {
+    dim3 grid(ceil_div(c.kc, 128), n);
+    split::k_slice_cols_i8<S><<<grid, 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, B);
+  }
+  split::k_slice_rows_i8<S><<<ceil_div(c.rows, 8), 256, 0, st>>>(Q, c.rows, n, ld, kr, A, c.erow);
+  CUtensorMap ta = make_map(c.A, kr, c.rows, S, 1);
+  CUtensorMap tb = make_map(c.B, kr, c.nrows, S, 1);
+  split::EpiArgs ep{Q, P, Qo, V, D, c.erow, c.fcol, w.status, c.rows, n, ld, c.kc, S, cb, ca};
+  const int tiles_n = c.nrows / split::NT, tiles_m = ceil_div(c.rows, split::BM);
+  const size_t smem = split::i8::smem_bytes(S);
+  static bool attr[6] = {false, false, false, false, false, false};
+  if (!attr[S]) {
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, split::k_split_gemm_i8<S>) != cudaSuccess ||
+        fa.numRegs < split::P_REG_LAUNCH)
+      throw std::runtime_error("INT8 split kernel built with " + std::to_string(fa.numRegs) +
+                               " registers per thread, needs " +
+                               std::to_string(split::P_REG_LAUNCH));
+    cudaFuncSetAttribute(split::k_split_gemm_i8<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr[S] = true;
+  }
+  const int tiles = tiles_n * tiles_m;
+  const int grid = std::min(tiles, sm_count());
+  if (ev) cudaEventRecord(ev[0], st);
+  split::k_split_gemm_i8<S><<<grid, split::P_THREADS, smem, st>>>(
+      ta, tb, ep, ceil_div(kr, split::i8::BK), tiles_n, tiles);
+  if (ev) cudaEventRecord(ev[1], st);
 }
 
 }  // namespace
@@ -859,18 +1262,31 @@ SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, un
 
 int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
                 int nang, int n, int ld, double cb, double ca, int slices, int variant,
-                cudaStream_t st) {
+                const cudaEvent_t* ev, cudaStream_t st) {
+  if (variant == kSplitInt8) {
+    switch (slices) {
+      case 3:
+        run_split_i8<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, st);
+        break;
+      case 4:
+        run_split_i8<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, st);
+        break;
+      default:
+        throw std::invalid_argument("INT8 split slices must be 3 or 4");
+    }
+    return 4;
+  }
   if (variant != kSplitPersistent && variant != kSplitPerTile)
     throw std::invalid_argument("unknown split kernel variant");
   switch (slices) {
     case 3:
-      run_split<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, variant, st);
+      run_split<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, variant, ev, st);
       break;
     case 4:
-      run_split<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, variant, st);
+      run_split<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, variant, ev, st);
       break;
     case 5:
-      run_split<5>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, variant, st);
+      run_split<5>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, variant, ev, st);
       break;
     default:
       throw std::invalid_argument("split slices must be 3, 4 or 5");

@@ -22,12 +22,15 @@ SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, un
 //     are drained to registers and the FP64 update runs during the next tile's MMAs;
 //   kSplitPerTile: one CTA per tile, the epilogue after the tile's MMAs.
 // Both use three FP32 accumulators (slice pairs with s+t = 0, 1, >= 2).
-enum SplitVariant { kSplitPersistent = 0, kSplitPerTile = 1 };
+//   kSplitInt8: the persistent form on signed 8-bit digits (kind::i8), one exact
+//     INT32 accumulator per digit level s+t (3 or 4 slices).
+enum SplitVariant { kSplitPersistent = 0, kSplitPerTile = 1, kSplitInt8 = 2 };
 
-// P += cb*(Q V + Q o D_a) with the potential product from BF16 slices; Qo = Q + ca*P.
-// Returns the number of kernels launched.
+// P += cb*(Q V + Q o D_a) with the potential product from BF16 or INT8 slices;
+// Qo = Q + ca*P.  When `ev` is given, ev[0] and ev[1] are recorded around the
+// tensor-core kernel.  Returns the number of kernels launched.
 int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
                 int nang, int n, int ld, double cb, double ca, int slices, int variant,
-                cudaStream_t st);
+                const cudaEvent_t* ev, cudaStream_t st);
 
 }  // namespace trhepd

@@ -17,11 +17,13 @@ LIB = HERE / "_lib" / "libtrhepd_b200.so"
 
 FP64 = 0
 SPLIT_BF16 = 1
+SPLIT_INT8 = 2
 OPT_RENORM_POLICY = 1
 OPT_RENORM_TAU = 2
 OPT_SPLIT_SLICES = 3
 OPT_PROFILE = 4
 OPT_SPLIT_KERNEL = 5
+OPT_GRAPHS = 6
 
 # every symbol include/trhepd_b200.h declares
 EXPORTS = [
@@ -157,7 +159,7 @@ class Context:
         return {"renormalisations": int(out[0]), "stage_products": int(out[1]),
                 "device_ms": float(out[2]), "stage_columns": int(out[3]),
                 "stage_kernel_ms": float(out[4]), "launches": int(out[5]),
-                "renorm_launches": int(out[6])}
+                "renorm_launches": int(out[6]), "tensor_kernel_ms": float(out[7])}
 
     def surf_run(self, bulkp, surf, dz2: float, int_method: int = 5, precision: int = FP64,
                  out_path=None):
