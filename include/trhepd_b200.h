@@ -52,9 +52,12 @@ enum trhepd_option {
   TRHEPD_OPT_SPLIT_KERNEL = 5,  /* BF16 split kernel: 0 persistent, one CTA per SM, epilogue of
                                    a tile overlapped with the next tile's MMAs (default);
                                    1 one CTA per tile */
-  TRHEPD_OPT_GRAPHS = 6         /* nonzero (default): a resident problem's solve is captured
+  TRHEPD_OPT_GRAPHS = 6,        /* nonzero (default): a resident problem's solve is captured
                                    into a CUDA graph on its second solve with the same
                                    options and replayed afterwards; 0: launch directly */
+  TRHEPD_OPT_FUSED_MAX_N = 7    /* FP64 RKN solves (int_method 5, 6) with 2 <= nb <= this value
+                                   (at most 64; default 64, 0 disables) integrate every slice in
+                                   one launch, one CTA per angle, state in shared memory */
 };
 
 typedef struct trhepd_context trhepd_context;

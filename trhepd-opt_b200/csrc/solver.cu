@@ -22,6 +22,7 @@
 #include "bulk_model.h"
 #include "host_model.h"
 #include "kernels.h"
+#include "small.h"
 #include "split_gemm.h"
 
 using namespace trhepd;
@@ -169,6 +170,7 @@ struct trhepd_context {
   int split_variant = kSplitPersistent;
   int profile = 0;               // 1: time every stage-product launch with events
   int graphs = 1;                // 1: replay resident solves from a captured CUDA graph
+  int fused_max_n = kFusedMaxBeams;  // FP64 RKN solves with n <= this run fused (0: never)
   double stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<cudaEvent_t> evpool;
   // device buffers (grown on demand, reused across calls)
@@ -581,6 +583,31 @@ void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) 
   const double dz = Pb.dz;
   begin_run(C, Pb, precision, I.s * Pb.ns, R);
   const bool every_slice = (Pb.n == 1 && Pb.int_method == 6);  // hp_int_spa1d renormalises each slice
+  if (!R.split && Pb.n >= 2 && Pb.n <= std::min(C->fused_max_n, kFusedMaxBeams)) {
+    // whole integration in one launch, state in shared memory (small.cu)
+    FusedRkn f{};
+    f.Q = R.Q;
+    f.P = R.P;
+    f.table = R.table;
+    f.pair = R.pair;
+    f.D = R.D;
+    f.status = R.status;
+    f.n = R.n;
+    f.ld = R.ld;
+    f.nv = R.nv;
+    f.nang = R.nang;
+    f.ns = R.ns;
+    f.s = I.s;
+    f.policy = C->renorm_policy;
+    f.interval = R.interval;
+    f.dz = dz;
+    for (int q = 0; q < 2 * I.s + 1; ++q) f.bab[q] = I.bab[q];
+    R.launches += launch_fused_rkn(f, R.st);
+    R.products += (long)I.s * R.ns - 1;
+    R.renorms += (C->renorm_policy == 1) ? (R.ns - 1) / R.interval : R.ns - 1;
+    finish_device(C, Pb, R);
+    return;
+  }
   for (int l = 1; l <= R.ns; ++l) {
     for (int k = 1; k <= I.s; ++k) {
       const int col = I.s * (l - 1) + k - 1;
@@ -794,7 +821,7 @@ std::vector<void*> buffer_signature(const trhepd_context* C) {
 void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
   const std::vector<double> key = {(double)precision, (double)C->split_slices,
                                    (double)C->split_variant, (double)C->renorm_policy,
-                                   C->renorm_tau};
+                                   C->renorm_tau, (double)C->fused_max_n};
   if (!C->graphs || C->profile) {
     Pb.drop_graph();
     RunState R;
@@ -1305,6 +1332,10 @@ int trhepd_set_option(trhepd_context* c, int option, double value) {
       return TRHEPD_OK;
     case TRHEPD_OPT_GRAPHS:
       c->graphs = value != 0.0;
+      return TRHEPD_OK;
+    case TRHEPD_OPT_FUSED_MAX_N:
+      if (value < 0) return fail(c, TRHEPD_EINVAL, "fused beam limit must be >= 0");
+      c->fused_max_n = (int)value;
       return TRHEPD_OK;
   }
   return fail(c, TRHEPD_EINVAL, "unknown option");

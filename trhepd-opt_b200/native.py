@@ -24,6 +24,7 @@ OPT_SPLIT_SLICES = 3
 OPT_PROFILE = 4
 OPT_SPLIT_KERNEL = 5
 OPT_GRAPHS = 6
+OPT_FUSED_MAX_N = 7
 
 # every symbol include/trhepd_b200.h declares
 EXPORTS = [
