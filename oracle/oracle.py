@@ -128,6 +128,12 @@ def bulk_run(bulk_txt, out_path) -> None:
         raise RuntimeError("oracle bulk: " + err.value.decode())
 
 
+def set_bulk_scale(s: float) -> None:
+    """Rescale the bulk slice potentials by s in bulk_run (1 = off); a scale of
+    1 + 2^-50 measures the rounding sensitivity of each bulk record."""
+    lib().oracle_set_bulk_scale(ctypes.c_double(s))
+
+
 def set_max_slices(n: int) -> None:
     """Integrate only the first n slices (0 = all); for bounded timing samples."""
     lib().oracle_set_max_slices(int(n))

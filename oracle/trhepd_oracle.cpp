@@ -774,6 +774,7 @@ static const double kRkn611[23] = {
 // every k slices regardless of the estimate (used to study how the result depends
 // on where renormalisation happens).
 static int g_renorm_every = 0;
+static double g_bulk_scale = 1.0;  // bulk potential rescale (conditioning tests only)
 
 // Test knob: emulate the split-precision stage product.  0 = off (default,
 // plain zgemm).  S > 0: the potential part of Q*M is formed from S fixed-point
@@ -2017,6 +2018,13 @@ static void bulk_run(const std::string& bulk_txt, const std::string& out_path) {
       scpot(nv, nv, vv, vvi, natm, ielm.data(), z.data(), zi - cc, E, asf, 1.0, Ghk, ocr.data(),
             s3.data());
     }
+    // test knob: a rounding-level rescale of the slice potentials, which shows how
+    // much each record moves under perturbations of that size (conditioning)
+    if (g_bulk_scale != 1.0)
+      for (size_t q = 0; q < v.size(); ++q) {
+        v[q] *= g_bulk_scale;
+        vi[q] *= g_bulk_scale;
+      }
     // blkref angle loop (bulk.f90:24-126); the work of every (angle, group) is
     // independent, so it is computed in parallel and written in file order.
     double azr = azi + rdom[idom];
@@ -2077,6 +2085,7 @@ struct OracleSurface {
 extern "C" {
 
 void oracle_set_renorm_every(int k) { g_renorm_every = k; }
+void oracle_set_bulk_scale(double s) { g_bulk_scale = s; }
 
 // Plane-group images in 1x1-lattice units (strfac.f90:15-64); returns the count.
 int oracle_plane_group_images(int nsg, int ma, int mb, int na, int nb, double x, double y,

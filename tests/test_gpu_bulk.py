@@ -4,8 +4,10 @@ The reference's bulkP.b files (tests/golden/*/bulkP.b, written by the original
 eigen-decomposition path of trmat, sim-trhepd-rheed/src/bulk.f90:130-264) pin the
 reflection records; the GPU builds the slice transfer matrix from the matrix
 cosine/sine series instead of eigenvectors, so records agree to rounding of
-the two constructions.  Header records must be byte-identical.  Synthetic
-structures are checked against the oracle's restatement.
+the two constructions, amplified by the conditioning of the layer recursion.
+Header records must be byte-identical.  Synthetic structures are checked against
+the oracle's restatement, with bounds set by the oracle's own rounding
+sensitivity (a 2^-50 rescale of the potential).
 """
 from __future__ import annotations
 
@@ -66,17 +68,86 @@ def test_bulk_golden(golden, ctx, tmp_path, case, tol):
     assert worst <= tol, worst
 
 
+def golden_variant(src, seed: int) -> str:
+    """A seeded variant of a reference bulk.txt: Debye-Waller factors, atom heights
+    and glancing-angle range redrawn, beams and cell kept (such structures keep the
+    layer recursion well-conditioned, unlike the synthetic cells below)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for line in open(src).read().split("\n"):
+        if "BH(I)" in line:
+            b = rng.uniform(0.3, 1.0)
+            line = f"{b:.4f},{b:.4f},{b:.4f}\t\t\t,BH(I),BK(I),BZ(I)"
+        elif "IELM(I),ocr(I),X(I),Y(I),Z(I)" in line:
+            f = line.split(",")
+            f[4] = f"  {float(f[4].split()[0]) + rng.uniform(-0.1, 0.1):.5f}\t\t"
+            line = ",".join(f)
+        elif "BE,AZI" in line:
+            f = line.split(",")
+            gi = rng.uniform(0.1, 2.0)
+            f[4], f[5], f[6] = f"{gi:.2f}", f"{gi + rng.integers(3, 8) * 0.3:.2f}", "0.3\t\t\t"
+            line = ",".join(f)
+        out.append(line)
+    return "\n".join(out)
+
+
+def sensitivity(oracle_mod, bulk_txt, tmp_path):
+    """The oracle's records and how far each entry moves when the slice potentials
+    are rescaled by 1 + 2^-50: the rounding sensitivity of the problem itself."""
+    a, b = tmp_path / "oracle.b", tmp_path / "oracle_pert.b"
+    oracle_mod.set_bulk_scale(1.0)
+    oracle_mod.bulk_run(bulk_txt, a)
+    oracle_mod.set_bulk_scale(1.0 + 2.0 ** -50)
+    try:
+        oracle_mod.bulk_run(bulk_txt, b)
+    finally:
+        oracle_mod.set_bulk_scale(1.0)
+    return records(a), records(b)
+
+
+@pytest.mark.parametrize("case,seed", [("test23", 1), ("test23", 2), ("test47", 1)])
+def test_bulk_synthetic_vs_oracle(oracle_mod, ctx, golden, tmp_path, case, seed):
+    """Seeded variants of the reference structures, tight bound (the oracle's own
+    rounding sensitivity on them is below 1e-9)."""
+    bulk_txt = tmp_path / "bulk.txt"
+    bulk_txt.write_text(golden_variant(golden / case / "bulk.txt", seed))
+    ours = tmp_path / "gpu.b"
+    ctx.bulk_run(bulk_txt, ours)
+    ref, pert = sensitivity(oracle_mod, bulk_txt, tmp_path)
+    _, sens = compare(pert, ref)
+    assert sens <= 1e-9, sens  # the case is well-conditioned
+    nnum, worst = compare(records(ours), ref)
+    assert nnum > 0
+    assert worst <= 1e-8, worst
+
+
 @pytest.mark.parametrize("n,seed", [(23, 5), (95, 7)])
-def test_bulk_synthetic_vs_oracle(oracle_mod, ctx, tmp_path, n, seed):
+def test_bulk_ill_conditioned_within_sensitivity(oracle_mod, ctx, tmp_path, n, seed):
+    """The synthetic 2x2 cells have strongly evanescent bulk beams (decay constants
+    up to ~15/A over a 3.14 A layer): the reference's own records move by up to
+    O(1) under a 2^-50 rescale of the potential.  Each entry must then agree with
+    the oracle within 1e-8 of its record maximum plus 64 times that entry's
+    sensitivity, and entries the rescale leaves unchanged must agree tightly."""
     from trhepd_opt_b200 import generator
     s = generator.dense(n, seed=seed, n_angles=7, region=4.0, dz=0.02)
     bulk_txt, _ = s.write(tmp_path)
-    ours, theirs = tmp_path / "gpu.b", tmp_path / "oracle.b"
+    ours = tmp_path / "gpu.b"
     ctx.bulk_run(bulk_txt, ours)
-    oracle_mod.bulk_run(bulk_txt, theirs)
-    nnum, worst = compare(records(ours), records(theirs))
+    ref, pert = sensitivity(oracle_mod, bulk_txt, tmp_path)
+    mine = records(ours)
+    assert len(mine) == len(ref)
+    nnum = 0
+    for x, y, z in zip(mine, ref, pert):
+        if x == y:
+            continue
+        assert len(x) == len(y) and len(x) % 16 == 0
+        xa, ya, za = (np.frombuffer(v, np.complex128) for v in (x, y, z))
+        assert np.isfinite(xa).all()
+        scale = max(np.abs(ya).max(), 1e-300)
+        bound = 1e-8 * scale + 64.0 * np.abs(za - ya)
+        assert (np.abs(xa - ya) <= bound).all(), float((np.abs(xa - ya) / bound).max())
+        nnum += 1
     assert nnum > 0
-    assert worst <= 1e-8, worst
 
 
 def test_bulk_then_surface(golden, ctx, oracle_mod, tmp_path):

@@ -38,3 +38,33 @@ def test_bulk_records(golden, oracle_mod, tmp_path, case, tol):
         xa, ya = np.frombuffer(x, np.complex128), np.frombuffer(y, np.complex128)
         worst = max(worst, np.abs(xa - ya).max() / max(np.abs(ya).max(), 1e-300))
     assert worst <= tol, worst
+
+
+def test_bulk_conditioning(golden, oracle_mod, tmp_path):
+    """The reference's bulk records are well-conditioned on its own structures and
+    not on strongly evanescent synthetic cells: a 2^-50 rescale of the slice
+    potentials moves test23's records by < 1e-10 and a synthetic 2x2 cell's by
+    > 1e-4 (the bound the GPU bulk tests derive their tolerances from)."""
+    from trhepd_opt_b200 import generator
+
+    def sens(bulk_txt, d):
+        d.mkdir(exist_ok=True)
+        oracle_mod.set_bulk_scale(1.0)
+        oracle_mod.bulk_run(bulk_txt, d / "a.b")
+        oracle_mod.set_bulk_scale(1.0 + 2.0 ** -50)
+        try:
+            oracle_mod.bulk_run(bulk_txt, d / "b.b")
+        finally:
+            oracle_mod.set_bulk_scale(1.0)
+        worst = 0.0
+        for x, y in zip(records(d / "a.b"), records(d / "b.b")):
+            if x != y:
+                xa, ya = np.frombuffer(x, np.complex128), np.frombuffer(y, np.complex128)
+                worst = max(worst, float(np.abs(xa - ya).max() / np.abs(xa).max()))
+        return worst
+
+    assert sens(golden / "test23" / "bulk.txt", tmp_path / "g") < 1e-10
+    s = generator.dense(23, seed=5, n_angles=7, region=4.0, dz=0.02)
+    bulk_txt, _ = s.write(tmp_path / "s")
+    assert sens(bulk_txt, tmp_path / "s") > 1e-4
+
