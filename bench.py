@@ -493,6 +493,8 @@ def main():
                                          native.FP64: "fp64"}[prec],
                            "split_slices": slices if split else None,
                            "renormalisation": "growth bound ln(1e3)",
+                           "renormalisations_per_solve": stp["renormalisations"],
+                           "stage_products_per_solve": stp["stage_products"],
                            "bulk_boundary": "non-reflecting bulk records (f = 0)",
                            "l2": "inputs larger than L2 (state + stage table > 1 GB)",
                            "parallelism": f"replicas x{ws}"},

@@ -754,17 +754,22 @@ __device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint6
       : "memory");
 }
 
-// Balanced base-256 digits of rint(x 2^(7 - e + 8(S-1))), most significant first.
+// Balanced base-256 digits of X = rint(x * scale), scale = 2^(7 - e + 8(S-1)),
+// most significant first.  |X| < 2^(7 + 8(S-1)) fits 32 bits for S <= 4.
 template <int S>
-__device__ __forceinline__ void digits_i8(double x, int e, int* d) {
-  long long X = __double2ll_rn(ldexp(x, 7 - e + 8 * (S - 1)));
+__device__ __forceinline__ void digits_i8(double x, double scale, int* d) {
+  static_assert(S <= 4, "32-bit digit arithmetic");
+  int X = __double2int_rn(x * scale);
 #pragma unroll
   for (int s = S - 1; s >= 1; --s) {
-    const int lo = (int)((X + 128) & 255) - 128;
+    const int lo = ((X + 128) & 255) - 128;
     d[s] = lo;
     X = (X - lo) >> 8;
   }
-  d[0] = (int)X;
+  d[0] = X;
+}
+__device__ __forceinline__ double digit_scale(int e, int S) {
+  return pow2(7 - e + 8 * (S - 1));
 }
 __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
   return (uint32_t)(a & 255) | ((uint32_t)(b & 255) << 8) | ((uint32_t)(c & 255) << 16) |
@@ -791,39 +796,56 @@ __global__ void k_slice_rows_i8(const cd* __restrict__ Q, int rows, int n, int l
   int e = 0;
   if (m > 0.0) frexp(m * kDigitHeadroom, &e);
   if (lane == 0) erow[r] = e;
+  const double sc = digit_scale(e, S);
   const int kw = kr / 4;      // 32-bit words per slice row (two complex k each)
   for (int w = lane; w < kw; w += 32) {
     const int k0 = 2 * w, k1 = 2 * w + 1;
     const cd v0 = (k0 < n && k0 != i) ? q[k0] : cd{0.0, 0.0};
     const cd v1 = (k1 < n && k1 != i) ? q[k1] : cd{0.0, 0.0};
     int a[S], b[S], c[S], d[S];
-    digits_i8<S>(v0.x, e, a);
-    digits_i8<S>(v0.y, e, b);
-    digits_i8<S>(v1.x, e, c);
-    digits_i8<S>(v1.y, e, d);
+    digits_i8<S>(v0.x, sc, a);
+    digits_i8<S>(v0.y, sc, b);
+    digits_i8<S>(v1.x, sc, c);
+    digits_i8<S>(v1.y, sc, d);
 #pragma unroll
     for (int s = 0; s < S; ++s) A[((size_t)s * rows + r) * kw + w] = pack4(a[s], b[s], c[s], d[s]);
   }
 }
 
-// B^T digit slices: row 2j (Re-out) = [Vr(k,j), -Vi(k,j)]_k, row 2j+1 (Im-out) =
-// [Vi, Vr]_k; -Vi gets its own digits (negating digits could leave 128).
+// One block per column j of Voff: the column exponent (maximum times the
+// headroom), then the B^T digit slices: row 2j (Re-out) = [Vr(k,j), -Vi(k,j)]_k,
+// row 2j+1 (Im-out) = [Vi, Vr]_k; -Vi gets its own digits (negating digits could
+// leave 128).
 template <int S>
-__global__ void k_slice_cols_i8(const cd* __restrict__ V, int n, int ld, int kc, int nrows,
-                                const int* __restrict__ fcol, uint16_t* __restrict__ B) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
-  if (k >= kc || j >= n) return;
-  const cd v = (k < n) ? V[(size_t)k * ld + j] : cd{0.0, 0.0};
-  const int e = fcol[j];
-  int dr[S], di[S], dn[S];
-  digits_i8<S>(v.x, e, dr);
-  digits_i8<S>(v.y, e, di);
-  digits_i8<S>(-v.y, e, dn);
+__global__ void __launch_bounds__(128) k_slice_cols_i8(const cd* __restrict__ V, int n, int ld,
+                                                        int kc, int nrows, int* __restrict__ fcol,
+                                                        uint16_t* __restrict__ B) {
+  __shared__ double red[4];
+  const int j = blockIdx.x, tid = threadIdx.x;
+  double m = 0.0;
+  for (int k = tid; k < n; k += 128) {
+    const cd v = V[(size_t)k * ld + j];
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((tid & 31) == 0) red[tid >> 5] = m;
+  __syncthreads();
+  m = fmax(fmax(red[0], red[1]), fmax(red[2], red[3]));
+  int e = 0;
+  if (m > 0.0) frexp(m * kDigitHeadroom, &e);
+  if (tid == 0) fcol[j] = e;
+  const double sc = digit_scale(e, S);
+  for (int k = tid; k < kc; k += 128) {
+    const cd v = (k < n) ? V[(size_t)k * ld + j] : cd{0.0, 0.0};
+    int dr[S], di[S], dn[S];
+    digits_i8<S>(v.x, sc, dr);
+    digits_i8<S>(v.y, sc, di);
+    digits_i8<S>(-v.y, sc, dn);
 #pragma unroll
-  for (int s = 0; s < S; ++s) {
-    B[((size_t)s * nrows + 2 * j) * kc + k] = pack2(dr[s], dn[s]);
-    B[((size_t)s * nrows + 2 * j + 1) * kc + k] = pack2(di[s], dr[s]);
+    for (int s = 0; s < S; ++s) {
+      B[((size_t)s * nrows + 2 * j) * kc + k] = pack2(dr[s], dn[s]);
+      B[((size_t)s * nrows + 2 * j + 1) * kc + k] = pack2(di[s], dr[s]);
+    }
   }
 }
 
@@ -1020,12 +1042,20 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&tempty);
+      cd qd[2][2];  // diagonal of each of this lane's rows
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int r = m0 + 16 * h + 8 * u + t1;
+          qd[h][u] = (r < ep.rows) ? ep.Q[(size_t)r * ep.ld + ri[h][u]] : cd{0.0, 0.0};
+        }
 #pragma unroll
       for (int g = 0; g < 8; ++g) {
         const int j = jh + 4 * g + t0;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          cd qv[2], pv[2], qd[2], vv[2], dv[2];
+          cd qv[2], pv[2], vv[2], dv[2];
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
             const int r = m0 + 16 * h + 8 * u + t1;
@@ -1033,7 +1063,6 @@ __global__ void __launch_bounds__(P_THREADS, 1)
               const size_t ro = (size_t)r * ep.ld;
               qv[u] = ep.Q[ro + j];
               pv[u] = ep.P[ro + j];
-              qd[u] = ep.Q[ro + ri[h][u]];
               vv[u] = ep.V[(size_t)ri[h][u] * ep.ld + j];
               dv[u] = ep.D[(size_t)ra[h][u] * ep.ld + j];
             }
@@ -1043,7 +1072,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
             const int r = m0 + 16 * h + 8 * u + t1;
             if (r < ep.rows && j < ep.n) {
               const size_t ro = (size_t)r * ep.ld;
-              const cd acc = vals[g][h][u] + qd[u] * vv[u] + qv[u] * (dv[u] + vd);
+              const cd acc = vals[g][h][u] + qd[h][u] * vv[u] + qv[u] * (dv[u] + vd);
               const cd p = pv[u] + ep.cb * acc;
               ep.P[ro + j] = p;
               ep.Qo[ro + j] = qv[u] + ep.ca * p;
@@ -1208,12 +1237,7 @@ void run_split_i8(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd*
   const int kr = 2 * c.kc;
   uint16_t* B = reinterpret_cast<uint16_t*>(c.B);
   uint32_t* A = reinterpret_cast<uint32_t*>(c.A);
-  split::k_col_exponents<<<ceil_div(n, 32), 256, 0, st>>>(V, n, ld, split::kDigitHeadroom,
-                                                          c.fcol);
-  {
-    dim3 grid(ceil_div(c.kc, 128), n);
-    split::k_slice_cols_i8<S><<<grid, 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, B);
-  }
+  split::k_slice_cols_i8<S><<<n, 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, B);
   split::k_slice_rows_i8<S><<<ceil_div(c.rows, 8), 256, 0, st>>>(Q, c.rows, n, ld, kr, A, c.erow);
   CUtensorMap ta = make_map(c.A, kr, c.rows, S, 1);
   CUtensorMap tb = make_map(c.B, kr, c.nrows, S, 1);
