@@ -55,9 +55,12 @@ enum trhepd_option {
   TRHEPD_OPT_GRAPHS = 6,        /* nonzero (default): a resident problem's solve is captured
                                    into a CUDA graph on its second solve with the same
                                    options and replayed afterwards; 0: launch directly */
-  TRHEPD_OPT_FUSED_MAX_N = 7    /* FP64 RKN solves (int_method 5, 6) with 2 <= nb <= this value
+  TRHEPD_OPT_FUSED_MAX_N = 7,   /* FP64 RKN solves (int_method 5, 6) with 2 <= nb <= this value
                                    (at most 64; default 64, 0 disables) integrate every slice in
                                    one launch, one CTA per angle, state in shared memory */
+  TRHEPD_OPT_STREAM_PRIORITY = 8 /* 0 (default, lowest) .. 1 (highest): priority of the
+                                   context's stream; the block scheduler starts pending work of
+                                   higher-priority streams first when several contexts share a GPU */
 };
 
 typedef struct trhepd_context trhepd_context;

@@ -1333,6 +1333,23 @@ int trhepd_set_option(trhepd_context* c, int option, double value) {
     case TRHEPD_OPT_GRAPHS:
       c->graphs = value != 0.0;
       return TRHEPD_OK;
+    case TRHEPD_OPT_STREAM_PRIORITY: {
+      // replace the context's stream by one of the given priority (graphs are not
+      // bound to a stream and stay valid)
+      if (value < 0 || value > 1) return fail(c, TRHEPD_EINVAL, "stream priority must be in [0, 1]");
+      int least = 0, greatest = 0;
+      cudaSetDevice(c->device);
+      if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess)
+        return fail(c, TRHEPD_ECUDA, "stream priority range unavailable");
+      const int prio = least + (int)std::lround(value * (greatest - least));
+      cudaStream_t ns = nullptr;
+      if (cudaStreamCreateWithPriority(&ns, cudaStreamNonBlocking, prio) != cudaSuccess)
+        return fail(c, TRHEPD_ECUDA, "cudaStreamCreateWithPriority failed");
+      cudaStreamSynchronize(c->stream);
+      cudaStreamDestroy(c->stream);
+      c->stream = ns;
+      return TRHEPD_OK;
+    }
     case TRHEPD_OPT_FUSED_MAX_N:
       if (value < 0) return fail(c, TRHEPD_EINVAL, "fused beam limit must be >= 0");
       c->fused_max_n = (int)value;

@@ -25,6 +25,7 @@ OPT_PROFILE = 4
 OPT_SPLIT_KERNEL = 5
 OPT_GRAPHS = 6
 OPT_FUSED_MAX_N = 7
+OPT_STREAM_PRIORITY = 8
 
 # every symbol include/trhepd_b200.h declares
 EXPORTS = [

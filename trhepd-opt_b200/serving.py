@@ -10,12 +10,19 @@ data; trhepd_problem_*), is solved, and its intensities are returned.  The
 bulk boundary of a (base structure, angle grid) is written once and reused by
 every candidate of that base.
 
+Scheduling keeps small requests from queueing behind large ones: a free slot
+takes the oldest pending request of the smallest beam count first, at most
+`slots - 1` slots run large requests (N >= `large_n`) at once, and each solve
+runs on a stream whose priority falls with N, so the block scheduler starts the
+kernels of small requests first.  Requests with N <= 64 run the fused FP64
+kernel whatever the server's precision (one launch per solve, exact FP64);
+larger ones use the server's precision form.
+
 Latency is completion minus arrival; the report gives p50/p99 and angle-solves/s.
 """
 from __future__ import annotations
 
 import dataclasses
-import queue
 import tempfile
 import threading
 import time
@@ -71,16 +78,80 @@ def poisson_stream(rate: float, duration: float, seed: int = 0, mix=None,
         rid += 1
 
 
+FUSED_MAX_N = 64
+# stream priority (0 lowest .. 1 highest) by beam count
+PRIORITY = ((64, 1.0), (95, 0.75), (191, 0.5))
+
+
+def priority_for(n: int) -> float:
+    for limit, p in PRIORITY:
+        if n <= limit:
+            return p
+    return 0.0
+
+
+class _Pending:
+    """Pending requests; workers take the smallest beam count first (oldest first
+    within it), large requests only while fewer than `large_cap` are running."""
+
+    def __init__(self, large_n: int, large_cap: int):
+        self.items: list = []
+        self.cv = threading.Condition()
+        self.unfinished = 0
+        self.large_n, self.large_cap, self.large_running = large_n, large_cap, 0
+
+    def put(self, r) -> None:
+        with self.cv:
+            self.items.append(r)
+            if r is not None:
+                self.unfinished += 1
+            self.cv.notify_all()
+
+    def get(self):
+        with self.cv:
+            while True:
+                if any(r is None for r in self.items) and all(
+                        r is None for r in self.items):
+                    self.items.remove(None)
+                    return None
+                pick = None
+                for r in self.items:
+                    if r is None:
+                        continue
+                    if r.n >= self.large_n and self.large_running >= self.large_cap:
+                        continue
+                    if pick is None or r.n < pick.n:
+                        pick = r
+                if pick is not None:
+                    self.items.remove(pick)
+                    if pick.n >= self.large_n:
+                        self.large_running += 1
+                    return pick
+                self.cv.wait(timeout=0.5)
+
+    def task_done(self, r) -> None:
+        with self.cv:
+            if r.n >= self.large_n:
+                self.large_running -= 1
+            self.unfinished -= 1
+            self.cv.notify_all()
+
+    def join(self) -> None:
+        with self.cv:
+            while self.unfinished:
+                self.cv.wait(timeout=0.5)
+
+
 class Server:
     def __init__(self, device: int = 0, slots: int = 4, mem_budget_gb: float = 120.0,
                  precision: int = native.FP64, region: float = 15.0, dz: float = 0.02,
-                 renorm_policy: int = 1):
+                 renorm_policy: int = 1, large_n: int = 191):
         self.device, self.slots, self.precision = device, slots, precision
         self.region, self.dz = region, dz
         self.budget = mem_budget_gb * 1e9
         self.in_use = 0.0
         self.cv = threading.Condition()
-        self.q: queue.Queue = queue.Queue()
+        self.q = _Pending(large_n, max(1, slots - 1))
         self.tmp = Path(tempfile.mkdtemp(prefix="trhepd_serve_"))
         self.bulk_cache: dict = {}
         self.bulk_lock = threading.Lock()
@@ -136,6 +207,10 @@ class Server:
             self.in_use -= need
             self.cv.notify_all()
 
+    def precision_for(self, n: int) -> int:
+        """The form a request of n beams runs in: fused FP64 up to 64 beams."""
+        return native.FP64 if n <= FUSED_MAX_N else self.precision
+
     def _work(self, ctx: native.Context) -> None:
         while True:
             r = self.q.get()
@@ -149,8 +224,9 @@ class Server:
                                          6 * sp.args.ns + 1)
                 self._admit(need)
                 r.start = time.perf_counter() - self.t0
+                ctx.set_option(native.OPT_STREAM_PRIORITY, priority_for(r.n))
                 rp = sp.resident()
-                rp.solve(self.precision)
+                rp.solve(self.precision_for(r.n))
                 r.device_ms = ctx.last_stats()["device_ms"]
                 _, r.f2 = rp.fetch()
                 rp.close()
@@ -163,7 +239,7 @@ class Server:
                 r.finish = time.perf_counter() - self.t0
                 with self.cv:
                     self.done.append(r)
-                self.q.task_done()
+                self.q.task_done(r)
 
     def close(self) -> None:
         for _ in self.workers:
