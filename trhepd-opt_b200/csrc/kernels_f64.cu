@@ -411,7 +411,7 @@ void launch_cond_est(const cd* Q, int nang, int n, int ld, int force, int* flag,
 //   C1 <- W1 C1,   C2 <- C2 - L2 C1
 // to all remaining columns (Q columns right of the panel and every P column).
 constexpr int kW = 16;
-constexpr int kUpdCols = 64;
+constexpr int kUpdCols = 128;  // trailing columns per update block
 
 struct GJScratch {
   int* piv;   // nang x kW
@@ -563,69 +563,81 @@ __global__ void k_gj_panel(const cd* __restrict__ Q, const int* __restrict__ fla
 }
 
 // Each CTA owns kUpdCols of the remaining columns of one angle.
-__global__ void k_gj_update(cd* __restrict__ Q, cd* __restrict__ P, const int* __restrict__ flag,
-                            int n, int ld, int c0, int w, GJScratch sc) {
+// One thread per column of the trailing matrix (Q columns right of the panel,
+// then every P column), 128 columns per block: the column's pivot-row values C1
+// stay in registers; the multipliers L2 of 32 rows at a time are staged in shared
+// memory and read as broadcasts.
+constexpr int kUpdRows = 32;
+__global__ void __launch_bounds__(kUpdCols) k_gj_update(cd* __restrict__ Q, cd* __restrict__ P,
+                                                        const int* __restrict__ flag, int n,
+                                                        int ld, int c0, int w, GJScratch sc) {
   const int a = blockIdx.y;
   if (flag && !flag[a]) return;
   const int qrest = n - (c0 + w);          // Q columns right of the panel
-  const int vc = blockIdx.x * kUpdCols + threadIdx.x % kUpdCols;  // virtual column
+  const int vc = blockIdx.x * kUpdCols + threadIdx.x;  // virtual column
   const int total = qrest + n;
-  __shared__ cd C1[kW][kUpdCols];
   __shared__ cd W1[kW * kW];
+  __shared__ cd Ls[kUpdRows][kW];
   __shared__ int piv[kW];
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int e = tid; e < kW * kW; e += nt) W1[e] = sc.W1[(size_t)a * kW * kW + e];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < kW * kW; e += kUpdCols) W1[e] = sc.W1[(size_t)a * kW * kW + e];
   if (tid < kW) piv[tid] = sc.piv[a * kW + tid];
   __syncthreads();
   const bool valid = vc < total;
   cd* base = nullptr;
   if (valid) base = (vc < qrest) ? Q + (size_t)a * n * ld + (c0 + w + vc)
                                  : P + (size_t)a * n * ld + (vc - qrest);
-  const int lane_col = tid % kUpdCols, rgrp = tid / kUpdCols, nrg = nt / kUpdCols;
-  // row swaps (one thread per column does all of them, in order)
-  if (valid && rgrp == 0) {
+  // row swaps in order, then C1 = the pivot rows (values after the swaps)
+  cd c1[kW];
+  if (valid) {
     for (int jj = 0; jj < w; ++jj) {
-      int r0 = c0 + jj, r1 = piv[jj];
+      const int r0 = c0 + jj, r1 = piv[jj];
       if (r1 != r0) {
-        cd t0 = base[(size_t)r0 * ld], t1 = base[(size_t)r1 * ld];
+        const cd t0 = base[(size_t)r0 * ld], t1 = base[(size_t)r1 * ld];
         base[(size_t)r0 * ld] = t1;
         base[(size_t)r1 * ld] = t0;
       }
     }
-  }
-  __syncthreads();
-  // C1 = pivot rows (original values)
-  for (int k = rgrp; k < kW; k += nrg)
-    C1[k][lane_col] = (valid && k < w) ? base[(size_t)(c0 + k) * ld] : cd{0.0, 0.0};
-  __syncthreads();
-  // pivot rows <- W1 C1
-  for (int k = rgrp; k < w; k += nrg) {
-    if (!valid) continue;
-    cd s = cd{0.0, 0.0};
-    for (int m = 0; m < w; ++m) s = s + W1[k * kW + m] * C1[m][lane_col];
-    base[(size_t)(c0 + k) * ld] = s;
-  }
-  // other rows <- C2 - L2 C1; eight rows per thread at a time so that their
-  // loads are in flight together
-  if (!valid) return;
-  const cd* L2 = sc.L2 + (size_t)a * n * kW;
-  constexpr int U = 8;
-  for (int i0 = rgrp; i0 < n; i0 += U * nrg) {
-    cd s[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int i = i0 + u * nrg;
-      const bool row = i < n && !(i >= c0 && i < c0 + w);
-      s[u] = row ? base[(size_t)i * ld] : cd{0.0, 0.0};
+    for (int k = 0; k < kW; ++k) c1[k] = (k < w) ? base[(size_t)(c0 + k) * ld] : cd{0.0, 0.0};
+    // pivot rows <- W1 C1
+    for (int k = 0; k < w; ++k) {
+      cd v = cd{0.0, 0.0};
+#pragma unroll
+      for (int m = 0; m < kW; ++m)
+        if (m < w) v = v + W1[k * kW + m] * c1[m];  // entries past w are not written
+      base[(size_t)(c0 + k) * ld] = v;
     }
+  }
+  // other rows <- C2 - L2 C1
+  const cd* L2 = sc.L2 + (size_t)a * n * kW;
+  for (int i0 = 0; i0 < n; i0 += kUpdRows) {
+    __syncthreads();
+    for (int e = tid; e < kUpdRows * kW; e += kUpdCols) {
+      const int i = i0 + e / kW;
+      Ls[e / kW][e % kW] = (i < n) ? L2[(size_t)i * kW + e % kW] : cd{0.0, 0.0};
+    }
+    __syncthreads();
+    if (!valid) continue;
+    constexpr int U = 8;
+    for (int q = 0; q < kUpdRows; q += U) {
+      cd v[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int i = i0 + u * nrg;
-      if (i < n && !(i >= c0 && i < c0 + w)) {
-        const cd* l = L2 + (size_t)i * kW;
-        cd v = s[u];
-        for (int m = 0; m < w; ++m) v = v - l[m] * C1[m][lane_col];
-        base[(size_t)i * ld] = v;
+      for (int u = 0; u < U; ++u) {
+        const int i = i0 + q + u;
+        const bool row = i < n && !(i >= c0 && i < c0 + w);
+        v[u] = row ? base[(size_t)i * ld] : cd{0.0, 0.0};
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int i = i0 + q + u;
+        if (i < n && !(i >= c0 && i < c0 + w)) {
+          cd x = v[u];
+#pragma unroll
+          for (int m = 0; m < kW; ++m)
+            if (m < w) x = x - Ls[q + u][m] * c1[m];
+          base[(size_t)i * ld] = x;
+        }
       }
     }
   }
@@ -645,7 +657,7 @@ void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld,
     k_gj_panel<<<nang, 256, smem, st>>>(Q, flag, n, ld, c0, w, sc, status);
     int total = (n - (c0 + w)) + n;
     dim3 grid(ceil_div(total, kUpdCols), nang);
-    k_gj_update<<<grid, 256, 0, st>>>(Q, P, flag, n, ld, c0, w, sc);
+    k_gj_update<<<grid, kUpdCols, 0, st>>>(Q, P, flag, n, ld, c0, w, sc);
   }
 }
 

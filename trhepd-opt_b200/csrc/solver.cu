@@ -56,21 +56,28 @@ struct CudaError : std::runtime_error {
                       e_ == cudaErrorMemoryAllocation ? TRHEPD_ENOMEM : TRHEPD_ECUDA);     \
   } while (0)
 
+// Device memory is stream-ordered (cudaMallocAsync / cudaFreeAsync from the
+// device's default pool) on the stream of the call in progress: cudaFree would
+// synchronise the whole device, so a context growing or freeing a buffer would
+// wait for every kernel other contexts have queued (a small serving request
+// behind a large one).  Buffers are only used on the stream that allocated them.
+thread_local cudaStream_t t_alloc_stream = nullptr;
+
 struct DevBuf {
   void* p = nullptr;
   size_t n = 0;
   void* ensure(size_t bytes) {
     if (bytes <= n && p) return p;
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, t_alloc_stream);
     p = nullptr;
     n = 0;
     if (bytes == 0) bytes = 256;
-    CK(cudaMalloc(&p, bytes));
+    CK(cudaMallocAsync(&p, bytes, t_alloc_stream));
     n = bytes;
     return p;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, t_alloc_stream);
     p = nullptr;
     n = 0;
   }
@@ -1185,6 +1192,7 @@ int guarded(trhepd_context* ctx, F&& f) {
   if (!ctx) return TRHEPD_EINVAL;
   try {
     CK(cudaSetDevice(ctx->device));
+    t_alloc_stream = ctx->stream;
     f();
     ctx->err.clear();
     return TRHEPD_OK;
@@ -1279,6 +1287,13 @@ int trhepd_create(int device, trhepd_context** out) {
     delete c;
     return TRHEPD_ECUDA;
   }
+  // freed buffers stay in the device's default pool for the next allocation
+  // instead of going back to the driver at every synchronisation
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   *out = c;
   return TRHEPD_OK;
 }
@@ -1287,6 +1302,10 @@ void trhepd_destroy(trhepd_context* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  t_alloc_stream = c->stream;
+  for (DevBuf& b : c->bk) b.release();
+  for (DevBuf& b : c->rk) b.release();
+  for (DevBuf& b : c->mg) b.release();
   DevBuf* all[] = {&c->asf, &c->b, &c->dchg, &c->ghk, &c->depth, &c->table, &c->pair,
                    &c->Q0, &c->Q1, &c->P, &c->V, &c->D, &c->gam, &c->F, &c->flags, &c->dval,
                    &c->gj, &c->f2, &c->wnsga2, &c->status, &c->split, &c->sgh, &c->sgk,
@@ -1487,6 +1506,9 @@ int trhepd_problem_info(const trhepd_problem* pb, int64_t* out, int n) {
 
 void trhepd_problem_destroy(trhepd_problem* pb) {
   if (!pb) return;
+  // every solve and fetch synchronises its stream, so the buffers are idle: free
+  // them in the order of the legacy stream, which does not wait for other streams
+  t_alloc_stream = nullptr;
   pb->release();
   delete pb;
 }
