@@ -36,6 +36,11 @@ from pathlib import Path
 
 import numpy as np
 
+# more hardware work queues than the default 8, so that the serving slots' streams
+# (and torch's) do not share one and serialise behind each other's kernels; read
+# when CUDA initialises, so it is set before any CUDA call of this process
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = Path(__file__).resolve().parent
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
@@ -243,7 +248,8 @@ def serve_leg(device: int, seconds: float, load: float, precision: int, seed: in
     `load` times the throughput the isolated solve times allow; reports p50/p99
     latency, angle-solves/s and each request's latency over its isolated time."""
     from trhepd_opt_b200 import serving
-    srv = serving.Server(device=device, slots=4, mem_budget_gb=120.0, precision=precision)
+    srv = serving.Server(device=device, slots=serving.DEFAULT_SLOTS, mem_budget_gb=120.0,
+                         precision=precision)
     try:
         cases = [(n, g) for n in serving.DEFAULT_MIX for g in serving.GRIDS]
         iso = serving.isolated_times(srv, cases)
@@ -259,7 +265,10 @@ def serve_leg(device: int, seconds: float, load: float, precision: int, seed: in
                 "mean_isolated_request_s": busy,
                 "isolated_s": {f"{n}x{g}": t for (n, g), t in iso.items()},
                 "mix": {str(k): v for k, v in serving.DEFAULT_MIX.items()},
-                "grids": list(serving.GRIDS), "slots": 4, "hbm_budget_gb": 120.0,
+                "grids": list(serving.GRIDS),
+                "slots": [{"n_min": lo, "n_max": hi, "stream_priority": p}
+                          for lo, hi, p in serving.DEFAULT_SLOTS],
+                "hbm_budget_gb": 120.0,
                 "structures": "dense(N) base per (N, grid), 15 A region in 0.02 A slices, "
                               "surface atoms jittered by sigma in [0.05, 0.2] A per request"})
     return out

@@ -30,24 +30,24 @@ def test_summary_percentiles():
     assert s["angle_solves_per_s"] == 3100.0
 
 
-def test_pending_order_and_large_cap():
-    """Smallest beam count first (oldest first within it); large requests only
-    while fewer than the cap are running, so a slot stays free for small ones."""
+def test_pending_ranges_and_order():
+    """A worker takes the smallest pending request of its beam-count range (oldest
+    first among equals) and never one outside it; closing releases idle workers
+    once their range is empty."""
     from trhepd_opt_b200 import serving
-    q = serving._Pending(large_n=191, large_cap=1)
+    q = serving._Pending()
     reqs = [serving.Request(rid=i, n=n, n_angles=31, sigma=0.1, seed=i)
             for i, n in enumerate([521, 95, 23, 191, 23])]
     for r in reqs:
         q.put(r)
-    first = q.get()
+    first = q.get(0, 95)
     assert (first.n, first.rid) == (23, 2)
-    assert q.get().rid == 4
-    assert q.get().n == 95
-    big = q.get()
-    assert big.n == 191            # the smaller large request
-    q.put(serving.Request(rid=9, n=47, n_angles=31, sigma=0.1, seed=9))
-    assert q.get().rid == 9        # 521 is held back while a large one runs
-    q.task_done(big)
-    assert q.get().n == 521
+    assert q.get(0, 95).rid == 4
+    assert q.get(0, 95).n == 95
+    assert q.get(96, 191).n == 191
+    assert q.get(192, 1 << 30).n == 521
     q.put(None)
-    assert q.get() is None
+    assert q.get(0, 95) is None
+    for r in reqs:
+        q.task_done(r)
+    q.join()

@@ -438,9 +438,6 @@ static_assert(128 * P_REG_CTRL + 256 * P_REG_EPI <= P_THREADS * P_REG_LAUNCH,
 __host__ __device__ constexpr int pstages_for(int S) { return stages_for(S); }
 inline size_t psmem_bytes(int S) { return smem_bytes(S); }
 
-__device__ __forceinline__ void prefetch_l1(const void* p) {
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -1053,28 +1050,11 @@ __global__ void __launch_bounds__(P_THREADS, 1)
           const int r = m0 + 16 * h + 8 * u + t1;
           qd[h][u] = (r < ep.rows) ? ep.Q[(size_t)r * ep.ld + ri[h][u]] : cd{0.0, 0.0};
         }
-      // Q and P of the (g, h) step two steps ahead are prefetched into L1, so the
-      // loads of each step mostly hit L1 instead of waiting on HBM
-      auto prefetch_step = [&](int idx) {
-        const int g = idx >> 1, h = idx & 1, j = jh + 4 * g + t0;
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int r = m0 + 16 * h + 8 * u + t1;
-          if (r < ep.rows && j < ep.n) {
-            const size_t o = (size_t)r * ep.ld + j;
-            prefetch_l1(ep.Q + o);
-            prefetch_l1(ep.P + o);
-          }
-        }
-      };
-      prefetch_step(0);
-      prefetch_step(1);
 #pragma unroll
       for (int g = 0; g < 8; ++g) {
         const int j = jh + 4 * g + t0;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          if (2 * g + h + 2 < 16) prefetch_step(2 * g + h + 2);
           cd qv[2], pv[2], vv[2], dv[2];
 #pragma unroll
           for (int u = 0; u < 2; ++u) {

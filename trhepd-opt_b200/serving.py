@@ -10,13 +10,16 @@ data; trhepd_problem_*), is solved, and its intensities are returned.  The
 bulk boundary of a (base structure, angle grid) is written once and reused by
 every candidate of that base.
 
-Scheduling keeps small requests from queueing behind large ones: a free slot
-takes the oldest pending request of the smallest beam count first, at most
-`slots - 1` slots run large requests (N >= `large_n`) at once, and each solve
-runs on a stream whose priority falls with N, so the block scheduler starts the
-kernels of small requests first.  Requests with N <= 64 run the fused FP64
-kernel whatever the server's precision (one launch per solve, exact FP64);
-larger ones use the server's precision form.
+Scheduling keeps small requests from queueing behind large ones.  Each slot
+serves one range of beam counts and owns one stream of a fixed priority (the
+default layout: two slots for N <= 95 at the highest priority, one for
+96..191, one for N >= 192 at the lowest); a free slot takes the smallest
+pending request of its range.  Streams are created once per slot: a stream
+made per request would be mapped round-robin onto the GPU's few hardware work
+queues and could land on the queue of a running large solve, behind all of its
+queued kernels.  Requests with N <= 64 run the fused FP64 kernel whatever the
+server's precision (one launch per solve, exact FP64); larger ones use the
+server's precision form.
 
 Latency is completion minus arrival; the report gives p50/p99 and angle-solves/s.
 """
@@ -79,60 +82,45 @@ def poisson_stream(rate: float, duration: float, seed: int = 0, mix=None,
 
 
 FUSED_MAX_N = 64
-# stream priority (0 lowest .. 1 highest) by beam count
-PRIORITY = ((64, 1.0), (95, 0.75), (191, 0.5))
-
-
-def priority_for(n: int) -> float:
-    for limit, p in PRIORITY:
-        if n <= limit:
-            return p
-    return 0.0
+# slot layout: (smallest N, largest N, stream priority 0 lowest .. 1 highest)
+DEFAULT_SLOTS = ((0, 95, 1.0), (0, 95, 1.0), (96, 191, 0.5), (192, 1 << 30, 0.0))
 
 
 class _Pending:
-    """Pending requests; workers take the smallest beam count first (oldest first
-    within it), large requests only while fewer than `large_cap` are running."""
+    """Pending requests; a worker serving beam counts lo..hi takes the smallest
+    pending request in that range (oldest first among equals)."""
 
-    def __init__(self, large_n: int, large_cap: int):
+    def __init__(self):
         self.items: list = []
         self.cv = threading.Condition()
         self.unfinished = 0
-        self.large_n, self.large_cap, self.large_running = large_n, large_cap, 0
+        self.closing = False
 
     def put(self, r) -> None:
         with self.cv:
-            self.items.append(r)
-            if r is not None:
+            if r is None:
+                self.closing = True
+            else:
+                self.items.append(r)
                 self.unfinished += 1
             self.cv.notify_all()
 
-    def get(self):
+    def get(self, lo: int = 0, hi: int = 1 << 30):
         with self.cv:
             while True:
-                if any(r is None for r in self.items) and all(
-                        r is None for r in self.items):
-                    self.items.remove(None)
-                    return None
                 pick = None
                 for r in self.items:
-                    if r is None:
-                        continue
-                    if r.n >= self.large_n and self.large_running >= self.large_cap:
-                        continue
-                    if pick is None or r.n < pick.n:
+                    if lo <= r.n <= hi and (pick is None or r.n < pick.n):
                         pick = r
                 if pick is not None:
                     self.items.remove(pick)
-                    if pick.n >= self.large_n:
-                        self.large_running += 1
                     return pick
+                if self.closing:
+                    return None
                 self.cv.wait(timeout=0.5)
 
     def task_done(self, r) -> None:
         with self.cv:
-            if r.n >= self.large_n:
-                self.large_running -= 1
             self.unfinished -= 1
             self.cv.notify_all()
 
@@ -143,24 +131,31 @@ class _Pending:
 
 
 class Server:
-    def __init__(self, device: int = 0, slots: int = 4, mem_budget_gb: float = 120.0,
+    def __init__(self, device: int = 0, slots=DEFAULT_SLOTS, mem_budget_gb: float = 120.0,
                  precision: int = native.FP64, region: float = 15.0, dz: float = 0.02,
-                 renorm_policy: int = 1, large_n: int = 191):
-        self.device, self.slots, self.precision = device, slots, precision
+                 renorm_policy: int = 1):
+        """`slots`: a sequence of (smallest N, largest N, stream priority) per slot,
+        or an int k for k slots that take any request at the default priority."""
+        if isinstance(slots, int):
+            slots = tuple((0, 1 << 30, 0.0) for _ in range(slots))
+        self.layout = tuple(slots)
+        self.slots = len(self.layout)
+        self.device, self.precision = device, precision
         self.region, self.dz = region, dz
         self.budget = mem_budget_gb * 1e9
         self.in_use = 0.0
         self.cv = threading.Condition()
-        self.q = _Pending(large_n, max(1, slots - 1))
+        self.q = _Pending()
         self.tmp = Path(tempfile.mkdtemp(prefix="trhepd_serve_"))
         self.bulk_cache: dict = {}
         self.bulk_lock = threading.Lock()
         self.t0 = time.perf_counter()
-        self.ctxs = [native.Context(device) for _ in range(slots)]
-        for c in self.ctxs:
+        self.ctxs = [native.Context(device) for _ in self.layout]
+        for c, (_, _, prio) in zip(self.ctxs, self.layout):
             c.set_option(native.OPT_RENORM_POLICY, renorm_policy)
-        self.workers = [threading.Thread(target=self._work, args=(c,), daemon=True)
-                        for c in self.ctxs]
+            c.set_option(native.OPT_STREAM_PRIORITY, prio)
+        self.workers = [threading.Thread(target=self._work, args=(c, lo, hi), daemon=True)
+                        for c, (lo, hi, _) in zip(self.ctxs, self.layout)]
         self.done: list[Request] = []
         for w in self.workers:
             w.start()
@@ -211,9 +206,9 @@ class Server:
         """The form a request of n beams runs in: fused FP64 up to 64 beams."""
         return native.FP64 if n <= FUSED_MAX_N else self.precision
 
-    def _work(self, ctx: native.Context) -> None:
+    def _work(self, ctx: native.Context, lo: int, hi: int) -> None:
         while True:
-            r = self.q.get()
+            r = self.q.get(lo, hi)
             if r is None:
                 return
             need = 0.0
@@ -224,7 +219,6 @@ class Server:
                                          6 * sp.args.ns + 1)
                 self._admit(need)
                 r.start = time.perf_counter() - self.t0
-                ctx.set_option(native.OPT_STREAM_PRIORITY, priority_for(r.n))
                 rp = sp.resident()
                 rp.solve(self.precision_for(r.n))
                 r.device_ms = ctx.last_stats()["device_ms"]
@@ -242,8 +236,7 @@ class Server:
                 self.q.task_done(r)
 
     def close(self) -> None:
-        for _ in self.workers:
-            self.q.put(None)
+        self.q.put(None)
         for w in self.workers:
             w.join(timeout=600)
         for c in self.ctxs:
