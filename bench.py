@@ -274,6 +274,43 @@ def serve_leg(device: int, seconds: float, load: float, precision: int, seed: in
     return out
 
 
+def uneven_leg(ctx, precision: int, per_n: int = 8, seed: int = 0) -> dict:
+    """Candidate-structure batch of uneven beam counts: per_n jittered candidates
+    (sigma 0.1 A) of a base structure for each N in {23, 47, 95, 191}, 61 angles,
+    15 A in 0.02 A slices, all solved by one trhepd_batch_solve (the N <= 64 ones
+    in shared fused launches); the first batch solve warms up, the next two are
+    timed (device time from the library's events)."""
+    tmp = Path(tempfile.mkdtemp(prefix="trhepd_uneven_"))
+    probs, nang = [], 0
+    for n in (23, 47, 95, 191):
+        base = generator.dense(n, seed=20 + n + seed, n_angles=61, region=15.0, dz=0.02)
+        for k in range(per_n):
+            s = generator.jitter(base, 0.1, 1000 * n + k)
+            d = tmp / f"n{n}_{k}"
+            s.write(d)
+            bulkfile.write_bulkp(s, d / "bulkP.b")
+            sp = surface.SurfaceProblem(ctx, d / "bulkP.b", d / "surf.txt", s.surface_dz,
+                                        s.int_method)
+            probs.append((sp, sp.resident()))
+            nang += probs[-1][1].nangles
+    rps = [rp for _, rp in probs]
+    surface.solve_batch(ctx, rps, precision)
+    ms = []
+    for _ in range(2):
+        surface.solve_batch(ctx, rps, precision)
+        ms.append(ctx.last_stats()["device_ms"])
+    st = ctx.last_stats()
+    for sp, rp in probs:
+        rp.close()
+        sp.close()
+    t = sum(ms) / len(ms) / 1e3
+    return {"structures": len(probs), "beam_counts": [23, 47, 95, 191], "per_n": per_n,
+            "angles_per_structure": 61, "slices": "15 A in 0.02 A", "angle_solves": nang,
+            "seconds_per_batch": t, "angle_solves_per_s": nang / t,
+            "launches_per_batch": st["launches"],
+            "note": "N <= 64 in fused FP64 launches, N = 95, 191 in the requested form"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -288,6 +325,7 @@ def main():
     ap.add_argument("--no-bf16", action="store_true", help="skip the BF16 split comparison")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven candidate batch")
     ap.add_argument("--serve-seconds", type=float, default=40.0)
     ap.add_argument("--serve-load", type=float, default=0.5,
                     help="arrival rate as a fraction of the isolated-solve throughput")
@@ -480,6 +518,9 @@ def main():
 
     rp.close()
     sp.close()
+    uneven = None
+    if rank == 0 and ws == 1 and not args.no_uneven:
+        uneven = uneven_leg(ctx, prec)
     ctx.close()
 
     serve = None
@@ -507,7 +548,8 @@ def main():
                            "bulk_boundary": "non-reflecting bulk records (f = 0)",
                            "l2": "inputs larger than L2 (state + stage table > 1 GB)",
                            "parallelism": f"replicas x{ws}"},
-                "roofline": roof, "fp64": fp64, "bf16_split": bf16, "e2e": e2e,
+                "roofline": roof, "fp64": fp64, "bf16_split": bf16, "uneven_batch": uneven,
+                "e2e": e2e,
                 "cpu_baseline": cpu,
                 "gpu_launches": launches, "clocks": clk, "wall_seconds_timed": t_wall,
                 "serving": serve}

@@ -196,6 +196,16 @@ typedef struct trhepd_problem trhepd_problem;
 int trhepd_problem_create(trhepd_context* ctx, const trhepd_pot_state* pot,
                           const trhepd_srfref_args* args, trhepd_problem** out);
 int trhepd_problem_solve(trhepd_context* ctx, trhepd_problem* pb, int precision);
+/* Solve several resident problems together (no counterpart in the reference,
+   whose driver solves one structure at a time; this is the candidate-structure
+   batch of a refinement step).  Problems with int_method 5 or 6 and
+   2 <= nb <= TRHEPD_OPT_FUSED_MAX_N are integrated by shared launches in their own
+   buffers: one launch per integrator for up to 192 problems, any mix of beam
+   counts, slice counts and angle grids, in plain FP64.  The other problems are
+   solved one after another in `precision`.  Each problem's intensities are then
+   read with trhepd_problem_fetch; trhepd_last_stats reports the whole batch. */
+int trhepd_batch_solve(trhepd_context* ctx, trhepd_problem* const* problems, int count,
+                       int precision);
 int trhepd_problem_fetch(trhepd_context* ctx, trhepd_problem* pb, double* f2, double* angle_deg);
 int trhepd_problem_info(const trhepd_problem* pb, int64_t* out, int n);
 void trhepd_problem_destroy(trhepd_problem* pb);

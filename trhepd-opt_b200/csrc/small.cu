@@ -16,8 +16,12 @@
 //     always on the last) is an in-place Gauss-Jordan of [Q | P] with partial
 //     pivoting on max |re| + |im| (matAbdivB, matcomp.f90:53-69), then Q = I.
 // The stage order, merged half kicks and coefficients are those of run_rkn.
+// One launch can carry several problems (their own tables, beam counts up to
+// the launch's NP, slice counts and renormalisation intervals): each CTA finds
+// its problem in the launch parameters.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <stdexcept>
 
 #include "small.h"
@@ -47,8 +51,14 @@ __device__ __forceinline__ void fdmma(double& c0, double& c1, double& c2, double
 }
 
 template <int NP>
-__global__ void __launch_bounds__(Cfg<NP>::THREADS) k_fused_rkn(const FusedRkn a) {
+__global__ void __launch_bounds__(Cfg<NP>::THREADS)
+    k_fused_rkn(const __grid_constant__ FusedLaunch L) {
   using C = Cfg<NP>;
+  // this CTA's problem: the last whose first CTA is <= blockIdx.x
+  int pi = 0;
+  for (int q = 1; q < L.nprob; ++q)
+    if (L.p[q].first_cta <= (int)blockIdx.x) pi = q;
+  const FusedProblem& a = L.p[pi];
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd* Qs = reinterpret_cast<cd*>(smem_raw);
   cd* Ps = Qs + NP * C::QSTR;
@@ -57,7 +67,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS) k_fused_rkn(const FusedRkn a
   __shared__ int piv_sh, renorm_sh;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int n = a.n, ld = a.ld, ang = blockIdx.x;
+  const int n = a.n, ld = a.ld, ang = blockIdx.x - a.first_cta;
   cd* Qg = a.Q + (size_t)ang * n * ld;
   cd* Pg = a.P + (size_t)ang * n * ld;
   const cd* Dg = a.D + (size_t)ang * ld;
@@ -289,22 +299,22 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS) k_fused_rkn(const FusedRkn a
     }
   };
 
-  const int s = a.s, ns = a.ns;
+  const int s = L.s, ns = a.ns;
   const double dz = a.dz;
   load_col(0);
   store_col();
   __syncthreads();
   load_col(1);
-  identity_stage(a.bab[0] * dz, a.bab[1] * dz);
+  identity_stage(L.bab[0] * dz, L.bab[1] * dz);
   __syncthreads();
   store_col();
   __syncthreads();
   for (int l = 1; l <= ns; ++l) {
     for (int k = (l == 1) ? 2 : 1; k <= s; ++k) {
       const int col = s * (l - 1) + k - 1;
-      const double ca = a.bab[2 * k - 1] * dz;
+      const double ca = L.bab[2 * k - 1] * dz;
       // k == 1 merges the end-of-slice half kick of slice l-1 with the first kick
-      const double cb = (k == 1) ? 2.0 * a.bab[0] * dz : a.bab[2 * k - 2] * dz;
+      const double cb = (k == 1) ? 2.0 * L.bab[0] * dz : L.bab[2 * k - 2] * dz;
       load_col(col + 1);  // the next stage's matrix (the last column after slice ns)
       product_stage(cb, ca);
       store_col();        // V is no longer read: the next stage's matrix goes in
@@ -312,14 +322,14 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS) k_fused_rkn(const FusedRkn a
     }
     const bool last = l == ns;
     bool renorm = last;
-    if (!last) renorm = (a.policy == 0) ? needs_renorm() : (l % a.interval) == 0;
+    if (!last) renorm = (L.policy == 0) ? needs_renorm() : (l % a.interval) == 0;
     if (renorm) {
       gauss_jordan();
       __syncthreads();
     }
   }
   // final half kick with Q = I: P += b1 dz M(end)
-  identity_stage(a.bab[0] * dz, 0.0);
+  identity_stage(L.bab[0] * dz, 0.0);
   __syncthreads();
   for (int e = tid; e < n * n; e += C::THREADS) {
     const int i = e / n, j = e % n;
@@ -329,7 +339,7 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS) k_fused_rkn(const FusedRkn a
 }
 
 template <int NP>
-void launch(const FusedRkn& a, cudaStream_t st) {
+void launch(const FusedLaunch& L, cudaStream_t st) {
   using C = Cfg<NP>;
   static bool attr = false;
   if (!attr) {
@@ -337,22 +347,32 @@ void launch(const FusedRkn& a, cudaStream_t st) {
                          (int)C::SMEM);
     attr = true;
   }
-  k_fused_rkn<NP><<<a.nang, C::THREADS, C::SMEM, st>>>(a);
+  k_fused_rkn<NP><<<L.total_ctas, C::THREADS, C::SMEM, st>>>(L);
 }
 
 }  // namespace fused
 
-int launch_fused_rkn(const FusedRkn& a, cudaStream_t st) {
-  if (a.n < 2 || a.n > kFusedMaxBeams || a.s < 1 || a.s > 11 || a.ns < 1 || a.interval < 1)
-    throw std::invalid_argument("fused integration: unsupported sizes");
-  if (a.n <= 16)
-    fused::launch<16>(a, st);
-  else if (a.n <= 32)
-    fused::launch<32>(a, st);
-  else if (a.n <= 48)
-    fused::launch<48>(a, st);
+int launch_fused_rkn(const FusedLaunch& L, cudaStream_t st) {
+  if (L.nprob < 1 || L.nprob > kFusedMaxProblems || L.s < 1 || L.s > 11)
+    throw std::invalid_argument("fused integration: bad launch");
+  int nmax = 0, ctas = 0;
+  for (int q = 0; q < L.nprob; ++q) {
+    const FusedProblem& a = L.p[q];
+    if (a.n < 2 || a.n > kFusedMaxBeams || a.ns < 1 || a.interval < 1 || a.nang < 1 ||
+        a.first_cta != ctas)
+      throw std::invalid_argument("fused integration: unsupported problem");
+    ctas += a.nang;
+    nmax = std::max(nmax, a.n);
+  }
+  if (ctas != L.total_ctas) throw std::invalid_argument("fused integration: CTA count");
+  if (nmax <= 16)
+    fused::launch<16>(L, st);
+  else if (nmax <= 32)
+    fused::launch<32>(L, st);
+  else if (nmax <= 48)
+    fused::launch<48>(L, st);
   else
-    fused::launch<64>(a, st);
+    fused::launch<64>(L, st);
   return 1;
 }
 

@@ -297,6 +297,19 @@ struct RunState {
   bool capturing = false;    // launches go into a CUDA graph: no events on the stream
 };
 
+// The device buffers one integration works in: the context's (one solve at a
+// time) or a problem's own (problems solved together in a batch).
+struct Workspace {
+  DevBuf *Q0, *Q1, *P, *V, *flags, *dval, *gj, *status, *split;
+};
+struct OwnWorkspace {
+  DevBuf Q0, Q1, P, V, flags, dval, gj, status, split;
+  Workspace view() { return {&Q0, &Q1, &P, &V, &flags, &dval, &gj, &status, &split}; }
+  void release() {
+    for (DevBuf* b : {&Q0, &Q1, &P, &V, &flags, &dval, &gj, &status, &split}) b->release();
+  }
+};
+
 }  // namespace
 
 // Device-resident problem: stage table, beam-pair map, bulk boundary, gammas.
@@ -312,6 +325,7 @@ struct trhepd_problem {
   // CUDA graph of the whole solve, valid for `graph_key` and the context buffers
   // in `graph_sig`; `last_sig` holds the buffers of the last uncaptured solve.
   cudaGraphExec_t graph = nullptr;
+  OwnWorkspace own;            // buffers of batch solves (trhepd_batch_solve)
   std::vector<double> graph_key;
   std::vector<void*> graph_sig, last_sig;
   RunState graph_run;
@@ -325,6 +339,7 @@ struct trhepd_problem {
   }
   void release() {
     drop_graph();
+    own.release();
     for (DevBuf* b : {&table, &pair, &gam, &D, &F, &wnsga2, &f2}) b->release();
   }
 };
@@ -438,7 +453,12 @@ void prepare(trhepd_context* C, const SolveArgs& A, trhepd_problem& Pb) {
 
 // Buffers, the boundary transform invstransh (matcomp.f90:140-172) and the
 // renormalisation schedule; Q = I and P = P0 afterwards.
-void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_max, RunState& R) {
+Workspace context_workspace(trhepd_context* C) {
+  return {&C->Q0, &C->Q1, &C->P, &C->V, &C->flags, &C->dval, &C->gj, &C->status, &C->split};
+}
+
+void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_max, RunState& R,
+               const Workspace& W) {
   R.n = Pb.n;
   R.ns = Pb.ns;
   R.nv = Pb.nv;
@@ -453,20 +473,20 @@ void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_m
   const int n = R.n, nang = R.nang, ld = R.ld;
   cudaStream_t st = R.st;
   R.sbytes = (size_t)nang * n * ld * sizeof(cd);
-  R.Q = (cd*)C->Q0.ensure(R.sbytes);
-  R.Qn = (cd*)C->Q1.ensure(R.sbytes);
-  R.P = (cd*)C->P.ensure(R.sbytes);
-  R.V = (cd*)C->V.ensure((size_t)(R.kpad + 1) * ld * sizeof(cd));
-  R.flags = (int*)C->flags.ensure(std::max(nang, 4) * sizeof(int));
-  R.dval = (double*)C->dval.ensure(std::max(nang, 4) * sizeof(double));
-  R.gjs = C->gj.ensure(gj_scratch_bytes(nang, n));
-  R.status = (unsigned*)C->status.ensure(16);
+  R.Q = (cd*)W.Q0->ensure(R.sbytes);
+  R.Qn = (cd*)W.Q1->ensure(R.sbytes);
+  R.P = (cd*)W.P->ensure(R.sbytes);
+  R.V = (cd*)W.V->ensure((size_t)(R.kpad + 1) * ld * sizeof(cd));
+  R.flags = (int*)W.flags->ensure(std::max(nang, 4) * sizeof(int));
+  R.dval = (double*)W.dval->ensure(std::max(nang, 4) * sizeof(double));
+  R.gjs = W.gj->ensure(gj_scratch_bytes(nang, n));
+  R.status = (unsigned*)W.status->ensure(16);
   R.split = precision == TRHEPD_SPLIT_BF16 || precision == TRHEPD_SPLIT_INT8;
   R.split_variant = (precision == TRHEPD_SPLIT_INT8) ? kSplitInt8 : C->split_variant;
   if (precision == TRHEPD_SPLIT_INT8 && C->split_slices > 4)
     throw std::invalid_argument("the INT8 split form takes 3 or 4 slices");
   if (R.split)
-    R.sw = split_workspace_carve(C->split.ensure(split_workspace_bytes(nang, n, C->split_slices)),
+    R.sw = split_workspace_carve(W.split->ensure(split_workspace_bytes(nang, n, C->split_slices)),
                                  nang, n, C->split_slices, R.status, st);
   R.gj_per = 2 * ceil_div(n, 16);
   if (C->profile && (int)C->evpool.size() < 4 * nprod_max) {
@@ -584,32 +604,42 @@ void finish_host(trhepd_context* C, trhepd_problem& Pb, RunState& R) {
     throw CudaError("non-finite value or zero pivot in the surface solve", TRHEPD_ENONFINITE);
 }
 
+// The fused-kernel descriptor of a run whose begin_run has been issued.
+FusedProblem fused_problem(const RunState& R, double dz, int first_cta) {
+  FusedProblem f{};
+  f.Q = R.Q;
+  f.P = R.P;
+  f.table = R.table;
+  f.pair = R.pair;
+  f.D = R.D;
+  f.status = R.status;
+  f.n = R.n;
+  f.ld = R.ld;
+  f.nv = R.nv;
+  f.nang = R.nang;
+  f.ns = R.ns;
+  f.interval = R.interval;
+  f.first_cta = first_cta;
+  f.dz = dz;
+  return f;
+}
+
 // Symplectic RKN (hp_int_spa, surf_prkn.f90:278-330) batched over angles.
 void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
   const Integrator& I = Pb.I;
   const double dz = Pb.dz;
-  begin_run(C, Pb, precision, I.s * Pb.ns, R);
+  begin_run(C, Pb, precision, I.s * Pb.ns, R, context_workspace(C));
   const bool every_slice = (Pb.n == 1 && Pb.int_method == 6);  // hp_int_spa1d renormalises each slice
   if (!R.split && Pb.n >= 2 && Pb.n <= std::min(C->fused_max_n, kFusedMaxBeams)) {
     // whole integration in one launch, state in shared memory (small.cu)
-    FusedRkn f{};
-    f.Q = R.Q;
-    f.P = R.P;
-    f.table = R.table;
-    f.pair = R.pair;
-    f.D = R.D;
-    f.status = R.status;
-    f.n = R.n;
-    f.ld = R.ld;
-    f.nv = R.nv;
-    f.nang = R.nang;
-    f.ns = R.ns;
-    f.s = I.s;
-    f.policy = C->renorm_policy;
-    f.interval = R.interval;
-    f.dz = dz;
-    for (int q = 0; q < 2 * I.s + 1; ++q) f.bab[q] = I.bab[q];
-    R.launches += launch_fused_rkn(f, R.st);
+    static thread_local FusedLaunch L;  // 17 KB of kernel parameters
+    L.nprob = 1;
+    L.s = I.s;
+    L.policy = C->renorm_policy;
+    L.total_ctas = R.nang;
+    for (int q = 0; q < 2 * I.s + 1; ++q) L.bab[q] = I.bab[q];
+    L.p[0] = fused_problem(R, dz, 0);
+    R.launches += launch_fused_rkn(L, R.st);
     R.products += (long)I.s * R.ns - 1;
     R.renorms += (C->renorm_policy == 1) ? (R.ns - 1) / R.interval : R.ns - 1;
     finish_device(C, Pb, R);
@@ -649,7 +679,7 @@ void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) 
 // which gives the reference's Q = I shortcut exactly.
 void run_lf(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
   const double dz = Pb.dz;
-  begin_run(C, Pb, precision, Pb.ns, R);
+  begin_run(C, Pb, precision, Pb.ns, R, context_workspace(C));
   gather(R, 0, false);  // any finite stage matrix: cb = 0 below
   launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, 0.0, 0.5 * dz, R.st);
   R.launches += 1;
@@ -668,7 +698,7 @@ void run_lf(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
 // kernel into a zeroed buffer (cb = 1, ca = 0).
 void run_rk4(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
   const double dz = Pb.dz;
-  begin_run(C, Pb, precision, 4 * Pb.ns, R);
+  begin_run(C, Pb, precision, 4 * Pb.ns, R, context_workspace(C));
   const size_t sb = R.sbytes;
   cd* Qt = (cd*)C->rk[0].ensure(sb);
   cd* Pt = (cd*)C->rk[1].ensure(sb);
@@ -715,7 +745,7 @@ void run_magnus(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& 
     throw std::invalid_argument("the Magnus integrators (int_method 1-3) run in plain FP64 only");
   const double dz = Pb.dz;
   const Family fam = Pb.I.family;
-  begin_run(C, Pb, precision, 0, R);
+  begin_run(C, Pb, precision, 0, R, context_workspace(C));
   const int n = R.n, nang = R.nang, ld = R.ld;
   cudaStream_t st = R.st;
   const size_t sb = R.sbytes, vb = (size_t)(R.kpad + 1) * ld * sizeof(cd);
@@ -874,6 +904,94 @@ void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
   CK(cudaGraphLaunch(Pb.graph, C->stream));
   CK(cudaEventRecord(C->ev1, C->stream));
   finish_host(C, Pb, R);
+}
+
+// Problems solved together (no counterpart in the reference, whose driver solves
+// one structure at a time).  Problems the fused kernel takes (RKN, 2 <= n <= the
+// fused limit) are integrated by shared launches, each in its own buffers: one
+// launch per integrator and kFusedMaxProblems problems, whatever their beam
+// counts, slice counts and angle grids; the boundary kernels of each problem run
+// around it.  Other problems are solved one after another (graph replays from
+// their second solve on).  The split forms apply to those; fused problems are FP64.
+void batch_solve(trhepd_context* C, trhepd_problem* const* probs, int count, int precision) {
+  cudaStream_t st = C->stream;
+  const int fmax = std::min(C->fused_max_n, kFusedMaxBeams);
+  std::vector<trhepd_problem*> fused[2], rest;  // by integrator: RKN-4 (s = 6), RKN-6 (s = 11)
+  for (int q = 0; q < count; ++q) {
+    trhepd_problem* p = probs[q];
+    if (!p) throw std::invalid_argument("null problem in batch");
+    if (p->I.family == kRkn && p->n >= 2 && p->n <= fmax)
+      fused[p->I.s == 6 ? 0 : 1].push_back(p);
+    else
+      rest.push_back(p);
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  long launches = 0, products = 0, renorms = 0;
+  std::vector<unsigned*> statuses;
+  try {
+    CK(cudaEventRecord(e0, st));
+    static thread_local FusedLaunch L;
+    for (auto& group : fused)
+      for (size_t g0 = 0; g0 < group.size(); g0 += kFusedMaxProblems) {
+        const size_t g1 = std::min(group.size(), g0 + (size_t)kFusedMaxProblems);
+        std::vector<RunState> runs(g1 - g0);
+        const Integrator& I = group[g0]->I;
+        L.nprob = (int)(g1 - g0);
+        L.s = I.s;
+        L.policy = C->renorm_policy;
+        for (int q = 0; q < 2 * I.s + 1; ++q) L.bab[q] = I.bab[q];
+        int ctas = 0;
+        for (size_t q = g0; q < g1; ++q) {
+          RunState& R = runs[q - g0];
+          R.capturing = true;  // timing events belong to the batch
+          begin_run(C, *group[q], TRHEPD_FP64, 0, R, group[q]->own.view());
+          L.p[q - g0] = fused_problem(R, group[q]->dz, ctas);
+          ctas += R.nang;
+          products += (long)I.s * R.ns - 1;
+          renorms += (C->renorm_policy == 1) ? (R.ns - 1) / R.interval : R.ns - 1;
+        }
+        L.total_ctas = ctas;
+        launches += launch_fused_rkn(L, st);
+        for (size_t q = g0; q < g1; ++q) {
+          RunState& R = runs[q - g0];
+          finish_device(C, *group[q], R);
+          launches += R.launches;
+          statuses.push_back(R.status);
+        }
+      }
+    std::vector<unsigned> hs(4 * statuses.size() + 4, 0);
+    for (size_t q = 0; q < statuses.size(); ++q)
+      CK(cudaMemcpyAsync(&hs[4 * q], statuses[q], 16, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (size_t q = 0; q < statuses.size(); ++q) {
+      if (hs[4 * q] & kStatusTimeout) throw CudaError("device wait timed out", TRHEPD_ETIMEOUT);
+      if (hs[4 * q] & (kStatusNonFinite | kStatusZeroPivot))
+        throw CudaError("non-finite value or zero pivot in a batch solve", TRHEPD_ENONFINITE);
+    }
+    for (trhepd_problem* p : rest) {
+      run(C, *p, precision);
+      products += (long)C->stats[1];
+      renorms += (long)C->stats[0];
+      launches += (long)C->stats[5];
+    }
+    CK(cudaEventRecord(e1, st));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    for (double& v : C->stats) v = 0.0;
+    C->stats[0] = (double)renorms;
+    C->stats[1] = (double)products;
+    C->stats[2] = ms;
+    C->stats[5] = (double)launches;
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
 }
 
 void fetch(trhepd_context* C, trhepd_problem& Pb, double* f2, double* angle_deg) {
@@ -1487,6 +1605,15 @@ int trhepd_problem_solve(trhepd_context* ctx, trhepd_problem* pb, int precision)
     if (!valid_precision(precision))
       throw std::invalid_argument("unknown precision form");
     run(ctx, *pb, precision);
+  });
+}
+
+int trhepd_batch_solve(trhepd_context* ctx, trhepd_problem* const* problems, int count,
+                       int precision) {
+  return guarded(ctx, [&] {
+    if (!problems || count < 1) throw std::invalid_argument("empty batch");
+    if (!valid_precision(precision)) throw std::invalid_argument("unknown precision form");
+    batch_solve(ctx, problems, count, precision);
   });
 }
 

@@ -32,7 +32,7 @@ EXPORTS = [
     "trhepd_create", "trhepd_destroy", "trhepd_last_error", "trhepd_set_option",
     "trhepd_last_stats", "trhepd_structure_factors", "trhepd_plane_group_images",
     "trhepd_potential_table", "trhepd_srfref", "trhepd_surf_run", "trhepd_surf_load",
-    "trhepd_surf_free", "trhepd_surf_views", "trhepd_problem_create", "trhepd_problem_solve",
+    "trhepd_surf_free", "trhepd_surf_views", "trhepd_problem_create", "trhepd_problem_solve", "trhepd_batch_solve",
     "trhepd_problem_fetch", "trhepd_problem_info", "trhepd_problem_destroy",
     "trhepd_potential_table_noalloc", "trhepd_bulk_run",
 ]
@@ -111,6 +111,7 @@ def load():
     L.trhepd_problem_create.argtypes = [_P, ctypes.POINTER(PotState), ctypes.POINTER(SrfrefArgs),
                                         ctypes.POINTER(_P)]
     L.trhepd_problem_solve.argtypes = [_P, _P, _I]
+    L.trhepd_batch_solve.argtypes = [_P, _P, _I, _I]
     L.trhepd_problem_fetch.argtypes = [_P, _P, _P, _P]
     L.trhepd_problem_info.argtypes = [_P, _P, _I]
     L.trhepd_potential_table_noalloc.argtypes = [_P, _I, _I, _D, _P, _P, _P]

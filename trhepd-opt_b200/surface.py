@@ -124,3 +124,13 @@ class ResidentProblem:
             self.close()
         except Exception:
             pass
+
+
+def solve_batch(ctx: native.Context, problems, precision: int = native.FP64) -> None:
+    """Solve resident problems together (trhepd_batch_solve): the small-beam RKN
+    ones share fused launches whatever their beam counts and angle grids, the
+    others run one after another; read each with its fetch()."""
+    problems = list(problems)
+    arr = (ctypes.c_void_p * len(problems))(*[p._h.value for p in problems])
+    ctx._check(ctx._L.trhepd_batch_solve(ctx._h, arr, len(problems), int(precision)))
+
