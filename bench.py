@@ -278,7 +278,7 @@ def uneven_leg(ctx, precision: int, per_n: int = 8, seed: int = 0) -> dict:
     """Candidate-structure batch of uneven beam counts: per_n jittered candidates
     (sigma 0.1 A) of a base structure for each N in {23, 47, 95, 191}, 61 angles,
     15 A in 0.02 A slices, all solved by one trhepd_batch_solve (the N <= 64 ones
-    in shared fused launches); the first batch solve warms up, the next two are
+    in shared fused launches); two batch solves warm up, the next two are
     timed (device time from the library's events)."""
     tmp = Path(tempfile.mkdtemp(prefix="trhepd_uneven_"))
     probs, nang = [], 0
@@ -294,7 +294,8 @@ def uneven_leg(ctx, precision: int, per_n: int = 8, seed: int = 0) -> dict:
             probs.append((sp, sp.resident()))
             nang += probs[-1][1].nangles
     rps = [rp for _, rp in probs]
-    surface.solve_batch(ctx, rps, precision)
+    for _ in range(2):  # buffers sized, graphs of the larger problems captured
+        surface.solve_batch(ctx, rps, precision)
     ms = []
     for _ in range(2):
         surface.solve_batch(ctx, rps, precision)
