@@ -75,7 +75,7 @@ def test_batch_split_form_on_the_larger_problem(ctx, tmp_path):
     probs = [_resident(ctx, tmp_path / f"s{k}", s) for k, s in enumerate(_structures())]
     ref = []
     for sp, rp in probs:
-        rp.solve(native.SPLIT_INT8)
+        rp.solve(native.FP64 if rp.nb <= 64 else native.SPLIT_INT8)
         ref.append(rp.fetch()[1])
     surface.solve_batch(ctx, [rp for _, rp in probs], native.SPLIT_INT8)
     for (sp, rp), r in zip(probs, ref):
