@@ -523,13 +523,12 @@ void gather(RunState& R, int col, bool drop_diag) {
 
 // P += cb (Q M), Qo = Q + ca P with M from R.V (gathered for the chosen form).
 void stage_product(trhepd_context* C, RunState& R, const cd* Q, cd* P, cd* Qo, double cb,
-                   double ca, bool next_is_qo = true) {
+                   double ca) {
   const cudaEvent_t* ev = C->profile ? &C->evpool[4 * R.products] : nullptr;
   if (ev) CK(cudaEventRecord(ev[0], R.st));
   if (R.split) {
     R.launches += split_stage(R.sw, Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, cb, ca,
-                              C->split_slices, R.split_variant, ev ? ev + 1 : nullptr, next_is_qo,
-                              R.st);
+                              C->split_slices, R.split_variant, ev ? ev + 1 : nullptr, R.st);
   } else {
     if (ev) CK(cudaEventRecord(ev[1], R.st));
     launch_stage_gemm_f64(Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, R.kpad, cb, ca, R.st);
@@ -546,8 +545,6 @@ void stage_product(trhepd_context* C, RunState& R, const cd* Q, cd* P, cd* Qo, d
 // growth bound every R.interval slices (policy 1); always on the last slice.
 void renormalise(trhepd_context* C, RunState& R, int l, bool every_slice) {
   const bool last = (l == R.ns);
-  if (C->renorm_policy == 0 || last || every_slice || (l % R.interval) == 0)
-    R.sw.a_valid = false;  // Q changes (for some or all angles): re-slice next time
   if (C->renorm_policy == 0 && !every_slice) {
     launch_cond_est(R.Q, R.nang, R.n, R.ld, last ? 1 : 0, R.flags, R.dval, R.st);
     launch_gauss_jordan(R.Q, R.P, R.flags, R.nang, R.n, R.ld, R.gjs, R.status, R.st);
@@ -668,7 +665,6 @@ void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) 
         gather(R, col, false);
         launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, I.bab[0] * dz, ca, R.st);
         R.launches += 1;
-        R.sw.a_valid = false;
         continue;
       }
       // k == 1, l > 1 merges the end-of-slice half kick of slice l-1 (psave) with the
@@ -699,7 +695,6 @@ void run_lf(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
   gather(R, 0, false);  // any finite stage matrix: cb = 0 below
   launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, 0.0, 0.5 * dz, R.st);
   R.launches += 1;
-  R.sw.a_valid = false;
   for (int l = 1; l <= R.ns; ++l) {
     const double dz2 = (l == R.ns) ? dz / 2 : dz;
     gather(R, l - 1, R.split);
@@ -734,7 +729,7 @@ void run_rk4(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) 
     const double step[4] = {half, half, dz, 0.0};
     for (int j = 0; j < 4; ++j) {
       gather(R, cols[j], R.split);
-      stage_product(C, R, j == 0 ? R.Q : Qt, KP, R.Qn, 1.0, 0.0, false);
+      stage_product(C, R, j == 0 ? R.Q : Qt, KP, R.Qn, 1.0, 0.0);
       launch_rk4_combine(R.Q, R.P, Qt, Pt, KP, SQ, SP, j, w[j], step[j], dz / 6, R.nang, R.n,
                          R.ld, R.st);
       R.launches += 1;

@@ -783,8 +783,7 @@ __device__ __forceinline__ uint16_t pack2(int a, int b) {
 // digit slices of the row, (Re, Im) interleaved; each lane writes two complex k.
 template <int S>
 __global__ void k_slice_rows_i8(const cd* __restrict__ Q, int rows, int n, int ld, int kr,
-                                uint32_t* __restrict__ A, int* __restrict__ erow,
-                                unsigned long long* __restrict__ rmax) {
+                                uint32_t* __restrict__ A, int* __restrict__ erow) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= rows) return;
@@ -796,10 +795,7 @@ __global__ void k_slice_rows_i8(const cd* __restrict__ Q, int rows, int n, int l
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   int e = 0;
   if (m > 0.0) frexp(m * kDigitHeadroom, &e);
-  if (lane == 0) {
-    erow[r] = e;
-    rmax[r] = (unsigned long long)__double_as_longlong(m);
-  }
+  if (lane == 0) erow[r] = e;
   const double sc = digit_scale(e, S);
   const int kw = kr / 4;      // 32-bit words per slice row (two complex k each)
   for (int w = lane; w < kw; w += 32) {
@@ -853,62 +849,13 @@ __global__ void __launch_bounds__(128) k_slice_cols_i8(const cd* __restrict__ V,
   }
 }
 
-// Rows whose digits the stage epilogue could not write with its provisional
-// exponent (an entry outgrew it): one warp per flagged row re-slices the row of
-// the new state with the exact exponent of its maximum.
-template <int S>
-__global__ void k_fix_rows_i8(const cd* __restrict__ Q, int rows, int n, int ld, int kr,
-                              uint32_t* __restrict__ A, int* __restrict__ erow,
-                              const unsigned long long* __restrict__ rmax,
-                              int* __restrict__ flag) {
-  const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (r >= rows || !flag[r]) return;
-  const int i = r % n;
-  const cd* q = Q + (size_t)r * ld;
-  const double m = __longlong_as_double((long long)rmax[r]);
-  int e = 0;
-  if (m > 0.0) frexp(m * kDigitHeadroom, &e);
-  const double sc = digit_scale(e, S);
-  const int kw = kr / 4;
-  for (int w = lane; w < kw; w += 32) {
-    const int k0 = 2 * w, k1 = 2 * w + 1;
-    const cd v0 = (k0 < n && k0 != i) ? q[k0] : cd{0.0, 0.0};
-    const cd v1 = (k1 < n && k1 != i) ? q[k1] : cd{0.0, 0.0};
-    int a[S], b[S], c[S], d[S];
-    digits_i8<S>(v0.x, sc, a);
-    digits_i8<S>(v0.y, sc, b);
-    digits_i8<S>(v1.x, sc, c);
-    digits_i8<S>(v1.y, sc, d);
-#pragma unroll
-    for (int s = 0; s < S; ++s) A[((size_t)s * rows + r) * kw + w] = pack4(a[s], b[s], c[s], d[s]);
-  }
-  __syncwarp();
-  if (lane == 0) {
-    erow[r] = e;
-    flag[r] = 0;
-  }
-}
-
-// What the INT8 epilogue needs beyond the common arguments: where it writes the
-// digit slices of the new state Q' (exponent: one above that of the previous
-// state's row maximum), the row maxima of both states and the overflow flags.
-struct EpiArgsI8 {
-  uint8_t* An;                        // [S][rows][kr] digit slices of Q'
-  int* erow_n;                        // their row exponents
-  const unsigned long long* rmax_c;   // off-diagonal row maxima of Q (double bits)
-  unsigned long long* rmax_n;         // of Q', accumulated with atomicMax
-  int* flag;                          // rows whose provisional exponent overflowed
-  int kr, kc;
-};
-
 // Persistent INT8 stage product: the warp roles, barriers, register split and the
 // register-held drain of k_split_gemm_p, with S INT32 accumulators.
 template <int S>
 __global__ void __launch_bounds__(P_THREADS, 1)
     k_split_gemm_i8(const __grid_constant__ CUtensorMap tmA,
-                    const __grid_constant__ CUtensorMap tmB, EpiArgs ep, EpiArgsI8 nx, int nkb,
-                    int tiles_n, int tiles) {
+                    const __grid_constant__ CUtensorMap tmB, EpiArgs ep, int nkb, int tiles_n,
+                    int tiles) {
   static_assert(S * NT <= TMEM_COLS, "INT8 levels exceed the tensor memory");
   constexpr int STAGES = i8::stages_for(S);
   if (*(volatile unsigned*)ep.status & kStatusTimeout) return;
@@ -1095,22 +1042,13 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&tempty);
-      cd qd[2][2];      // diagonal of each of this lane's rows
-      double rml[2][2];  // off-diagonal maximum of the row in this tile of Q'
-      int en[2][2];      // provisional exponent of the row in Q'
-      unsigned ovf = 0;  // bit 2h+u: an entry of that row outgrew it
+      cd qd[2][2];  // diagonal of each of this lane's rows
 #pragma unroll
       for (int h = 0; h < 2; ++h)
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
           const int r = m0 + 16 * h + 8 * u + t1;
           qd[h][u] = (r < ep.rows) ? ep.Q[(size_t)r * ep.ld + ri[h][u]] : cd{0.0, 0.0};
-          int e = 0;
-          const double m =
-              (r < ep.rows) ? __longlong_as_double((long long)nx.rmax_c[r]) : 0.0;
-          if (m > 0.0) frexp(m * kDigitHeadroom, &e);
-          en[h][u] = e + 1;
-          rml[h][u] = 0.0;
         }
 #pragma unroll
       for (int g = 0; g < 8; ++g) {
@@ -1132,67 +1070,16 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
             const int r = m0 + 16 * h + 8 * u + t1;
-            cd nxt = cd{0.0, 0.0};  // entry of Q' off the diagonal (0 outside)
             if (r < ep.rows && j < ep.n) {
               const size_t ro = (size_t)r * ep.ld;
               const cd acc = vals[g][h][u] + qd[h][u] * vv[u] + qv[u] * (dv[u] + vd);
               const cd p = pv[u] + ep.cb * acc;
               ep.P[ro + j] = p;
-              const cd qo = qv[u] + ep.ca * p;
-              ep.Qo[ro + j] = qo;
-              if (j != ri[h][u]) nxt = qo;
+              ep.Qo[ro + j] = qv[u] + ep.ca * p;
             }
-            // digits of Q' for the next stage: 16 bits (Re, Im digit) per slice,
-            // gathered so that lane t0 = s stores slice s of 4 adjacent columns
-            rml[h][u] = fmax(rml[h][u], fmax(fabs(nxt.x), fabs(nxt.y)));
-            const double scn = digit_scale(en[h][u], S);
-            // |X| below 2^(7 + 8(S-1)) (1 - 2^-7) keeps the leading digit within +-127
-            constexpr double kLim = (double)(1ull << (7 + 8 * (S - 1))) * (1.0 - 1.0 / 128);
-            double yr = nxt.x * scn, yi = nxt.y * scn;
-            if (fabs(yr) >= kLim || fabs(yi) >= kLim) {
-              ovf |= 1u << (2 * h + u);
-              yr = 0.0;
-              yi = 0.0;
-            }
-            int dr[S], di[S];
-            digits_i8<S>(yr, 1.0, dr);
-            digits_i8<S>(yi, 1.0, di);
-            unsigned long long W = 0;
-#pragma unroll
-            for (int s = 0; s < S; ++s)
-              W |= (unsigned long long)((dr[s] & 255) | ((di[s] & 255) << 8)) << (16 * s);
-            unsigned long long out = 0;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              const unsigned val = (unsigned)((W >> (16 * ((t0 - c) & 3))) & 0xFFFFu);
-              const unsigned got = __shfl_sync(0xffffffffu, val, (lane & ~3) | ((t0 + c) & 3));
-              out |= (unsigned long long)got << (16 * ((t0 + c) & 3));
-            }
-            const int jg = jh + 4 * g;  // first column of the group (multiple of 4)
-            if (t0 < S && r < ep.rows && jg < nx.kc)
-              *reinterpret_cast<unsigned long long*>(nx.An + ((size_t)t0 * ep.rows + r) * nx.kr +
-                                                     2 * jg) = out;
           }
         }
       }
-      // row maxima and overflow flags of Q' (the 4 lanes of a row combine)
-#pragma unroll
-      for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          double m = rml[h][u];
-          m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 1));
-          m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 2));
-          int o = (ovf >> (2 * h + u)) & 1;
-          o |= __shfl_xor_sync(0xffffffffu, o, 1);
-          o |= __shfl_xor_sync(0xffffffffu, o, 2);
-          const int r = m0 + 16 * h + 8 * u + t1;
-          if (t0 == 0 && r < ep.rows) {
-            atomicMax(nx.rmax_n + r, (unsigned long long)__double_as_longlong(m));
-            if (o) nx.flag[r] = 1;
-            nx.erow_n[r] = en[h][u];
-          }
-        }
     }
   }
   tc_fence_before();
@@ -1342,70 +1229,19 @@ void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V,
   }
 }
 
-// INT8 workspace: two A digit buffers (the stage's input and its output state),
-// B^T digits, row exponents and maxima for both, column exponents, row flags.
-struct CarveI8 {
-  uint8_t* A[2];
-  uint16_t* B;
-  int* erow[2];
-  unsigned long long* rmax[2];
-  int* fcol;
-  int* flag;
-  int rows, kc, kr, npad, nrows;
-  size_t bytes;
-};
-
-CarveI8 carve_i8(void* base, int nang, int n, int S) {
-  CarveI8 c;
-  c.rows = nang * n;
-  c.kc = round_up(n, 16);
-  c.kr = 2 * c.kc;
-  c.npad = round_up(n, split::NC);
-  c.nrows = 2 * c.npad;
-  char* p = reinterpret_cast<char*>(base);
-  size_t o = 0;
-  for (int q = 0; q < 2; ++q) {
-    c.A[q] = reinterpret_cast<uint8_t*>(p + o);
-    o = align256(o + (size_t)S * c.rows * c.kr);
-  }
-  c.B = reinterpret_cast<uint16_t*>(p + o);
-  o = align256(o + (size_t)S * c.nrows * c.kc * 2);
-  for (int q = 0; q < 2; ++q) {
-    c.erow[q] = reinterpret_cast<int*>(p + o);
-    o = align256(o + (size_t)c.rows * sizeof(int));
-    c.rmax[q] = reinterpret_cast<unsigned long long*>(p + o);
-    o = align256(o + (size_t)c.rows * sizeof(unsigned long long));
-  }
-  c.fcol = reinterpret_cast<int*>(p + o);
-  o = align256(o + (size_t)c.npad * sizeof(int));
-  c.flag = reinterpret_cast<int*>(p + o);
-  o = align256(o + (size_t)c.rows * sizeof(int));
-  c.bytes = o + 256;
-  return c;
-}
-
-// One INT8 stage product.  The A digits of Q come from the previous stage's
-// epilogue when w.a_valid, else from the slicing kernel; the epilogue writes the
-// digits of Qo into the other buffer (rows it could not fit are re-sliced by
-// k_fix_rows_i8), which the next call uses when next_is_qo.
 template <int S>
-int run_split_i8(SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
-                 int nang, int n, int ld, double cb, double ca, const cudaEvent_t* ev,
-                 bool next_is_qo, cudaStream_t st) {
-  CarveI8 c = carve_i8(w.base, nang, n, S);
-  const int cur = w.cur, nxt = 1 - w.cur;
-  int launches = 3;
-  split::k_slice_cols_i8<S><<<n, 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, c.B);
-  if (!w.a_valid) {
-    split::k_slice_rows_i8<S><<<ceil_div(c.rows, 8), 256, 0, st>>>(
-        Q, c.rows, n, ld, c.kr, reinterpret_cast<uint32_t*>(c.A[cur]), c.erow[cur], c.rmax[cur]);
-    ++launches;
-  }
-  cudaMemsetAsync(c.rmax[nxt], 0, (size_t)c.rows * sizeof(unsigned long long), st);
-  CUtensorMap ta = make_map(c.A[cur], c.kr, c.rows, S, 1);
-  CUtensorMap tb = make_map(c.B, c.kr, c.nrows, S, 1);
-  split::EpiArgs ep{Q, P, Qo, V, D, c.erow[cur], c.fcol, w.status, c.rows, n, ld, c.kc, S, cb, ca};
-  split::EpiArgsI8 nx{c.A[nxt], c.erow[nxt], c.rmax[cur], c.rmax[nxt], c.flag, c.kr, c.kc};
+void run_split_i8(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
+                  int nang, int n, int ld, double cb, double ca, const cudaEvent_t* ev,
+                  cudaStream_t st) {
+  Carve c = carve(w.base, nang, n, S, 2);
+  const int kr = 2 * c.kc;
+  uint16_t* B = reinterpret_cast<uint16_t*>(c.B);
+  uint32_t* A = reinterpret_cast<uint32_t*>(c.A);
+  split::k_slice_cols_i8<S><<<n, 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, B);
+  split::k_slice_rows_i8<S><<<ceil_div(c.rows, 8), 256, 0, st>>>(Q, c.rows, n, ld, kr, A, c.erow);
+  CUtensorMap ta = make_map(c.A, kr, c.rows, S, 1);
+  CUtensorMap tb = make_map(c.B, kr, c.nrows, S, 1);
+  split::EpiArgs ep{Q, P, Qo, V, D, c.erow, c.fcol, w.status, c.rows, n, ld, c.kc, S, cb, ca};
   const int tiles_n = c.nrows / split::NT, tiles_m = ceil_div(c.rows, split::BM);
   const size_t smem = split::i8::smem_bytes(S);
   static bool attr[6] = {false, false, false, false, false, false};
@@ -1424,23 +1260,15 @@ int run_split_i8(SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, con
   const int grid = std::min(tiles, sm_count());
   if (ev) cudaEventRecord(ev[0], st);
   split::k_split_gemm_i8<S><<<grid, split::P_THREADS, smem, st>>>(
-      ta, tb, ep, nx, ceil_div(c.kr, split::i8::BK), tiles_n, tiles);
+      ta, tb, ep, ceil_div(kr, split::i8::BK), tiles_n, tiles);
   if (ev) cudaEventRecord(ev[1], st);
-  split::k_fix_rows_i8<S><<<ceil_div(c.rows, 8), 256, 0, st>>>(
-      Qo, c.rows, n, ld, c.kr, reinterpret_cast<uint32_t*>(c.A[nxt]), c.erow[nxt], c.rmax[nxt],
-      c.flag);
-  w.cur = nxt;
-  w.a_valid = next_is_qo;
-  return launches;
 }
 
 }  // namespace
 
 size_t split_workspace_bytes(int nang, int n, int slices) {
   Carve c = carve(nullptr, nang, n, slices);
-  const size_t bf16 = reinterpret_cast<size_t>(c.fcol) + align256((size_t)c.npad * sizeof(int)) + 256;
-  const size_t i8 = carve_i8(nullptr, nang, n, std::min(slices, 4)).bytes;
-  return std::max(bf16, i8);
+  return reinterpret_cast<size_t>(c.fcol) + align256((size_t)c.npad * sizeof(int)) + 256;
 }
 
 SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, unsigned* status,
@@ -1456,20 +1284,22 @@ SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, un
   return w;
 }
 
-int split_stage(SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
+int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
                 int nang, int n, int ld, double cb, double ca, int slices, int variant,
-                const cudaEvent_t* ev, bool next_is_qo, cudaStream_t st) {
+                const cudaEvent_t* ev, cudaStream_t st) {
   if (variant == kSplitInt8) {
     switch (slices) {
       case 3:
-        return run_split_i8<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, next_is_qo, st);
+        run_split_i8<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, st);
+        break;
       case 4:
-        return run_split_i8<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, next_is_qo, st);
+        run_split_i8<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, st);
+        break;
       default:
         throw std::invalid_argument("INT8 split slices must be 3 or 4");
     }
+    return 4;
   }
-  w.a_valid = false;
   if (variant != kSplitPersistent && variant != kSplitPerTile)
     throw std::invalid_argument("unknown split kernel variant");
   switch (slices) {

@@ -10,11 +10,6 @@ struct SplitWorkspace {
   void* base = nullptr;
   int nang = 0, n = 0, slices = 0;
   unsigned* status = nullptr;  // device status word (kStatus* bits)
-  // INT8 form: the epilogue of a stage writes the digit slices of its output
-  // state into the other A buffer; a_valid says whether A[cur] holds the digits
-  // of the state the next stage multiplies (false after any other change of Q)
-  int cur = 0;
-  bool a_valid = false;
 };
 
 size_t split_workspace_bytes(int nang, int n, int slices);
@@ -34,10 +29,8 @@ enum SplitVariant { kSplitPersistent = 0, kSplitPerTile = 1, kSplitInt8 = 2 };
 // P += cb*(Q V + Q o D_a) with the potential product from BF16 or INT8 slices;
 // Qo = Q + ca*P.  When `ev` is given, ev[0] and ev[1] are recorded around the
 // tensor-core kernel.  Returns the number of kernels launched.
-// next_is_qo: the next stage product multiplies Qo (RKN, leapfrog), so the INT8
-// form keeps the digits its epilogue writes; otherwise it re-slices next time.
-int split_stage(SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
+int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
                 int nang, int n, int ld, double cb, double ca, int slices, int variant,
-                const cudaEvent_t* ev, bool next_is_qo, cudaStream_t st);
+                const cudaEvent_t* ev, cudaStream_t st);
 
 }  // namespace trhepd
