@@ -206,6 +206,20 @@ int trhepd_problem_solve(trhepd_context* ctx, trhepd_problem* pb, int precision)
    read with trhepd_problem_fetch; trhepd_last_stats reports the whole batch. */
 int trhepd_batch_solve(trhepd_context* ctx, trhepd_problem* const* problems, int count,
                        int precision);
+
+/* Gaussian convolution of rocking curves (make_convolution.py,
+   str-lapack/tool/make_convolution.py:21-29, 97-109): f2[rows][nb] with angles
+   angle_deg[rows] (degrees) in blocks of `scan` consecutive rows (one block per
+   outer loop index of srfref, so scan = the inner scan's angle count);
+   out[i][b] = sum_k f2[k][b] g(theta_i - theta_k) dtheta within a block, g the
+   normalised Gaussian of FWHM omega_deg, dtheta the block's first angle step. */
+int trhepd_rocking_convolution(trhepd_context* ctx, const double* angle_deg, const double* f2,
+                               int rows, int scan, int nb, double omega_deg, double* out);
+/* The same on a solved resident problem's intensities, on the device (no round
+   trip of the intensities); out: (nangles, nb) host buffer.  No counterpart in the
+   reference beyond make_convolution.py. */
+int trhepd_problem_convolve(trhepd_context* ctx, trhepd_problem* pb, double omega_deg,
+                            double* out);
 int trhepd_problem_fetch(trhepd_context* ctx, trhepd_problem* pb, double* f2, double* angle_deg);
 int trhepd_problem_info(const trhepd_problem* pb, int64_t* out, int n);
 void trhepd_problem_destroy(trhepd_problem* pb);

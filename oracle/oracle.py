@@ -137,3 +137,25 @@ def set_bulk_scale(s: float) -> None:
 def set_max_slices(n: int) -> None:
     """Integrate only the first n slices (0 = all); for bounded timing samples."""
     lib().oracle_set_max_slices(int(n))
+
+
+def rocking_convolution(angle_deg, f2, omega: float = 0.5, scan: int | None = None):
+    """Gaussian convolution of rocking curves along the scanned angle, restating
+    the reference's make_convolution.py (str-lapack/tool/make_convolution.py:21-29
+    for sigma = omega / (2 sqrt(2 ln 2)) and the normalised Gaussian, :97-109 for
+    C_i = sum_k I_k g(theta_i - theta_k) dtheta with dtheta = theta_1 - theta_0).
+    Rows come in consecutive blocks of `scan` angles (one block per outer loop
+    index of srfref; the script handles one block); each block is convolved alone."""
+    import numpy as np
+    angle_deg = np.asarray(angle_deg, dtype=float)
+    f2 = np.asarray(f2, dtype=float)
+    scan = scan or len(angle_deg)
+    sigma = 0.5 * omega / np.sqrt(2.0 * np.log(2.0))
+    out = np.zeros_like(f2)
+    for b0 in range(0, len(angle_deg), scan):
+        a = angle_deg[b0:b0 + scan]
+        d = a[1] - a[0]
+        x = a[:, None] - a[None, :]
+        g = (1.0 / (sigma * np.sqrt(2.0 * np.pi))) * np.exp(-0.5 * x ** 2 / sigma ** 2)
+        out[b0:b0 + scan] = (g * d) @ f2[b0:b0 + scan]
+    return out

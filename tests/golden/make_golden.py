@@ -7,7 +7,9 @@ and writes, per test case (test23 / test47 / test521):
   reference's regression runs used (test/<case>/);
 * ``<case>/perf-<method>-<dz>.npz`` — angles and intensities of the committed
   outputs test/<case>/test-results/perf-<method>-<dz>.txt (E23.15, 15 digits),
-  for the integrators and slice thicknesses listed below.
+  for the integrators and slice thicknesses listed below;
+* ``conv-<name>.npz`` — a sample's rocking curves (surf-bulkP.s) and the
+  convolution.txt the reference's make_convolution.py wrote from them.
 
 Run once in a container that has the reference; the fixtures travel with the
 repository and nothing at test time reads the reference.
@@ -28,6 +30,9 @@ SEL = {
 }
 
 
+CONV = [("ge001", "sim-trhepd-rheed", "Ge_001_c4x2"), ("t4al", "str-lapack", "T4Al_on_Si_111")]
+
+
 def parse_s(path):
     sys.path.insert(0, str(HERE.parents[1] / "trhepd-opt_b200"))
     from formats import read_rocking_curves
@@ -46,6 +51,14 @@ def main(ref: Path):
             ang, f2, hdr = parse_s(p)
             np.savez_compressed(dst / f"perf-{m}-{dz}.npz", angle=ang, f2=f2,
                                 beams=hdr["beams"], naz=hdr["naz"], ng=hdr["ng"])
+    # rocking-curve convolution samples: the reference's surf-bulkP.s and the
+    # convolution.txt its make_convolution.py wrote from it (omega 0.5 deg)
+    for name, tree, samp in CONV:
+        src = ref / tree / "sample" / samp / "output"
+        ang, f2, hdr = parse_s(src / "surf-bulkP.s")
+        conv = np.loadtxt(src / "convolution.txt")
+        np.savez_compressed(HERE / f"conv-{name}.npz", angle=ang, f2=f2, beams=hdr["beams"],
+                            conv=conv[:, 1:], conv_angle=conv[:, 0])
     print("fixtures written to", HERE)
 
 

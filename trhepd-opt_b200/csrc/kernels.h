@@ -91,5 +91,9 @@ void launch_intensities(const cd* R, const cd* gam, const double* wnsga2, int na
                         int nb0, double* f2, cudaStream_t st);
 // Non-finite scan of a state buffer (sets kStatusNonFinite).
 void launch_check_finite(const cd* X, size_t count, unsigned* status, cudaStream_t st);
+// Gaussian convolution (FWHM omega, degrees) of rocking curves f2[rows][nb] along
+// their angles ang[rows], in blocks of `scan` consecutive rows (make_convolution.py).
+void launch_rocking_convolution(const double* ang, const double* f2, int rows, int scan, int nb,
+                                double omega, double* out, cudaStream_t st);
 
 }  // namespace trhepd

@@ -800,3 +800,38 @@ void launch_check_finite(const cd* X, size_t count, unsigned* status, cudaStream
 }
 
 }  // namespace trhepd
+
+namespace trhepd {
+
+// ============================================================ rocking-curve convolution
+// make_convolution.py (str-lapack/tool/make_convolution.py:21-29, 97-109): rows in
+// blocks of `scan` consecutive angles; within a block
+//   out[i][b] = sum_k f2[k][b] g(theta_i - theta_k) dtheta,  dtheta = theta_1 - theta_0,
+//   g(x) = exp(-x^2 / (2 sigma^2)) / (sigma sqrt(2 pi)),     sigma = omega / (2 sqrt(2 ln 2)),
+// summed in the script's order.  One thread per (row, beam).
+__global__ void k_rocking_convolution(const double* __restrict__ ang,
+                                      const double* __restrict__ f2, int rows, int scan, int nb,
+                                      double sigma, double* __restrict__ out) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (b >= nb || i >= rows) return;
+  const int b0 = (i / scan) * scan;
+  const double d = ang[b0 + 1] - ang[b0];
+  const double norm = 1.0 / (sigma * sqrt(2.0 * 3.14159265358979323846));
+  double acc = 0.0;
+  for (int k = 0; k < scan; ++k) {
+    const double x = ang[i] - ang[b0 + k];
+    const double g = norm * exp(-0.5 * (x * x) / (sigma * sigma));
+    acc += f2[(size_t)(b0 + k) * nb + b] * g * d;
+  }
+  out[(size_t)i * nb + b] = acc;
+}
+
+void launch_rocking_convolution(const double* ang, const double* f2, int rows, int scan, int nb,
+                                double omega, double* out, cudaStream_t st) {
+  const double sigma = 0.5 * omega / std::sqrt(2.0 * std::log(2.0));
+  dim3 grid(ceil_div(nb, 128), rows);
+  k_rocking_convolution<<<grid, 128, 0, st>>>(ang, f2, rows, scan, nb, sigma, out);
+}
+
+}  // namespace trhepd

@@ -184,6 +184,7 @@ struct trhepd_context {
   DevBuf asf, b, dchg, ghk, z[3], ocr[3], ielm[3], st[3], depth, table, pair;
   DevBuf Q0, Q1, P, V, D, gam, F, flags, dval, gj, f2, wnsga2, status, split;
   DevBuf sgh, sgk, simg, snimg, sst;
+  DevBuf cva, cvf, cvo;  // rocking-curve convolution of host curves
   DevBuf bk[24];  // bulk-solve work arrays
   DevBuf rk[5];   // RK4 / Magnus stage buffers
   DevBuf mg[9];   // Magnus shared matrices
@@ -318,10 +319,11 @@ struct OwnWorkspace {
 // fetched.
 struct trhepd_problem {
   int n = 0, ns = 0, nv = 0, nang = 0, ld = 0, nb0 = 0, int_method = 5;
+  int nrep2 = 1;               // angles of the inner scan (rows per block of the output)
   Integrator I{};
   double dz = 0, kappa_max = 0;
   int ncol = 0;
-  DevBuf table, pair, gam, D, F, wnsga2, f2;
+  DevBuf table, pair, gam, D, F, wnsga2, f2, dang, conv;
   std::vector<double> angle_deg;
   // CUDA graph of the whole solve, valid for `graph_key` and the context buffers
   // in `graph_sig`; `last_sig` holds the buffers of the last uncaptured solve.
@@ -341,7 +343,7 @@ struct trhepd_problem {
   void release() {
     drop_graph();
     own.release();
-    for (DevBuf* b : {&table, &pair, &gam, &D, &F, &wnsga2, &f2}) b->release();
+    for (DevBuf* b : {&table, &pair, &gam, &D, &F, &wnsga2, &f2, &dang, &conv}) b->release();
   }
 };
 
@@ -386,6 +388,7 @@ void prepare(trhepd_context* C, const SolveArgs& A, trhepd_problem& Pb) {
   if ((long long)nang * n > 65535)
     throw std::invalid_argument("angles x beams exceeds 65535 stacked rows; split the scan");
   Pb.nang = nang;
+  Pb.nrep2 = nrep2;
   Pb.ld = ld;
   std::vector<cd> gam((size_t)nang * n), Dm((size_t)nang * ld, cd{0, 0}), F((size_t)nang * n * n);
   std::vector<double> wnsga2(nang);
@@ -1439,7 +1442,7 @@ void trhepd_destroy(trhepd_context* c) {
   DevBuf* all[] = {&c->asf, &c->b, &c->dchg, &c->ghk, &c->depth, &c->table, &c->pair,
                    &c->Q0, &c->Q1, &c->P, &c->V, &c->D, &c->gam, &c->F, &c->flags, &c->dval,
                    &c->gj, &c->f2, &c->wnsga2, &c->status, &c->split, &c->sgh, &c->sgk,
-                   &c->simg, &c->snimg, &c->sst};
+                   &c->simg, &c->snimg, &c->sst, &c->cva, &c->cvf, &c->cvo};
   for (DevBuf* b : all) b->release();
   for (int p = 0; p < 3; ++p) {
     c->z[p].release();
@@ -1617,6 +1620,44 @@ int trhepd_problem_solve(trhepd_context* ctx, trhepd_problem* pb, int precision)
     if (!valid_precision(precision))
       throw std::invalid_argument("unknown precision form");
     run(ctx, *pb, precision);
+  });
+}
+
+int trhepd_rocking_convolution(trhepd_context* ctx, const double* angle_deg, const double* f2,
+                               int rows, int scan, int nb, double omega_deg, double* out) {
+  return guarded(ctx, [&] {
+    if (!angle_deg || !f2 || !out || rows < 2 || scan < 2 || nb < 1 || rows % scan ||
+        !(omega_deg > 0))
+      throw std::invalid_argument("bad convolution arguments");
+    cudaStream_t st = ctx->stream;
+    double* da = (double*)ctx->cva.ensure((size_t)rows * sizeof(double));
+    double* df = (double*)ctx->cvf.ensure((size_t)rows * nb * sizeof(double));
+    double* dout = (double*)ctx->cvo.ensure((size_t)rows * nb * sizeof(double));
+    CK(cudaMemcpyAsync(da, angle_deg, (size_t)rows * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(df, f2, (size_t)rows * nb * sizeof(double), cudaMemcpyHostToDevice, st));
+    launch_rocking_convolution(da, df, rows, scan, nb, omega_deg, dout, st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout, (size_t)rows * nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int trhepd_problem_convolve(trhepd_context* ctx, trhepd_problem* pb, double omega_deg,
+                            double* out) {
+  return guarded(ctx, [&] {
+    if (!pb || !out || !(omega_deg > 0)) throw std::invalid_argument("bad convolution arguments");
+    if (pb->nrep2 < 2) throw std::invalid_argument("the inner scan has fewer than 2 angles");
+    cudaStream_t st = ctx->stream;
+    const size_t rows = (size_t)pb->nang, nb = (size_t)pb->n;
+    double* da = (double*)pb->dang.ensure(rows * sizeof(double));
+    CK(cudaMemcpyAsync(da, pb->angle_deg.data(), rows * sizeof(double), cudaMemcpyHostToDevice,
+                       st));
+    double* dout = (double*)pb->conv.ensure(rows * nb * sizeof(double));
+    launch_rocking_convolution(da, pb->f2.as<double>(), (int)rows, pb->nrep2, (int)nb, omega_deg,
+                               dout, st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout, rows * nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
   });
 }
 

@@ -438,10 +438,6 @@ static_assert(128 * P_REG_CTRL + 256 * P_REG_EPI <= P_THREADS * P_REG_LAUNCH,
 __host__ __device__ constexpr int pstages_for(int S) { return stages_for(S); }
 inline size_t psmem_bytes(int S) { return smem_bytes(S); }
 
-// Bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned) into L2 by the TMA unit.
-__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -979,25 +975,6 @@ __global__ void __launch_bounds__(P_THREADS, 1)
         consumed_sh = g;
         tc_commit(&drain_bar);
         if (!mbar_wait(&drain_bar, 0)) atomicOr(ep.status, kStatusTimeout);
-      }
-    } else {
-      // ---------------- warps 2-3: when a tile's mainloop starts, prefetch the Q and
-      // P rows its epilogue will read into L2 (64 rows per warp, 1 KB per row)
-      const int pw = warp - 2;
-      int it = 0;
-      for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
-        if (it > 0 && !mbar_wait(&tfull, (it - 1) & 1)) break;
-        if (ld_volatile(&abort_sh)) break;
-        const int m0 = (tile / tiles_n) * BM, j0 = (tile % tiles_n) * NC;
-        const int cols = min(NC, ep.n - j0);
-        if (cols <= 0) continue;
-        for (int rl = pw * 64 + lane; rl < pw * 64 + 64; rl += 32) {
-          const int r = m0 + rl;
-          if (r >= ep.rows) break;
-          const size_t o = (size_t)r * ep.ld + j0;
-          prefetch_l2_bulk(ep.Q + o, (uint32_t)cols * 16u);
-          prefetch_l2_bulk(ep.P + o, (uint32_t)cols * 16u);
-        }
       }
     }
   } else {

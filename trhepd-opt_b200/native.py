@@ -32,7 +32,7 @@ EXPORTS = [
     "trhepd_create", "trhepd_destroy", "trhepd_last_error", "trhepd_set_option",
     "trhepd_last_stats", "trhepd_structure_factors", "trhepd_plane_group_images",
     "trhepd_potential_table", "trhepd_srfref", "trhepd_surf_run", "trhepd_surf_load",
-    "trhepd_surf_free", "trhepd_surf_views", "trhepd_problem_create", "trhepd_problem_solve", "trhepd_batch_solve",
+    "trhepd_surf_free", "trhepd_surf_views", "trhepd_problem_create", "trhepd_problem_solve", "trhepd_batch_solve", "trhepd_rocking_convolution", "trhepd_problem_convolve",
     "trhepd_problem_fetch", "trhepd_problem_info", "trhepd_problem_destroy",
     "trhepd_potential_table_noalloc", "trhepd_bulk_run",
 ]
@@ -112,6 +112,8 @@ def load():
                                         ctypes.POINTER(_P)]
     L.trhepd_problem_solve.argtypes = [_P, _P, _I]
     L.trhepd_batch_solve.argtypes = [_P, _P, _I, _I]
+    L.trhepd_rocking_convolution.argtypes = [_P, _P, _P, _I, _I, _I, _D, _P]
+    L.trhepd_problem_convolve.argtypes = [_P, _P, _D, _P]
     L.trhepd_problem_fetch.argtypes = [_P, _P, _P, _P]
     L.trhepd_problem_info.argtypes = [_P, _P, _I]
     L.trhepd_potential_table_noalloc.argtypes = [_P, _I, _I, _D, _P, _P, _P]
@@ -187,6 +189,17 @@ class Context:
                                             str(out_path).encode(), st.ctypes.data))
         return {"device_ms": float(st[0]), "layers": int(st[1]), "double_angle_steps": int(st[2]),
                 "items": int(st[3])}
+
+    def rocking_convolution(self, angle_deg, f2, omega: float = 0.5, scan: int | None = None):
+        """Gaussian convolution of rocking curves on the GPU (make_convolution.py)."""
+        ang = np.ascontiguousarray(angle_deg, dtype=np.float64)
+        f = np.ascontiguousarray(f2, dtype=np.float64)
+        out = np.zeros_like(f)
+        rows, nb = f.shape
+        self._check(self._L.trhepd_rocking_convolution(self._h, ang.ctypes.data, f.ctypes.data,
+                                                       rows, int(scan or rows), nb,
+                                                       float(omega), out.ctypes.data))
+        return out
 
     def close(self):
         if getattr(self, "_h", None):

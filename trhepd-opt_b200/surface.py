@@ -114,6 +114,13 @@ class ResidentProblem:
                                                      ang.ctypes.data))
         return ang, f2
 
+    def convolve(self, omega: float = 0.5):
+        """The solved intensities convolved on the device (make_convolution.py)."""
+        out = np.zeros((self.nangles, self.nb))
+        self.ctx._check(self._L.trhepd_problem_convolve(self.ctx._h, self._h, float(omega),
+                                                        out.ctypes.data))
+        return out
+
     def close(self):
         if getattr(self, "_h", None):
             self._L.trhepd_problem_destroy(self._h)
