@@ -327,6 +327,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven candidate batch")
+    ap.add_argument("--uneven-per-n", type=int, default=8,
+                    help="candidates per beam count in the uneven batch (64: 256 structures)")
     ap.add_argument("--serve-seconds", type=float, default=40.0)
     ap.add_argument("--serve-load", type=float, default=0.5,
                     help="arrival rate as a fraction of the isolated-solve throughput")
@@ -521,7 +523,7 @@ def main():
     sp.close()
     uneven = None
     if rank == 0 and ws == 1 and not args.no_uneven:
-        uneven = uneven_leg(ctx, prec)
+        uneven = uneven_leg(ctx, prec, per_n=args.uneven_per_n)
     ctx.close()
 
     serve = None
