@@ -247,9 +247,14 @@ def serve_leg(device: int, seconds: float, load: float, precision: int, seed: in
     """Poisson stream of mixed-N refinement requests through the serving loop at
     `load` times the throughput the isolated solve times allow; reports p50/p99
     latency, angle-solves/s and each request's latency over its isolated time."""
-    from trhepd_opt_b200 import serving
+    from trhepd_opt_b200 import autotune, serving
+    tctx = native.Context(device)
+    try:
+        table = autotune.tune(tctx, beam_counts=tuple(serving.DEFAULT_MIX))
+    finally:
+        tctx.close()
     srv = serving.Server(device=device, slots=serving.DEFAULT_SLOTS, mem_budget_gb=120.0,
-                         precision=precision)
+                         precision=precision, schedules=table)
     try:
         cases = [(n, g) for n in serving.DEFAULT_MIX for g in serving.GRIDS]
         iso = serving.isolated_times(srv, cases)
@@ -261,6 +266,8 @@ def serve_leg(device: int, seconds: float, load: float, precision: int, seed: in
     finally:
         srv.close()
     out["by_n"] = {str(k): v for k, v in out["by_n"].items()}
+    out["schedules"] = {str(n): {"fp64": e["fp64"], "split": e["split"],
+                                 "times_ms": e["times_ms"]} for n, e in table.items()}
     out.update({"arrival_rate_req_s": rate, "duration_s": seconds, "target_load": load,
                 "mean_isolated_request_s": busy,
                 "isolated_s": {f"{n}x{g}": t for (n, g), t in iso.items()},

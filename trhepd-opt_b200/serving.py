@@ -133,9 +133,12 @@ class _Pending:
 class Server:
     def __init__(self, device: int = 0, slots=DEFAULT_SLOTS, mem_budget_gb: float = 120.0,
                  precision: int = native.FP64, region: float = 15.0, dz: float = 0.02,
-                 renorm_policy: int = 1):
+                 renorm_policy: int = 1, schedules: dict | None = None):
         """`slots`: a sequence of (smallest N, largest N, stream priority) per slot,
-        or an int k for k slots that take any request at the default priority."""
+        or an int k for k slots that take any request at the default priority.
+        `schedules`: an autotune table (N -> chosen schedules); a request uses the
+        entry of the nearest tuned N, else the fixed rule of precision_for."""
+        self.schedules = schedules
         if isinstance(slots, int):
             slots = tuple((0, 1 << 30, 0.0) for _ in range(slots))
         self.layout = tuple(slots)
@@ -206,6 +209,17 @@ class Server:
         """The form a request of n beams runs in: fused FP64 up to 64 beams."""
         return native.FP64 if n <= FUSED_MAX_N else self.precision
 
+    def _configure(self, ctx: native.Context, n: int) -> int:
+        """Set the slot context for a request of n beams; returns its precision."""
+        if not self.schedules:
+            ctx.set_option(native.OPT_FUSED_MAX_N, FUSED_MAX_N)
+            return self.precision_for(n)
+        from . import autotune
+        near = min(self.schedules, key=lambda k: abs(k - n))
+        entry = self.schedules[near]
+        name = entry["fp64"] if self.precision == native.FP64 else entry["split"]
+        return autotune.apply(ctx, autotune.schedule_by_name(name))
+
     def _work(self, ctx: native.Context, lo: int, hi: int) -> None:
         while True:
             r = self.q.get(lo, hi)
@@ -220,7 +234,7 @@ class Server:
                 self._admit(need)
                 r.start = time.perf_counter() - self.t0
                 rp = sp.resident()
-                rp.solve(self.precision_for(r.n))
+                rp.solve(self._configure(ctx, r.n))
                 r.device_ms = ctx.last_stats()["device_ms"]
                 _, r.f2 = rp.fetch()
                 rp.close()
