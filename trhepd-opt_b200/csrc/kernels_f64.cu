@@ -405,12 +405,13 @@ void launch_cond_est(const cd* Q, int nang, int n, int ld, int force, int* flag,
 // ============================================================ K8 blocked Gauss-Jordan
 // [Q | P] -> [I | Q^{-1} P] with partial pivoting (pivot = max |re|+|im| among the
 // rows not yet used, lowest index on ties, as zgetrf's izamax).  Panels of kW
-// columns: the panel kernel factors rows c0.. of the panel (LU with row swaps) and
+// columns (24 where the n x 24 panel fits shared memory, else 16; fewer panels
+// mean fewer passes over the trailing matrix): the panel kernel factors rows c0.. of the panel (LU with row swaps) and
 // forms W1 = B1^{-1} and the elimination multipliers L2 = B2 B1^{-1} for every
 // other row; the update kernel applies the swaps and
 //   C1 <- W1 C1,   C2 <- C2 - L2 C1
 // to all remaining columns (Q columns right of the panel and every P column).
-constexpr int kW = 16;
+constexpr int kWMax = 24;      // widest panel; the scratch is sized for it
 constexpr int kUpdCols = 128;  // trailing columns per update block
 
 struct GJScratch {
@@ -420,11 +421,11 @@ struct GJScratch {
 };
 
 size_t gj_scratch_bytes(int nang, int n) {
-  size_t b = (size_t)nang * kW * sizeof(int);
+  size_t b = (size_t)nang * kWMax * sizeof(int);
   b = (b + 255) & ~size_t(255);
-  b += (size_t)nang * kW * kW * sizeof(cd);
+  b += (size_t)nang * kWMax * kWMax * sizeof(cd);
   b = (b + 255) & ~size_t(255);
-  b += (size_t)nang * n * kW * sizeof(cd);
+  b += (size_t)nang * n * kWMax * sizeof(cd);
   return b + 256;
 }
 
@@ -432,16 +433,17 @@ static GJScratch gj_carve(void* scratch, int nang, int n) {
   GJScratch s;
   char* p = reinterpret_cast<char*>(scratch);
   s.piv = reinterpret_cast<int*>(p);
-  size_t b = (size_t)nang * kW * sizeof(int);
+  size_t b = (size_t)nang * kWMax * sizeof(int);
   b = (b + 255) & ~size_t(255);
   s.W1 = reinterpret_cast<cd*>(p + b);
-  b += (size_t)nang * kW * kW * sizeof(cd);
+  b += (size_t)nang * kWMax * kWMax * sizeof(cd);
   b = (b + 255) & ~size_t(255);
   s.L2 = reinterpret_cast<cd*>(p + b);
   return s;
 }
 
 // Column-major complex access helper for the panel held in shared memory: S[i*kW + k].
+template <int kW>
 __global__ void k_gj_panel(const cd* __restrict__ Q, const int* __restrict__ flag, int n, int ld,
                            int c0, int w, GJScratch sc, unsigned* status) {
   const int a = blockIdx.x;
@@ -568,6 +570,7 @@ __global__ void k_gj_panel(const cd* __restrict__ Q, const int* __restrict__ fla
 // stay in registers; the multipliers L2 of 32 rows at a time are staged in shared
 // memory and read as broadcasts.
 constexpr int kUpdRows = 32;
+template <int kW>
 __global__ void __launch_bounds__(kUpdCols) k_gj_update(cd* __restrict__ Q, cd* __restrict__ P,
                                                         const int* __restrict__ flag, int n,
                                                         int ld, int c0, int w, GJScratch sc) {
@@ -643,22 +646,33 @@ __global__ void __launch_bounds__(kUpdCols) k_gj_update(cd* __restrict__ Q, cd* 
   }
 }
 
-void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld, void* scratch,
-                         unsigned* status, cudaStream_t st) {
-  GJScratch sc = gj_carve(scratch, nang, n);
-  size_t smem = (size_t)n * kW * sizeof(cd);
+template <int kW>
+static void gauss_jordan_panels(cd* Q, cd* P, const int* flag, int nang, int n, int ld,
+                                const GJScratch& sc, unsigned* status, cudaStream_t st) {
+  const size_t smem = (size_t)n * kW * sizeof(cd);
   static size_t attr = 0;
   if (smem > attr) {
-    cudaFuncSetAttribute(k_gj_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_gj_panel<kW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = smem;
   }
   for (int c0 = 0; c0 < n; c0 += kW) {
     int w = (n - c0 < kW) ? n - c0 : kW;
-    k_gj_panel<<<nang, 256, smem, st>>>(Q, flag, n, ld, c0, w, sc, status);
+    k_gj_panel<kW><<<nang, 256, smem, st>>>(Q, flag, n, ld, c0, w, sc, status);
     int total = (n - (c0 + w)) + n;
     dim3 grid(ceil_div(total, kUpdCols), nang);
-    k_gj_update<<<grid, kUpdCols, 0, st>>>(Q, P, flag, n, ld, c0, w, sc);
+    k_gj_update<kW><<<grid, kUpdCols, 0, st>>>(Q, P, flag, n, ld, c0, w, sc);
   }
+}
+
+void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld, void* scratch,
+                         unsigned* status, cudaStream_t st) {
+  GJScratch sc = gj_carve(scratch, nang, n);
+  // the panel kernel holds n x kW complex values plus three kW x kW blocks
+  const size_t need24 = (size_t)n * 24 * sizeof(cd) + 3 * 24 * 24 * sizeof(cd) + 1024;
+  if (need24 <= 227 * 1024)
+    gauss_jordan_panels<24>(Q, P, flag, nang, n, ld, sc, status, st);
+  else
+    gauss_jordan_panels<16>(Q, P, flag, nang, n, ld, sc, status, st);
 }
 
 // ============================================================ RK4 stage combination
