@@ -90,3 +90,29 @@ def test_batch_rejects_empty(ctx):
     from trhepd_opt_b200 import native, surface
     with pytest.raises(native.TrhepdError):
         surface.solve_batch(ctx, [], native.FP64)
+
+
+@pytest.mark.parametrize("precision", [0, 2], ids=["fp64", "int8"])
+def test_stacked_candidates_equal_individual(ctx, tmp_path, precision):
+    """Candidates of one base structure (same beams, slices, angle grid) are
+    integrated as one stacked solve, every row tile with its own stage matrix:
+    each must equal its own solve.  A structure with another angle grid is
+    solved on its own, a small one in the fused launch."""
+    from trhepd_opt_b200 import generator, native, surface
+    base = generator.dense(95, n_angles=5, region=2.0, seed=12)
+    structs = [generator.jitter(base, 0.1, k) for k in range(3)]
+    structs.append(generator.dense(95, n_angles=4, region=2.0, seed=13))
+    structs.append(generator.jitter(generator.small23(), 0.1, 5))
+    probs = [_resident(ctx, tmp_path / f"s{k}", s) for k, s in enumerate(structs)]
+    ref = []
+    for sp, rp in probs:
+        rp.solve(native.FP64 if rp.nb <= 64 else precision)
+        ref.append(rp.fetch()[1])
+    surface.solve_batch(ctx, [rp for _, rp in probs], precision)
+    for (sp, rp), r in zip(probs, ref):
+        _, got = rp.fetch()
+        assert np.isfinite(got).all()
+        assert spot_errors(got, r)[0] <= 1e-12, rp.nb
+    for sp, rp in probs:
+        rp.close()
+        sp.close()

@@ -35,6 +35,14 @@ struct TableEntry {  // per (stage column, Fourier component): u = v + vi, w = v
   cd u, w;
 };
 
+// Several problems stacked in one integration: problem b owns the rows_b stacked
+// rows from b * rows_b and its stage matrix at V + b * vstride.  rows_b = 0
+// (the default): one problem.
+struct StackedRows {
+  int rows_b = 0;
+  long long vstride = 0;
+};
+
 // K3: stage potential table T[c * nv + k] for the ncol depths in `depth`.
 void launch_potential_table(const PotInputs& in, const double* depth, int ncol, TableEntry* table,
                             cudaStream_t st);
@@ -51,14 +59,19 @@ void launch_structure_factor(const double* gh, const double* gk, int nv, const d
 // value at V[kpad * ld]; V must hold (kpad + 1) * ld elements.
 void launch_gather_stage(const TableEntry* table_col, const int* pair, int n, int kpad, int ld,
                          bool drop_diag, cd* V, cudaStream_t st);
+// The stage matrices of a stacked group (tables[b] + coloff for problem b).
+void launch_gather_stage_multi(const TableEntry* const* tables, size_t coloff, const int* pair,
+                               int n, int kpad, int ld, bool drop_diag, cd* V, long long vstride,
+                               int nprob, cudaStream_t st);
 
 // Elementwise stage with Q = I:  P += cb*(V + diag(D_a));  Q = I + ca*P.
 void launch_stage_identity(cd* Q, cd* P, const cd* V, const cd* D, int nang, int n, int ld,
-                           double cb, double ca, cudaStream_t st);
+                           double cb, double ca, cudaStream_t st, StackedRows sr = {});
 
 // K5 (FP64 DMMA): P += cb*(Q V + Q o D_a);  Qo = Q + ca*P   (all angles, one launch)
 void launch_stage_gemm_f64(const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D, int nang, int n,
-                           int ld, int kpad, double cb, double ca, cudaStream_t st);
+                           int ld, int kpad, double cb, double ca, cudaStream_t st,
+                           StackedRows sr = {});
 
 // Q := I for angles whose flag is set (flag == nullptr: all angles).
 void launch_set_identity(cd* Q, const int* flag, int nang, int n, int ld, cudaStream_t st);

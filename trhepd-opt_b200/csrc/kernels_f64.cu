@@ -158,6 +158,39 @@ __global__ void k_gather_stage(const TableEntry* __restrict__ tc, const int* __r
   if (drop_diag && k == 0 && j == 0) V[(size_t)kpad * ld] = -conj(tc[0].u);
 }
 
+// One stage matrix per problem of a stacked group: problem b gathers from its own
+// table (tables[b] + coloff) into V + b * vstride.
+__global__ void k_gather_stage_multi(const TableEntry* const* __restrict__ tables, size_t coloff,
+                                     const int* __restrict__ pair, int n, int kpad, int ld,
+                                     int drop_diag, cd* __restrict__ V, long long vstride) {
+  const int b = blockIdx.z;
+  const TableEntry* tc = tables[b] + coloff;
+  cd* Vb = V + (size_t)b * vstride;
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = blockIdx.y;
+  if (j >= ld || k >= kpad) return;
+  cd v = cd{0.0, 0.0};
+  if (k < n && j < n) {
+    if (k < j) {
+      v = -conj(tc[pair[k * n + j]].u);
+    } else if (k > j) {
+      v = -tc[pair[k * n + j]].w;
+    } else if (!drop_diag) {
+      v = -conj(tc[0].u);
+    }
+  }
+  Vb[(size_t)k * ld + j] = v;
+  if (drop_diag && k == 0 && j == 0) Vb[(size_t)kpad * ld] = -conj(tc[0].u);
+}
+
+void launch_gather_stage_multi(const TableEntry* const* tables, size_t coloff, const int* pair,
+                               int n, int kpad, int ld, bool drop_diag, cd* V, long long vstride,
+                               int nprob, cudaStream_t st) {
+  dim3 grid(ceil_div(ld, 128), kpad, nprob);
+  k_gather_stage_multi<<<grid, 128, 0, st>>>(tables, coloff, pair, n, kpad, ld, drop_diag ? 1 : 0,
+                                             V, vstride);
+}
+
 void launch_gather_stage(const TableEntry* table_col, const int* pair, int n, int kpad, int ld,
                          bool drop_diag, cd* V, cudaStream_t st) {
   dim3 grid(ceil_div(ld, 128), kpad);
@@ -167,12 +200,13 @@ void launch_gather_stage(const TableEntry* table_col, const int* pair, int n, in
 // ============================================================ identity-stage elementwise
 __global__ void k_stage_identity(cd* __restrict__ Q, cd* __restrict__ P, const cd* __restrict__ V,
                                  const cd* __restrict__ D, int nang, int n, int ld, double cb,
-                                 double ca) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int r = blockIdx.y;  // stacked row
+                                 double ca, StackedRows sr) {
+  int j = blockIdx.y * blockDim.x + threadIdx.x;
+  int r = blockIdx.x;  // stacked row
   if (j >= n) return;
   int a = r / n, i = r - a * n;
   size_t o = (size_t)r * ld + j;
+  if (sr.rows_b > 0) V += (size_t)(r / sr.rows_b) * sr.vstride;
   cd m = V[(size_t)i * ld + j];
   if (i == j) m = m + D[(size_t)a * ld + j];
   cd p = P[o] + cb * m;
@@ -183,9 +217,9 @@ __global__ void k_stage_identity(cd* __restrict__ Q, cd* __restrict__ P, const c
 }
 
 void launch_stage_identity(cd* Q, cd* P, const cd* V, const cd* D, int nang, int n, int ld,
-                           double cb, double ca, cudaStream_t st) {
-  dim3 grid(ceil_div(n, 128), nang * n);
-  k_stage_identity<<<grid, 128, 0, st>>>(Q, P, V, D, nang, n, ld, cb, ca);
+                           double cb, double ca, cudaStream_t st, StackedRows sr) {
+  dim3 grid(nang * n, ceil_div(n, 128));  // rows on x: more than 65535 stacked rows
+  k_stage_identity<<<grid, 128, 0, st>>>(Q, P, V, D, nang, n, ld, cb, ca, sr);
 }
 
 // ============================================================ K5 FP64 DMMA stage GEMM
@@ -223,7 +257,7 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double& c2, double&
 __global__ void __launch_bounds__(128, 2)
     k_stage_gemm_f64(const cd* __restrict__ Q, cd* __restrict__ P, cd* __restrict__ Qo,
                      const cd* __restrict__ V, const cd* __restrict__ D, int rows, int n, int ld,
-                     int kpad, double cb, double ca) {
+                     int kpad, double cb, double ca, StackedRows sr) {
   using namespace f64gemm;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd* As = reinterpret_cast<cd*>(smem_raw);
@@ -231,7 +265,12 @@ __global__ void __launch_bounds__(128, 2)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const int bm = blockIdx.y * BM, bn = blockIdx.x * BN;
+  // row tile -> problem: tiles of one problem never take rows of the next
+  const int tpp = ceil_div(sr.rows_b, BM);
+  const int pb = blockIdx.y / tpp;
+  const int bm = pb * sr.rows_b + (blockIdx.y - pb * tpp) * BM, bn = blockIdx.x * BN;
+  rows = min(rows, (pb + 1) * sr.rows_b);
+  V += (size_t)pb * sr.vstride;
 
   auto load_stage = [&](int s, int k0) {
     cd* a = As + s * A_TILE;
@@ -326,7 +365,8 @@ __global__ void __launch_bounds__(128, 2)
 }
 
 void launch_stage_gemm_f64(const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D, int nang, int n,
-                           int ld, int kpad, double cb, double ca, cudaStream_t st) {
+                           int ld, int kpad, double cb, double ca, cudaStream_t st,
+                           StackedRows sr) {
   using namespace f64gemm;
   static bool attr = false;
   if (!attr) {
@@ -334,14 +374,16 @@ void launch_stage_gemm_f64(const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
     attr = true;
   }
   int rows = nang * n;
-  dim3 grid(ceil_div(n, BN), ceil_div(rows, BM));
-  k_stage_gemm_f64<<<grid, 128, SMEM, st>>>(Q, P, Qo, V, D, rows, n, ld, kpad, cb, ca);
+  if (sr.rows_b <= 0) sr = StackedRows{rows, 0};
+  const int nprob = ceil_div(rows, sr.rows_b);
+  dim3 grid(ceil_div(n, BN), nprob * ceil_div(sr.rows_b, BM));
+  k_stage_gemm_f64<<<grid, 128, SMEM, st>>>(Q, P, Qo, V, D, rows, n, ld, kpad, cb, ca, sr);
 }
 
 // ============================================================ identity / flags
 __global__ void k_set_identity(cd* __restrict__ Q, const int* __restrict__ flag, int n, int ld) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int r = blockIdx.y;
+  int j = blockIdx.y * blockDim.x + threadIdx.x;
+  int r = blockIdx.x;
   int a = r / n, i = r - a * n;
   if (j >= n) return;
   if (flag && !flag[a]) return;
@@ -349,7 +391,7 @@ __global__ void k_set_identity(cd* __restrict__ Q, const int* __restrict__ flag,
 }
 
 void launch_set_identity(cd* Q, const int* flag, int nang, int n, int ld, cudaStream_t st) {
-  dim3 grid(ceil_div(n, 128), nang * n);
+  dim3 grid(nang * n, ceil_div(n, 128));  // rows on x: more than 65535 stacked rows
   k_set_identity<<<grid, 128, 0, st>>>(Q, flag, n, ld);
 }
 
@@ -685,8 +727,8 @@ __global__ void k_rk4_combine(cd* __restrict__ Q, cd* __restrict__ P, cd* __rest
                               cd* __restrict__ Pt, cd* __restrict__ KP, cd* __restrict__ SQ,
                               cd* __restrict__ SP, int j, double w, double step, double h6, int n,
                               int ld) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r = blockIdx.y;
+  const int c = blockIdx.y * blockDim.x + threadIdx.x;
+  const int r = blockIdx.x;
   if (c >= n) return;
   const size_t o = (size_t)r * ld + c;
   const cd kq = (j == 0) ? P[o] : Pt[o];
@@ -713,15 +755,15 @@ __global__ void k_rk4_combine(cd* __restrict__ Q, cd* __restrict__ P, cd* __rest
 
 void launch_rk4_combine(cd* Q, cd* P, cd* Qt, cd* Pt, cd* KP, cd* SQ, cd* SP, int j, double w,
                         double step, double h6, int nang, int n, int ld, cudaStream_t st) {
-  dim3 grid(ceil_div(n, 128), nang * n);
+  dim3 grid(nang * n, ceil_div(n, 128));  // rows on x: more than 65535 stacked rows
   k_rk4_combine<<<grid, 128, 0, st>>>(Q, P, Qt, Pt, KP, SQ, SP, j, w, step, h6, n, ld);
 }
 
 // ============================================================ boundary transforms
 __global__ void k_invstransh_build(const cd* __restrict__ F, cd* __restrict__ Q,
                                    cd* __restrict__ P, int n, int ld) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int r = blockIdx.y;
+  int j = blockIdx.y * blockDim.x + threadIdx.x;
+  int r = blockIdx.x;
   if (j >= n) return;
   int a = r / n, i = r - a * n;
   cd fh = conj(F[((size_t)a * n + j) * n + i]);  // F^H(i,j) = conj(F(j,i))
@@ -736,14 +778,14 @@ __global__ void k_invstransh_build(const cd* __restrict__ F, cd* __restrict__ Q,
 }
 
 void launch_invstransh_build(const cd* F, cd* Q, cd* P, int nang, int n, int ld, cudaStream_t st) {
-  dim3 grid(ceil_div(n, 128), nang * n);
+  dim3 grid(nang * n, ceil_div(n, 128));  // rows on x: more than 65535 stacked rows
   k_invstransh_build<<<grid, 128, 0, st>>>(F, Q, P, n, ld);
 }
 
 __global__ void k_invstransh_finish(cd* __restrict__ P, const cd* __restrict__ gam, int n,
                                     int ld) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int r = blockIdx.y;
+  int j = blockIdx.y * blockDim.x + threadIdx.x;
+  int r = blockIdx.x;
   if (j >= n) return;
   int a = r / n, i = r - a * n;
   size_t o = (size_t)r * ld + j;
@@ -751,14 +793,14 @@ __global__ void k_invstransh_finish(cd* __restrict__ P, const cd* __restrict__ g
 }
 
 void launch_invstransh_finish(cd* P, const cd* gam, int nang, int n, int ld, cudaStream_t st) {
-  dim3 grid(ceil_div(n, 128), nang * n);
+  dim3 grid(nang * n, ceil_div(n, 128));  // rows on x: more than 65535 stacked rows
   k_invstransh_finish<<<grid, 128, 0, st>>>(P, gam, n, ld);
 }
 
 __global__ void k_stransh_build(cd* __restrict__ Q, cd* __restrict__ P, const cd* __restrict__ gam,
                                 int n, int ld) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  int r = blockIdx.y;
+  int j = blockIdx.y * blockDim.x + threadIdx.x;
+  int r = blockIdx.x;
   if (j >= n) return;
   int a = r / n, i = r - a * n;
   size_t o = (size_t)r * ld + j;
@@ -774,7 +816,7 @@ __global__ void k_stransh_build(cd* __restrict__ Q, cd* __restrict__ P, const cd
 }
 
 void launch_stransh_build(cd* Q, cd* P, const cd* gam, int nang, int n, int ld, cudaStream_t st) {
-  dim3 grid(ceil_div(n, 128), nang * n);
+  dim3 grid(nang * n, ceil_div(n, 128));  // rows on x: more than 65535 stacked rows
   k_stransh_build<<<grid, 128, 0, st>>>(Q, P, gam, n, ld);
 }
 

@@ -297,6 +297,9 @@ struct RunState {
   int gj_per = 0;
   bool capturing = false;    // launches go into a CUDA graph: no events on the stream
   long prof_entries = 0;     // event quadruples recorded in profile mode
+  int nprob = 1;             // stacked problems (see trhepd_problem::nprob)
+  const TableEntry* const* tables = nullptr;
+  StackedRows sr{};          // rows and stage-matrix stride per stacked problem
 };
 
 // The device buffers one integration works in: the context's (one solve at a
@@ -320,6 +323,11 @@ struct OwnWorkspace {
 struct trhepd_problem {
   int n = 0, ns = 0, nv = 0, nang = 0, ld = 0, nb0 = 0, int_method = 5;
   int nrep2 = 1;               // angles of the inner scan (rows per block of the output)
+  // a stacked group (problems of one batch solved as one integration): nprob
+  // problems of nang / nprob angles each, their stage tables in `tables` (device)
+  int nprob = 1;
+  const TableEntry* const* tables = nullptr;
+  std::vector<int> pair_host;  // the beam-pair map, to recognise problems that stack
   Integrator I{};
   double dz = 0, kappa_max = 0;
   int ncol = 0;
@@ -378,15 +386,14 @@ void prepare(trhepd_context* C, const SolveArgs& A, trhepd_problem& Pb) {
       pair[(size_t)k * n + j] = e - 1;
     }
   upload(Pb.pair, pair, st);
+  Pb.pair_host = pair;
 
   // angle schedule (surflf.f90:43-92)
   const bool ng_outer = A.ng > A.naz;
   const int nrep1 = ng_outer ? A.naz : A.ng, nrep2 = ng_outer ? A.ng : A.naz;
   const int nang = nrep1 * nrep2;
   const int ld = round_up(n, 16);
-  // row-parallel kernels index the nang*n stacked rows with the grid's y dimension
-  if ((long long)nang * n > 65535)
-    throw std::invalid_argument("angles x beams exceeds 65535 stacked rows; split the scan");
+
   Pb.nang = nang;
   Pb.nrep2 = nrep2;
   Pb.ld = ld;
@@ -480,7 +487,10 @@ void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_m
   R.Q = (cd*)W.Q0->ensure(R.sbytes);
   R.Qn = (cd*)W.Q1->ensure(R.sbytes);
   R.P = (cd*)W.P->ensure(R.sbytes);
-  R.V = (cd*)W.V->ensure((size_t)(R.kpad + 1) * ld * sizeof(cd));
+  R.nprob = Pb.nprob;
+  R.tables = Pb.tables;
+  if (R.nprob > 1) R.sr = StackedRows{(nang / R.nprob) * n, (long long)(R.kpad + 1) * ld};
+  R.V = (cd*)W.V->ensure((size_t)R.nprob * (R.kpad + 1) * ld * sizeof(cd));
   R.flags = (int*)W.flags->ensure(std::max(nang, 4) * sizeof(int));
   R.dval = (double*)W.dval->ensure(std::max(nang, 4) * sizeof(double));
   R.gjs = W.gj->ensure(gj_scratch_bytes(nang, n));
@@ -490,8 +500,9 @@ void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_m
   if (precision == TRHEPD_SPLIT_INT8 && C->split_slices > 4)
     throw std::invalid_argument("the INT8 split form takes 3 or 4 slices");
   if (R.split)
-    R.sw = split_workspace_carve(W.split->ensure(split_workspace_bytes(nang, n, C->split_slices)),
-                                 nang, n, C->split_slices, R.status, st);
+    R.sw = split_workspace_carve(
+        W.split->ensure(split_workspace_bytes(nang, n, C->split_slices, R.nprob)), nang, n,
+        C->split_slices, R.status, st, R.nprob);
   R.gj_per = 2 * ceil_div(n, 16);
   if (C->profile && (int)C->evpool.size() < 4 * nprod_max) {
     while ((int)C->evpool.size() < 4 * nprod_max) {
@@ -519,8 +530,12 @@ void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_m
 
 // Gather the stage matrix of table column `col` into R.V.
 void gather(RunState& R, int col, bool drop_diag) {
-  launch_gather_stage(R.table + (size_t)col * R.nv, R.pair, R.n, R.kpad, R.ld, drop_diag, R.V,
-                      R.st);
+  if (R.nprob > 1)
+    launch_gather_stage_multi(R.tables, (size_t)col * R.nv, R.pair, R.n, R.kpad, R.ld, drop_diag,
+                              R.V, R.sr.vstride, R.nprob, R.st);
+  else
+    launch_gather_stage(R.table + (size_t)col * R.nv, R.pair, R.n, R.kpad, R.ld, drop_diag, R.V,
+                        R.st);
   R.launches += 1;
 }
 
@@ -531,10 +546,10 @@ void stage_product(trhepd_context* C, RunState& R, const cd* Q, cd* P, cd* Qo, d
   if (ev) CK(cudaEventRecord(ev[0], R.st));
   if (R.split) {
     R.launches += split_stage(R.sw, Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, cb, ca,
-                              C->split_slices, R.split_variant, ev ? ev + 1 : nullptr, R.st);
+                              C->split_slices, R.split_variant, ev ? ev + 1 : nullptr, R.st, R.sr);
   } else {
     if (ev) CK(cudaEventRecord(ev[1], R.st));
-    launch_stage_gemm_f64(Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, R.kpad, cb, ca, R.st);
+    launch_stage_gemm_f64(Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, R.kpad, cb, ca, R.st, R.sr);
     if (ev) CK(cudaEventRecord(ev[2], R.st));
     R.launches += 1;
   }
@@ -635,7 +650,7 @@ void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) 
   const double dz = Pb.dz;
   begin_run(C, Pb, precision, I.s * Pb.ns, R, context_workspace(C));
   const bool every_slice = (Pb.n == 1 && Pb.int_method == 6);  // hp_int_spa1d renormalises each slice
-  if (!R.split && Pb.n >= 2 && Pb.n <= std::min(C->fused_max_n, kFusedMaxBeams)) {
+  if (!R.split && R.nprob == 1 && Pb.n >= 2 && Pb.n <= std::min(C->fused_max_n, kFusedMaxBeams)) {
     // whole integration in one launch, state in shared memory (small.cu)
     static thread_local FusedLaunch L;  // 17 KB of kernel parameters
     L.nprob = 1;
@@ -666,7 +681,8 @@ void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) 
       const double ca = I.bab[2 * k - 1] * dz;
       if (l == 1 && k == 1) {  // Q = I: elementwise stage
         gather(R, col, false);
-        launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, I.bab[0] * dz, ca, R.st);
+        launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, I.bab[0] * dz, ca, R.st,
+                              R.sr);
         R.launches += 1;
         continue;
       }
@@ -683,7 +699,7 @@ void run_rkn(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) 
   }
   // final half kick with Q = I: P += b1 dz M(end)
   gather(R, I.s * R.ns, false);
-  launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, I.bab[0] * dz, 0.0, R.st);
+  launch_stage_identity(R.Q, R.P, R.V, R.D, R.nang, R.n, R.ld, I.bab[0] * dz, 0.0, R.st, R.sr);
   R.launches += 1;
   finish_device(C, Pb, R);
 }
@@ -758,6 +774,9 @@ void bgemm(const cd* A, long long sA, const cd* B, long long sB, cd* Cm, long lo
 void run_magnus(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) {
   if (precision != TRHEPD_FP64)
     throw std::invalid_argument("the Magnus integrators (int_method 1-3) run in plain FP64 only");
+  // the Magnus element kernels index the stacked rows with the grid's y dimension
+  if ((long long)Pb.nang * Pb.n > 65535)
+    throw std::invalid_argument("Magnus: angles x beams exceeds 65535 stacked rows; split the scan");
   const double dz = Pb.dz;
   const Family fam = Pb.I.family;
   begin_run(C, Pb, precision, 0, R, context_workspace(C));
@@ -921,6 +940,74 @@ void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
   finish_host(C, Pb, R);
 }
 
+// Problems that can be integrated as one stacked solve: same beams and beam-pair
+// map, slice count and thickness, integrator and angle count (the candidates of
+// one base structure).  Their angles are stacked row-wise; each row tile of the
+// stage product reads its own problem's stage matrix.
+bool stackable(const trhepd_problem& a, const trhepd_problem& b) {
+  return a.n == b.n && a.ns == b.ns && a.dz == b.dz && a.int_method == b.int_method &&
+         a.nang == b.nang && a.nv == b.nv && a.ncol == b.ncol && a.nb0 == b.nb0 &&
+         a.pair_host == b.pair_host;
+}
+
+// One integration of a stacked group; the intensities go back to each problem.
+void solve_stacked(trhepd_context* C, const std::vector<trhepd_problem*>& g, int precision,
+                   double* stats) {
+  cudaStream_t st = C->stream;
+  const trhepd_problem& p0 = *g[0];
+  const int k = (int)g.size(), n = p0.n, ld = p0.ld, na = p0.nang;
+  trhepd_problem M;
+  M.n = n;
+  M.ns = p0.ns;
+  M.nv = p0.nv;
+  M.ld = ld;
+  M.nb0 = p0.nb0;
+  M.int_method = p0.int_method;
+  M.I = p0.I;
+  M.dz = p0.dz;
+  M.ncol = p0.ncol;
+  M.nrep2 = p0.nrep2;
+  M.nang = k * na;
+  M.nprob = k;
+  for (const trhepd_problem* p : g) M.kappa_max = std::max(M.kappa_max, p->kappa_max);
+  M.pair.p = p0.pair.p;    // borrowed (shared beam-pair map)
+  M.table.p = p0.table.p;  // borrowed (the tables array holds every problem's)
+  DevBuf tabs;
+  auto unborrow = [&]() {
+    M.pair.p = nullptr;
+    M.table.p = nullptr;
+    M.release();
+    tabs.release();
+  };
+  try {
+    std::vector<const TableEntry*> tp(k);
+    for (int q = 0; q < k; ++q) tp[q] = g[q]->table.as<TableEntry>();
+    M.tables = upload(tabs, tp, st);
+    auto stack = [&](DevBuf& dst, DevBuf trhepd_problem::*src, size_t per) {
+      char* d = (char*)dst.ensure(per * k);
+      for (int q = 0; q < k; ++q)
+        CK(cudaMemcpyAsync(d + per * q, (g[q]->*src).p, per, cudaMemcpyDeviceToDevice, st));
+    };
+    stack(M.gam, &trhepd_problem::gam, (size_t)na * n * sizeof(cd));
+    stack(M.D, &trhepd_problem::D, (size_t)na * ld * sizeof(cd));
+    stack(M.F, &trhepd_problem::F, (size_t)na * n * n * sizeof(cd));
+    stack(M.wnsga2, &trhepd_problem::wnsga2, (size_t)na * sizeof(double));
+    M.f2.ensure((size_t)M.nang * n * sizeof(double));
+    RunState R;
+    run_device(C, M, precision, R);
+    finish_host(C, M, R);
+    for (int q = 0; q < k; ++q)
+      CK(cudaMemcpyAsync(g[q]->f2.p, M.f2.as<double>() + (size_t)q * na * n,
+                         (size_t)na * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    for (int q = 0; q < 8; ++q) stats[q] = C->stats[q];
+  } catch (...) {
+    unborrow();
+    throw;
+  }
+  unborrow();
+}
+
 // Problems solved together (no counterpart in the reference, whose driver solves
 // one structure at a time).  Problems the fused kernel takes (RKN, 2 <= n <= the
 // fused limit) are integrated by shared launches, each in its own buffers: one
@@ -985,11 +1072,31 @@ void batch_solve(trhepd_context* C, trhepd_problem* const* probs, int count, int
       if (hs[4 * q] & (kStatusNonFinite | kStatusZeroPivot))
         throw CudaError("non-finite value or zero pivot in a batch solve", TRHEPD_ENONFINITE);
     }
-    for (trhepd_problem* p : rest) {
-      run(C, *p, precision);
-      products += (long)C->stats[1];
-      renorms += (long)C->stats[0];
-      launches += (long)C->stats[5];
+    // stack the rest into groups (RKN, FP64 or INT8), solve groups of two or more
+    // as one integration and the others one by one
+    std::vector<bool> done(rest.size(), false);
+    const bool stack_ok = precision == TRHEPD_FP64 || precision == TRHEPD_SPLIT_INT8;
+    for (size_t q = 0; q < rest.size(); ++q) {
+      if (done[q]) continue;
+      std::vector<trhepd_problem*> grp = {rest[q]};
+      done[q] = true;
+      if (stack_ok && rest[q]->I.family == kRkn && rest[q]->n >= 2)
+        for (size_t r = q + 1; r < rest.size(); ++r)
+          if (!done[r] && stackable(*rest[q], *rest[r]) &&
+              (long long)(grp.size() + 1) * rest[q]->nang * rest[q]->n <= (1 << 22)) {
+            grp.push_back(rest[r]);
+            done[r] = true;
+          }
+      double st8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (grp.size() > 1) {
+        solve_stacked(C, grp, precision, st8);
+      } else {
+        run(C, *grp[0], precision);
+        for (int k = 0; k < 8; ++k) st8[k] = C->stats[k];
+      }
+      products += (long)st8[1];
+      renorms += (long)st8[0];
+      launches += (long)st8[5];
     }
     CK(cudaEventRecord(e1, st));
     CK(cudaEventSynchronize(e1));

@@ -167,6 +167,11 @@ struct EpiArgs {
   unsigned* status;
   int rows, n, ld, kpad, S;
   double cb, ca;
+  // stacked problems (INT8 kernel): problem b owns rows [b rows_b, (b+1) rows_b),
+  // its stage matrix at V + b vstride and its column exponents at fcol + b fstride;
+  // tpp row tiles per problem
+  int rows_b = 0, fstride = 0, tpp = 0;
+  long long vstride = 0;
 };
 
 // ------------------------------------------------------------ slicing kernels
@@ -819,9 +824,13 @@ __global__ void k_slice_rows_i8(const cd* __restrict__ Q, int rows, int n, int l
 template <int S>
 __global__ void __launch_bounds__(128) k_slice_cols_i8(const cd* __restrict__ V, int n, int ld,
                                                         int kc, int nrows, int* __restrict__ fcol,
-                                                        uint16_t* __restrict__ B) {
+                                                        uint16_t* __restrict__ B,
+                                                        long long vstride, int fstride) {
   __shared__ double red[4];
   const int j = blockIdx.x, tid = threadIdx.x;
+  V += (size_t)blockIdx.y * vstride;  // problem blockIdx.y of a stacked group
+  fcol += (size_t)blockIdx.y * fstride;
+  B += (size_t)blockIdx.y * S * nrows * kc;
   double m = 0.0;
   for (int k = tid; k < n; k += 128) {
     const cd v = V[(size_t)k * ld + j];
@@ -901,7 +910,8 @@ __global__ void __launch_bounds__(P_THREADS, 1)
         int g = 0;
         bool stop = false;
         for (int tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x) {
-          const int m0 = (tile / tiles_n) * BM, n0 = (tile % tiles_n) * NT;
+          const int rt = tile / tiles_n, pb = rt / ep.tpp;
+          const int m0 = pb * ep.rows_b + (rt - pb * ep.tpp) * BM, n0 = (tile % tiles_n) * NT;
           for (int kb = 0; kb < nkb; ++kb, ++g) {
             const int st = g % STAGES, round = g / STAGES;
             if (round > 0 && !mbar_wait(&empty_bar[st], (round - 1) & 1)) {
@@ -920,7 +930,8 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 #pragma unroll
             for (int s = 0; s < S; ++s) {
               tma_load_3d(&tmA, &full_bar[st], sa + s * i8::A_SLICE_BYTES, kb * i8::BK, m0, s);
-              tma_load_3d(&tmB, &full_bar[st], sb + s * i8::B_SLICE_BYTES, kb * i8::BK, n0, s);
+              tma_load_3d(&tmB, &full_bar[st], sb + s * i8::B_SLICE_BYTES, kb * i8::BK, n0,
+                          pb * S + s);
             }
           }
         }
@@ -983,11 +994,15 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     const int q4 = warp & 3;
     const int half = (warp - 4) >> 2;
     const int t0 = lane & 3, t1 = lane >> 2;
-    const cd vd = ep.V[(size_t)ep.kpad * ep.ld];
     int it = 0;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
-      const int m0 = (tile / tiles_n) * BM + q4 * 32;
+      const int rt = tile / tiles_n, pb = rt / ep.tpp;
+      const int m0 = pb * ep.rows_b + (rt - pb * ep.tpp) * BM + q4 * 32;
+      const int rend = min(ep.rows, (pb + 1) * ep.rows_b);  // this problem's rows end here
       const int jh = (tile % tiles_n) * NC + half * (NC / 2);
+      const cd* Vb = ep.V + (size_t)pb * ep.vstride;
+      const int* fcb = ep.fcol + (size_t)pb * ep.fstride;
+      const cd vd = Vb[(size_t)ep.kpad * ep.ld];
       int er[2][2], ra[2][2], ri[2][2];
 #pragma unroll
       for (int h = 0; h < 2; ++h)
@@ -997,7 +1012,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
           er[h][u] = 0;
           ra[h][u] = 0;
           ri[h][u] = 0;
-          if (r < ep.rows) {
+          if (r < rend) {
             er[h][u] = ep.erow[r];
             ra[h][u] = r / ep.n;
             ri[h][u] = r - ra[h][u] * ep.n;
@@ -1007,7 +1022,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 #pragma unroll
       for (int g = 0; g < 8; ++g) {
         const int j = jh + 4 * g + t0;
-        fc[g] = (j < ep.n) ? ep.fcol[j] : 0;
+        fc[g] = (j < ep.n) ? fcb[j] : 0;
       }
       const bool ok = mbar_wait(&tfull, it & 1);
       if (epi_any(!ok)) {
@@ -1048,7 +1063,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
           const int r = m0 + 16 * h + 8 * u + t1;
-          qd[h][u] = (r < ep.rows) ? ep.Q[(size_t)r * ep.ld + ri[h][u]] : cd{0.0, 0.0};
+          qd[h][u] = (r < rend) ? ep.Q[(size_t)r * ep.ld + ri[h][u]] : cd{0.0, 0.0};
         }
 #pragma unroll
       for (int g = 0; g < 8; ++g) {
@@ -1059,18 +1074,18 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
             const int r = m0 + 16 * h + 8 * u + t1;
-            if (r < ep.rows && j < ep.n) {
+            if (r < rend && j < ep.n) {
               const size_t ro = (size_t)r * ep.ld;
               qv[u] = ep.Q[ro + j];
               pv[u] = ep.P[ro + j];
-              vv[u] = ep.V[(size_t)ri[h][u] * ep.ld + j];
+              vv[u] = Vb[(size_t)ri[h][u] * ep.ld + j];
               dv[u] = ep.D[(size_t)ra[h][u] * ep.ld + j];
             }
           }
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
             const int r = m0 + 16 * h + 8 * u + t1;
-            if (r < ep.rows && j < ep.n) {
+            if (r < rend && j < ep.n) {
               const size_t ro = (size_t)r * ep.ld;
               const cd acc = vals[g][h][u] + qd[h][u] * vv[u] + qv[u] * (dv[u] + vd);
               const cd p = pv[u] + ep.cb * acc;
@@ -1112,8 +1127,9 @@ struct Carve {
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 // Workspace layout: A slices, B^T slices (`cbytes` bytes per complex entry: 4 for
-// BF16 pairs, 2 for INT8 pairs), row and column exponents.
-Carve carve(void* base, int nang, int n, int S, int cbytes = 4) {
+// BF16 pairs, 2 for INT8 pairs; one set per problem of a stacked group), row and
+// column exponents.
+Carve carve(void* base, int nang, int n, int S, int cbytes = 4, int nprob = 1) {
   Carve c;
   c.rows = nang * n;
   c.kc = round_up(n, 16);                 // complex k (= ld of the state)
@@ -1124,7 +1140,7 @@ Carve carve(void* base, int nang, int n, int S, int cbytes = 4) {
   c.A = reinterpret_cast<__nv_bfloat162*>(p + o);
   o = align256(o + (size_t)S * c.rows * c.kc * cbytes);
   c.B = reinterpret_cast<__nv_bfloat162*>(p + o);
-  o = align256(o + (size_t)S * c.nrows * c.kc * cbytes);
+  o = align256(o + (size_t)nprob * S * c.nrows * c.kc * cbytes);
   c.erow = reinterpret_cast<int*>(p + o);
   o = align256(o + (size_t)c.rows * sizeof(int));
   c.fcol = reinterpret_cast<int*>(p + o);
@@ -1232,17 +1248,26 @@ void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V,
 template <int S>
 void run_split_i8(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
                   int nang, int n, int ld, double cb, double ca, const cudaEvent_t* ev,
-                  cudaStream_t st) {
-  Carve c = carve(w.base, nang, n, S, 2);
+                  StackedRows sr, cudaStream_t st) {
+  const int rows = nang * n;
+  if (sr.rows_b <= 0) sr = StackedRows{rows, 0};
+  const int nprob = ceil_div(rows, sr.rows_b);
+  Carve c = carve(w.base, nang, n, S, 2, nprob);
   const int kr = 2 * c.kc;
   uint16_t* B = reinterpret_cast<uint16_t*>(c.B);
   uint32_t* A = reinterpret_cast<uint32_t*>(c.A);
-  split::k_slice_cols_i8<S><<<n, 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, B);
+  split::k_slice_cols_i8<S><<<dim3(n, nprob), 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, B,
+                                                            sr.vstride, c.npad);
   split::k_slice_rows_i8<S><<<ceil_div(c.rows, 8), 256, 0, st>>>(Q, c.rows, n, ld, kr, A, c.erow);
   CUtensorMap ta = make_map(c.A, kr, c.rows, S, 1);
-  CUtensorMap tb = make_map(c.B, kr, c.nrows, S, 1);
+  CUtensorMap tb = make_map(c.B, kr, c.nrows, S * nprob, 1);
   split::EpiArgs ep{Q, P, Qo, V, D, c.erow, c.fcol, w.status, c.rows, n, ld, c.kc, S, cb, ca};
-  const int tiles_n = c.nrows / split::NT, tiles_m = ceil_div(c.rows, split::BM);
+  const int tpp = ceil_div(sr.rows_b, split::BM);
+  ep.rows_b = sr.rows_b;
+  ep.vstride = sr.vstride;
+  ep.fstride = c.npad;
+  ep.tpp = tpp;
+  const int tiles_n = c.nrows / split::NT, tiles_m = nprob * tpp;
   const size_t smem = split::i8::smem_bytes(S);
   static bool attr[6] = {false, false, false, false, false, false};
   if (!attr[S]) {
@@ -1266,13 +1291,13 @@ void run_split_i8(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd*
 
 }  // namespace
 
-size_t split_workspace_bytes(int nang, int n, int slices) {
-  Carve c = carve(nullptr, nang, n, slices);
-  return reinterpret_cast<size_t>(c.fcol) + align256((size_t)c.npad * sizeof(int)) + 256;
+size_t split_workspace_bytes(int nang, int n, int slices, int nprob) {
+  Carve c = carve(nullptr, nang, n, slices, 4, nprob);
+  return reinterpret_cast<size_t>(c.fcol) + align256((size_t)nprob * c.npad * sizeof(int)) + 256;
 }
 
 SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, unsigned* status,
-                                     cudaStream_t st) {
+                                     cudaStream_t st, int nprob) {
   SplitWorkspace w;
   w.base = base;
   w.nang = nang;
@@ -1280,20 +1305,20 @@ SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, un
   w.slices = slices;
   w.status = status;
   // padded rows of the slice buffers are never written by the slicing kernels
-  cudaMemsetAsync(base, 0, split_workspace_bytes(nang, n, slices), st);
+  cudaMemsetAsync(base, 0, split_workspace_bytes(nang, n, slices, nprob), st);
   return w;
 }
 
 int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
                 int nang, int n, int ld, double cb, double ca, int slices, int variant,
-                const cudaEvent_t* ev, cudaStream_t st) {
+                const cudaEvent_t* ev, cudaStream_t st, StackedRows sr) {
   if (variant == kSplitInt8) {
     switch (slices) {
       case 3:
-        run_split_i8<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, st);
+        run_split_i8<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, sr, st);
         break;
       case 4:
-        run_split_i8<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, st);
+        run_split_i8<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, sr, st);
         break;
       default:
         throw std::invalid_argument("INT8 split slices must be 3 or 4");
@@ -1302,6 +1327,8 @@ int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V
   }
   if (variant != kSplitPersistent && variant != kSplitPerTile)
     throw std::invalid_argument("unknown split kernel variant");
+  if (sr.rows_b > 0 && sr.rows_b < nang * n)
+    throw std::invalid_argument("stacked problems run the INT8 or FP64 form only");
   switch (slices) {
     case 3:
       run_split<3>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, variant, ev, st);

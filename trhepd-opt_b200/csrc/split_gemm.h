@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "kernels.h"
 
 namespace trhepd {
 
@@ -12,10 +13,10 @@ struct SplitWorkspace {
   unsigned* status = nullptr;  // device status word (kStatus* bits)
 };
 
-size_t split_workspace_bytes(int nang, int n, int slices);
+size_t split_workspace_bytes(int nang, int n, int slices, int nprob = 1);
 // Carve the workspace and zero it on `st` (padded slice rows stay zero).
 SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, unsigned* status,
-                                     cudaStream_t st);
+                                     cudaStream_t st, int nprob = 1);
 
 // Tensor-core kernel forms of the stage product.
 //   kSplitPersistent: one CTA per SM over all tiles; the accumulators of a tile
@@ -31,6 +32,6 @@ enum SplitVariant { kSplitPersistent = 0, kSplitPerTile = 1, kSplitInt8 = 2 };
 // tensor-core kernel.  Returns the number of kernels launched.
 int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
                 int nang, int n, int ld, double cb, double ca, int slices, int variant,
-                const cudaEvent_t* ev, cudaStream_t st);
+                const cudaEvent_t* ev, cudaStream_t st, StackedRows sr = {});
 
 }  // namespace trhepd
