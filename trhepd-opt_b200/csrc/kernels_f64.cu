@@ -446,14 +446,15 @@ void launch_cond_est(const cd* Q, int nang, int n, int ld, int force, int* flag,
 
 // ============================================================ K8 blocked Gauss-Jordan
 // [Q | P] -> [I | Q^{-1} P] with partial pivoting (pivot = max |re|+|im| among the
-// rows not yet used, lowest index on ties, as zgetrf's izamax).  Panels of kW
-// columns (24 where the n x 24 panel fits shared memory, else 16; fewer panels
-// mean fewer passes over the trailing matrix): the panel kernel factors rows c0.. of the panel (LU with row swaps) and
+// rows not yet used, lowest index on ties, as zgetrf's izamax).  Panels of kW = 16
+// columns (24-column panels, which fit shared memory up to n = 530, measured
+// slower at n = 521: the panel kernel's serial column steps outweigh the saved
+// passes over the trailing matrix): the panel kernel factors rows c0.. of the panel (LU with row swaps) and
 // forms W1 = B1^{-1} and the elimination multipliers L2 = B2 B1^{-1} for every
 // other row; the update kernel applies the swaps and
 //   C1 <- W1 C1,   C2 <- C2 - L2 C1
 // to all remaining columns (Q columns right of the panel and every P column).
-constexpr int kWMax = 24;      // widest panel; the scratch is sized for it
+constexpr int kWMax = 16;      // panel width the scratch is sized for
 constexpr int kUpdCols = 128;  // trailing columns per update block
 
 struct GJScratch {
@@ -709,12 +710,7 @@ static void gauss_jordan_panels(cd* Q, cd* P, const int* flag, int nang, int n, 
 void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld, void* scratch,
                          unsigned* status, cudaStream_t st) {
   GJScratch sc = gj_carve(scratch, nang, n);
-  // the panel kernel holds n x kW complex values plus three kW x kW blocks
-  const size_t need24 = (size_t)n * 24 * sizeof(cd) + 3 * 24 * 24 * sizeof(cd) + 1024;
-  if (need24 <= 227 * 1024)
-    gauss_jordan_panels<24>(Q, P, flag, nang, n, ld, sc, status, st);
-  else
-    gauss_jordan_panels<16>(Q, P, flag, nang, n, ld, sc, status, st);
+  gauss_jordan_panels<kWMax>(Q, P, flag, nang, n, ld, sc, status, st);
 }
 
 // ============================================================ RK4 stage combination
