@@ -472,6 +472,13 @@ def main():
             "note": "ops per launch = slice pairs x 8*nangles*N^3 (complex N^3 as a real "
                     "(nangles*N) x 2N x 2N product per slice pair); stage_product_ms adds "
                     "the slicing and exponent kernels of the same stage"}
+    # where the device time of one solve goes (the profiled solve; events between
+    # launches make it slightly longer than an unprofiled one)
+    breakdown = {"solve_ms": stp["device_ms"], "stage_products_ms": stp["stage_kernel_ms"],
+                 "renormalisations_ms": stp["renorm_ms"],
+                 "renormalisations": stp["renormalisations"],
+                 "rest_ms": stp["device_ms"] - stp["stage_kernel_ms"] - stp["renorm_ms"],
+                 "note": "rest = stage-matrix gathers, boundary transforms, intensities"}
 
     # ---- comparison forms on the same resident problem
     def compare(p):
@@ -558,7 +565,8 @@ def main():
                            "bulk_boundary": "non-reflecting bulk records (f = 0)",
                            "l2": "inputs larger than L2 (state + stage table > 1 GB)",
                            "parallelism": f"replicas x{ws}"},
-                "roofline": roof, "fp64": fp64, "bf16_split": bf16, "uneven_batch": uneven,
+                "roofline": roof, "breakdown": breakdown, "fp64": fp64, "bf16_split": bf16,
+                "uneven_batch": uneven,
                 "e2e": e2e,
                 "cpu_baseline": cpu,
                 "gpu_launches": launches, "clocks": clk, "wall_seconds_timed": t_wall,

@@ -74,7 +74,8 @@ int trhepd_set_option(trhepd_context* ctx, int option, double value);
    device milliseconds of the stage-product kernels (TRHEPD_OPT_PROFILE only),
    out[5] kernels launched, out[6] of which renormalisation kernels, out[7] summed
    device milliseconds of the tensor-core kernel alone inside the stage products
-   (TRHEPD_OPT_PROFILE only) */
+   (TRHEPD_OPT_PROFILE only), out[8] summed device milliseconds of the end-of-slice
+   renormalisations (TRHEPD_OPT_PROFILE only) */
 int trhepd_last_stats(const trhepd_context* ctx, double* out, int n);
 
 /*

@@ -178,8 +178,9 @@ struct trhepd_context {
   int profile = 0;               // 1: time every stage-product launch with events
   int graphs = 1;                // 1: replay resident solves from a captured CUDA graph
   int fused_max_n = kFusedMaxBeams;  // FP64 RKN solves with n <= this run fused (0: never)
-  double stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double stats[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<cudaEvent_t> evpool;
+  std::vector<cudaEvent_t> rnpool;  // profile mode: pairs around renormalisations
   // device buffers (grown on demand, reused across calls)
   DevBuf asf, b, dchg, ghk, z[3], ocr[3], ielm[3], st[3], depth, table, pair;
   DevBuf Q0, Q1, P, V, D, gam, F, flags, dval, gj, f2, wnsga2, status, split;
@@ -297,6 +298,7 @@ struct RunState {
   int gj_per = 0;
   bool capturing = false;    // launches go into a CUDA graph: no events on the stream
   long prof_entries = 0;     // event quadruples recorded in profile mode
+  long renorm_entries = 0;   // event pairs around renormalisations (profile mode)
   int nprob = 1;             // stacked problems (see trhepd_problem::nprob)
   const TableEntry* const* tables = nullptr;
   StackedRows sr{};          // rows and stage-matrix stride per stacked problem
@@ -511,6 +513,13 @@ void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_m
       C->evpool.push_back(e);
     }
   }
+  if (C->profile && (int)C->rnpool.size() < 2 * (Pb.ns + 2)) {
+    while ((int)C->rnpool.size() < 2 * (Pb.ns + 2)) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      C->rnpool.push_back(e);
+    }
+  }
   if (!R.capturing) CK(cudaEventRecord(C->ev0, st));
   CK(cudaMemsetAsync(R.status, 0, 16, st));
   CK(cudaMemsetAsync(R.Q, 0, R.sbytes, st));
@@ -558,11 +567,26 @@ void stage_product(trhepd_context* C, RunState& R, const cd* Q, cd* P, cd* Qo, d
   if (ev) ++R.prof_entries;
 }
 
+void renormalise_launch(trhepd_context* C, RunState& R, bool last, int l, bool every_slice);
+
 // End-of-slice renormalisation: the reference's Gershgorin test per angle
 // (policy 0, cond_est matcomp.f90:498-528 > 1e3, matAbdivB :53-69) or the
 // growth bound every R.interval slices (policy 1); always on the last slice.
 void renormalise(trhepd_context* C, RunState& R, int l, bool every_slice) {
   const bool last = (l == R.ns);
+  const long gj0 = R.gj_launches;
+  cudaEvent_t* ev = (C->profile && 2 * (R.renorm_entries + 1) <= (long)C->rnpool.size())
+                        ? &C->rnpool[2 * R.renorm_entries]
+                        : nullptr;
+  if (ev) CK(cudaEventRecord(ev[0], R.st));
+  renormalise_launch(C, R, last, l, every_slice);
+  if (ev && R.gj_launches != gj0) {
+    CK(cudaEventRecord(ev[1], R.st));
+    ++R.renorm_entries;
+  }
+}
+
+void renormalise_launch(trhepd_context* C, RunState& R, bool last, int l, bool every_slice) {
   if (C->renorm_policy == 0 && !every_slice) {
     launch_cond_est(R.Q, R.nang, R.n, R.ld, last ? 1 : 0, R.flags, R.dval, R.st);
     launch_gauss_jordan(R.Q, R.P, R.flags, R.nang, R.n, R.ld, R.gjs, R.status, R.st);
@@ -602,7 +626,13 @@ void finish_host(trhepd_context* C, trhepd_problem& Pb, RunState& R) {
   CK(cudaStreamSynchronize(st));
   float ms = 0;
   cudaEventElapsedTime(&ms, C->ev0, C->ev1);
-  double prod_ms = 0.0, tensor_ms = 0.0;
+  double prod_ms = 0.0, tensor_ms = 0.0, renorm_ms = 0.0;
+  if (C->profile)
+    for (long p = 0; p < R.renorm_entries; ++p) {
+      float e = 0;
+      cudaEventElapsedTime(&e, C->rnpool[2 * p], C->rnpool[2 * p + 1]);
+      renorm_ms += e;
+    }
   if (C->profile)
     for (long p = 0; p < R.prof_entries; ++p) {
       float e = 0, t = 0;
@@ -619,6 +649,7 @@ void finish_host(trhepd_context* C, trhepd_problem& Pb, RunState& R) {
   C->stats[5] = (double)R.launches;
   C->stats[6] = (double)R.gj_launches;
   C->stats[7] = tensor_ms;
+  C->stats[8] = renorm_ms;
   if (h_status[0] & kStatusTimeout) throw CudaError("device wait timed out", TRHEPD_ETIMEOUT);
   if (h_status[0] & (kStatusNonFinite | kStatusZeroPivot))
     throw CudaError("non-finite value or zero pivot in the surface solve", TRHEPD_ENONFINITE);
@@ -1619,7 +1650,7 @@ int trhepd_set_option(trhepd_context* c, int option, double value) {
 
 int trhepd_last_stats(const trhepd_context* c, double* out, int n) {
   if (!c || !out) return TRHEPD_EINVAL;
-  for (int i = 0; i < n && i < 8; ++i) out[i] = c->stats[i];
+  for (int i = 0; i < n && i < 9; ++i) out[i] = c->stats[i];
   return TRHEPD_OK;
 }
 

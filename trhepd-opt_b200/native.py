@@ -159,12 +159,13 @@ class Context:
         self._check(self._L.trhepd_set_option(self._h, option, float(value)))
 
     def last_stats(self) -> dict:
-        out = np.zeros(8)
-        self._check(self._L.trhepd_last_stats(self._h, out.ctypes.data, 8))
+        out = np.zeros(9)
+        self._check(self._L.trhepd_last_stats(self._h, out.ctypes.data, 9))
         return {"renormalisations": int(out[0]), "stage_products": int(out[1]),
                 "device_ms": float(out[2]), "stage_columns": int(out[3]),
                 "stage_kernel_ms": float(out[4]), "launches": int(out[5]),
-                "renorm_launches": int(out[6]), "tensor_kernel_ms": float(out[7])}
+                "renorm_launches": int(out[6]), "tensor_kernel_ms": float(out[7]),
+                "renorm_ms": float(out[8])}
 
     def surf_run(self, bulkp, surf, dz2: float, int_method: int = 5, precision: int = FP64,
                  out_path=None):
