@@ -610,24 +610,45 @@ __global__ void k_gj_panel(const cd* __restrict__ Q, const int* __restrict__ fla
 // Each CTA owns kUpdCols of the remaining columns of one angle.
 // One thread per column of the trailing matrix (Q columns right of the panel,
 // then every P column), 128 columns per block: the column's pivot-row values C1
-// stay in registers; the multipliers L2 of 32 rows at a time are staged in shared
-// memory and read as broadcasts.
+// stay in registers; the multipliers L2 of 32 rows at a time are copied into
+// shared memory asynchronously (two buffers: the next chunk is in flight while the
+// current one is applied) and read as broadcasts.  At most 128 registers per
+// thread, so four blocks share an SM and the 9 column blocks of all 61 angles of
+// an N = 521 solve run in one wave.
 constexpr int kUpdRows = 32;
 template <int kW>
-__global__ void __launch_bounds__(kUpdCols) k_gj_update(cd* __restrict__ Q, cd* __restrict__ P,
-                                                        const int* __restrict__ flag, int n,
-                                                        int ld, int c0, int w, GJScratch sc) {
+__global__ void __launch_bounds__(kUpdCols, 4) k_gj_update(cd* __restrict__ Q, cd* __restrict__ P,
+                                                           const int* __restrict__ flag, int n,
+                                                           int ld, int c0, int w, GJScratch sc) {
   const int a = blockIdx.y;
   if (flag && !flag[a]) return;
   const int qrest = n - (c0 + w);          // Q columns right of the panel
   const int vc = blockIdx.x * kUpdCols + threadIdx.x;  // virtual column
   const int total = qrest + n;
   __shared__ cd W1[kW * kW];
-  __shared__ cd Ls[kUpdRows][kW];
+  __shared__ __align__(16) cd Ls[2][kUpdRows][kW];  // 16-byte cp.async targets
   __shared__ int piv[kW];
   const int tid = threadIdx.x;
   for (int e = tid; e < kW * kW; e += kUpdCols) W1[e] = sc.W1[(size_t)a * kW * kW + e];
   if (tid < kW) piv[tid] = sc.piv[a * kW + tid];
+  const cd* L2 = sc.L2 + (size_t)a * n * kW;
+  constexpr int kStage = kUpdRows * kW / kUpdCols;  // multiplier entries per thread and chunk
+  static_assert(kUpdRows * kW % kUpdCols == 0, "chunk staging");
+  // asynchronous copies of the chunk at rows i0.. into Ls[b] (zeros past row n)
+  auto fetch = [&](int i0, int b) {
+#pragma unroll
+    for (int q = 0; q < kStage; ++q) {
+      const int e = tid + q * kUpdCols, i = i0 + e / kW;
+      const cd* src = L2 + (size_t)min(i, n - 1) * kW + e % kW;
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&Ls[b][e / kW][e % kW]);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+                   "r"(i < n ? 16 : 0)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  fetch(0, 0);
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
   const bool valid = vc < total;
   cd* base = nullptr;
@@ -656,36 +677,34 @@ __global__ void __launch_bounds__(kUpdCols) k_gj_update(cd* __restrict__ Q, cd* 
     }
   }
   // other rows <- C2 - L2 C1
-  const cd* L2 = sc.L2 + (size_t)a * n * kW;
-  for (int i0 = 0; i0 < n; i0 += kUpdRows) {
-    __syncthreads();
-    for (int e = tid; e < kUpdRows * kW; e += kUpdCols) {
-      const int i = i0 + e / kW;
-      Ls[e / kW][e % kW] = (i < n) ? L2[(size_t)i * kW + e % kW] : cd{0.0, 0.0};
-    }
-    __syncthreads();
-    if (!valid) continue;
-    constexpr int U = 8;
-    for (int q = 0; q < kUpdRows; q += U) {
-      cd v[U];
+  int buf = 0;
+  for (int i0 = 0; i0 < n; i0 += kUpdRows, buf ^= 1) {
+    if (i0 + kUpdRows < n) fetch(i0 + kUpdRows, buf ^ 1);
+    if (valid) {
+      constexpr int U = 8;
+      for (int q = 0; q < kUpdRows; q += U) {
+        cd v[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int i = i0 + q + u;
-        const bool row = i < n && !(i >= c0 && i < c0 + w);
-        v[u] = row ? base[(size_t)i * ld] : cd{0.0, 0.0};
-      }
+        for (int u = 0; u < U; ++u) {
+          const int i = i0 + q + u;
+          const bool row = i < n && !(i >= c0 && i < c0 + w);
+          v[u] = row ? base[(size_t)i * ld] : cd{0.0, 0.0};
+        }
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int i = i0 + q + u;
-        if (i < n && !(i >= c0 && i < c0 + w)) {
-          cd x = v[u];
+        for (int u = 0; u < U; ++u) {
+          const int i = i0 + q + u;
+          if (i < n && !(i >= c0 && i < c0 + w)) {
+            cd x = v[u];
 #pragma unroll
-          for (int m = 0; m < kW; ++m)
-            if (m < w) x = x - Ls[q + u][m] * c1[m];
-          base[(size_t)i * ld] = x;
+            for (int m = 0; m < kW; ++m)
+              if (m < w) x = x - Ls[buf][q + u][m] * c1[m];
+            base[(size_t)i * ld] = x;
+          }
         }
       }
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
   }
 }
 
