@@ -20,6 +20,14 @@ __host__ __device__ __forceinline__ cd operator*(cd a, cd b) {
 }
 __host__ __device__ __forceinline__ cd operator*(double s, cd a) { return cd{s * a.x, s * a.y}; }
 __host__ __device__ __forceinline__ cd conj(cd a) { return cd{a.x, -a.y}; }
+// acc + a b and acc - a b as four fused multiply-adds (rounds differently from
+// acc + (a * b) with the product formed first)
+__host__ __device__ __forceinline__ cd cfma(cd a, cd b, cd acc) {
+  return cd{fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y))};
+}
+__host__ __device__ __forceinline__ cd cfms(cd a, cd b, cd acc) {
+  return cd{fma(-a.x, b.x, fma(a.y, b.y, acc.x)), fma(-a.x, b.y, fma(-a.y, b.x, acc.y))};
+}
 __host__ __device__ __forceinline__ double cabs1(cd a) { return fabs(a.x) + fabs(a.y); }
 // a / b with the scaling of Smith's algorithm
 __host__ __device__ __forceinline__ cd cdiv(cd a, cd b) {

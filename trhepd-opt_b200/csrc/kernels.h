@@ -85,10 +85,11 @@ void launch_cond_est(const cd* Q, int nang, int n, int ld, int force, int* flag,
 constexpr int kMaxBeams = 832;
 
 // K8: Q^{-1} P by blocked Gauss-Jordan with partial pivoting, per flagged angle.
-// scratch: gj_scratch_bytes(nang, n) bytes.
+// scratch: gj_scratch_bytes(nang, n) bytes.  fused: complex multiply-adds as four
+// FMAs (faster, different rounding; the split forms' renormalisations).
 size_t gj_scratch_bytes(int nang, int n);
 void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld, void* scratch,
-                         unsigned* status, cudaStream_t st);
+                         unsigned* status, cudaStream_t st, bool fused = false);
 
 // RK4 stage combination (rk4_int, surf_rk.f90:27-91); see kernels_f64.cu.
 void launch_rk4_combine(cd* Q, cd* P, cd* Qt, cd* Pt, cd* KP, cd* SQ, cd* SP, int j, double w,

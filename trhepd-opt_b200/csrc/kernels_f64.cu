@@ -485,8 +485,22 @@ static GJScratch gj_carve(void* scratch, int nang, int n) {
   return s;
 }
 
+// Complex multiply-add of the elimination: kF selects four fused multiply-adds
+// (the split forms' renormalisations) or the product formed first (the FP64
+// form, whose results match the reference's rounding most closely).
+template <bool kF>
+__device__ __forceinline__ cd gj_add(cd s, cd a, cd b) {
+  if constexpr (kF) return cfma(a, b, s);
+  else return s + a * b;
+}
+template <bool kF>
+__device__ __forceinline__ cd gj_sub(cd s, cd a, cd b) {
+  if constexpr (kF) return cfms(a, b, s);
+  else return s - a * b;
+}
+
 // Column-major complex access helper for the panel held in shared memory: S[i*kW + k].
-template <int kW>
+template <int kW, bool kF>
 __global__ void k_gj_panel(const cd* __restrict__ Q, const int* __restrict__ flag, int n, int ld,
                            int c0, int w, GJScratch sc, unsigned* status) {
   const int a = blockIdx.x;
@@ -558,7 +572,7 @@ __global__ void k_gj_panel(const cd* __restrict__ Q, const int* __restrict__ fla
     for (int i = col + 1 + tid; i < n; i += nt) {
       cd l = S[i * kW + jj] * rinv;
       S[i * kW + jj] = l;
-      for (int k = jj + 1; k < w; ++k) S[i * kW + k] = S[i * kW + k] - l * S[col * kW + k];
+      for (int k = jj + 1; k < w; ++k) S[i * kW + k] = gj_sub<kF>(S[i * kW + k], l, S[col * kW + k]);
     }
     __syncthreads();
   }
@@ -598,9 +612,9 @@ __global__ void k_gj_panel(const cd* __restrict__ Q, const int* __restrict__ fla
     cd s = cd{0.0, 0.0};
     if (k < w) {
       if (i >= c0 + w) {
-        for (int m = 0; m < w; ++m) s = s + S[i * kW + m] * Linv[m * kW + k];
+        for (int m = 0; m < w; ++m) s = gj_add<kF>(s, S[i * kW + m], Linv[m * kW + k]);
       } else if (i < c0) {
-        for (int m = 0; m < w; ++m) s = s + S[i * kW + m] * W1s[m * kW + k];
+        for (int m = 0; m < w; ++m) s = gj_add<kF>(s, S[i * kW + m], W1s[m * kW + k]);
       }
     }
     L2[e] = s;
@@ -616,7 +630,7 @@ __global__ void k_gj_panel(const cd* __restrict__ Q, const int* __restrict__ fla
 // thread, so four blocks share an SM and the 9 column blocks of all 61 angles of
 // an N = 521 solve run in one wave.
 constexpr int kUpdRows = 32;
-template <int kW>
+template <int kW, bool kF>
 __global__ void __launch_bounds__(kUpdCols, 4) k_gj_update(cd* __restrict__ Q, cd* __restrict__ P,
                                                            const int* __restrict__ flag, int n,
                                                            int ld, int c0, int w, GJScratch sc) {
@@ -672,7 +686,7 @@ __global__ void __launch_bounds__(kUpdCols, 4) k_gj_update(cd* __restrict__ Q, c
       cd v = cd{0.0, 0.0};
 #pragma unroll
       for (int m = 0; m < kW; ++m)
-        if (m < w) v = v + W1[k * kW + m] * c1[m];  // entries past w are not written
+        if (m < w) v = gj_add<kF>(v, W1[k * kW + m], c1[m]);  // entries past w are not written
       base[(size_t)(c0 + k) * ld] = v;
     }
   }
@@ -697,7 +711,7 @@ __global__ void __launch_bounds__(kUpdCols, 4) k_gj_update(cd* __restrict__ Q, c
             cd x = v[u];
 #pragma unroll
             for (int m = 0; m < kW; ++m)
-              if (m < w) x = x - Ls[buf][q + u][m] * c1[m];
+              if (m < w) x = gj_sub<kF>(x, Ls[buf][q + u][m], c1[m]);
             base[(size_t)i * ld] = x;
           }
         }
@@ -708,28 +722,31 @@ __global__ void __launch_bounds__(kUpdCols, 4) k_gj_update(cd* __restrict__ Q, c
   }
 }
 
-template <int kW>
+template <int kW, bool kF>
 static void gauss_jordan_panels(cd* Q, cd* P, const int* flag, int nang, int n, int ld,
                                 const GJScratch& sc, unsigned* status, cudaStream_t st) {
   const size_t smem = (size_t)n * kW * sizeof(cd);
   static size_t attr = 0;
   if (smem > attr) {
-    cudaFuncSetAttribute(k_gj_panel<kW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_gj_panel<kW, kF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = smem;
   }
   for (int c0 = 0; c0 < n; c0 += kW) {
     int w = (n - c0 < kW) ? n - c0 : kW;
-    k_gj_panel<kW><<<nang, 256, smem, st>>>(Q, flag, n, ld, c0, w, sc, status);
+    k_gj_panel<kW, kF><<<nang, 256, smem, st>>>(Q, flag, n, ld, c0, w, sc, status);
     int total = (n - (c0 + w)) + n;
     dim3 grid(ceil_div(total, kUpdCols), nang);
-    k_gj_update<kW><<<grid, kUpdCols, 0, st>>>(Q, P, flag, n, ld, c0, w, sc);
+    k_gj_update<kW, kF><<<grid, kUpdCols, 0, st>>>(Q, P, flag, n, ld, c0, w, sc);
   }
 }
 
 void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld, void* scratch,
-                         unsigned* status, cudaStream_t st) {
+                         unsigned* status, cudaStream_t st, bool fused) {
   GJScratch sc = gj_carve(scratch, nang, n);
-  gauss_jordan_panels<kWMax>(Q, P, flag, nang, n, ld, sc, status, st);
+  if (fused)
+    gauss_jordan_panels<kWMax, true>(Q, P, flag, nang, n, ld, sc, status, st);
+  else
+    gauss_jordan_panels<kWMax, false>(Q, P, flag, nang, n, ld, sc, status, st);
 }
 
 // ============================================================ RK4 stage combination

@@ -589,13 +589,13 @@ void renormalise(trhepd_context* C, RunState& R, int l, bool every_slice) {
 void renormalise_launch(trhepd_context* C, RunState& R, bool last, int l, bool every_slice) {
   if (C->renorm_policy == 0 && !every_slice) {
     launch_cond_est(R.Q, R.nang, R.n, R.ld, last ? 1 : 0, R.flags, R.dval, R.st);
-    launch_gauss_jordan(R.Q, R.P, R.flags, R.nang, R.n, R.ld, R.gjs, R.status, R.st);
+    launch_gauss_jordan(R.Q, R.P, R.flags, R.nang, R.n, R.ld, R.gjs, R.status, R.st, R.split);
     launch_set_identity(R.Q, R.flags, R.nang, R.n, R.ld, R.st);
     R.launches += 2 + R.gj_per;
     R.gj_launches += R.gj_per;
     if (!last) ++R.renorms;  // upper bound; per-angle decisions stay on the device
   } else if (last || every_slice || (l % R.interval) == 0) {
-    launch_gauss_jordan(R.Q, R.P, nullptr, R.nang, R.n, R.ld, R.gjs, R.status, R.st);
+    launch_gauss_jordan(R.Q, R.P, nullptr, R.nang, R.n, R.ld, R.gjs, R.status, R.st, R.split);
     launch_set_identity(R.Q, nullptr, R.nang, R.n, R.ld, R.st);
     R.launches += 1 + R.gj_per;
     R.gj_launches += R.gj_per;
