@@ -58,9 +58,14 @@ enum trhepd_option {
   TRHEPD_OPT_FUSED_MAX_N = 7,   /* FP64 RKN solves (int_method 5, 6) with 2 <= nb <= this value
                                    (at most 64; default 64, 0 disables) integrate every slice in
                                    one launch, one CTA per angle, state in shared memory */
-  TRHEPD_OPT_STREAM_PRIORITY = 8 /* 0 (default, lowest) .. 1 (highest): priority of the
+  TRHEPD_OPT_STREAM_PRIORITY = 8, /* 0 (default, lowest) .. 1 (highest): priority of the
                                    context's stream; the block scheduler starts pending work of
                                    higher-priority streams first when several contexts share a GPU */
+  TRHEPD_OPT_VALIDATE = 9       /* nonzero: every split-form solve (trhepd_srfref,
+                                   trhepd_problem_solve) is checked against the plain FP64 form
+                                   of the same problem, solved first with the same options; the
+                                   per-curve errors are read with trhepd_last_curve_errors.  Costs
+                                   one FP64 solve (about 3.5x the INT8 solve at N = 521) */
 };
 
 typedef struct trhepd_context trhepd_context;
@@ -77,6 +82,13 @@ int trhepd_set_option(trhepd_context* ctx, int option, double value);
    (TRHEPD_OPT_PROFILE only), out[8] summed device milliseconds of the end-of-slice
    renormalisations (TRHEPD_OPT_PROFILE only) */
 int trhepd_last_stats(const trhepd_context* ctx, double* out, int n);
+/* Per-curve errors of the last validated split-form solve (TRHEPD_OPT_VALIDATE), one
+   rocking curve per angle row: out[3a] = max over every spot of |I - I64| / |I64| (a
+   spot with I64 = 0 counts 0 when I = 0 too), out[3a+1] = max |I - I64| over the
+   curve's largest |I64|, out[3a+2] = the curve's largest |I64|.  n: capacity of out in
+   doubles (at least 3 x angles).  EINVAL when the last solve was not a validated
+   split-form solve.  No counterpart in the reference, whose only form is FP64. */
+int trhepd_last_curve_errors(const trhepd_context* ctx, double* out, int n);
 
 /*
  * Structure state of the potential, mirroring module mod_scpot3
@@ -122,17 +134,19 @@ int trhepd_potential_table(trhepd_context* ctx, const trhepd_pot_state* pot, int
                            int ns, double dz, double* v, double* vi, int* ncol);
 
 /*
- * Same tables as trhepd_potential_table, for callers that cannot allocate device
- * memory (a host that hands the whole GPU to its own memory pool at start-up, or
- * a service whose device memory is planned once): no cudaMalloc/cudaFree, no
- * context.  Its device scratch (input copies and the table) is one 32 MiB array
- * inside the library, held by every GPU that loads it until the process exits.
- * Works on the current device and the legacy default stream, synchronously.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  Calls share the array (it keeps the last
- * call's contents; nothing in it has to start at zero, since each call writes what
- * it reads), so calls whose GPU work overlaps race.  Returns
- * TRHEPD_ENOMEM when the inputs and the table need more than the 32 MiB.
+ * Same tables as trhepd_potential_table (every int_method 1-7), for callers that
+ * cannot allocate device memory (a host that hands the whole GPU to its own memory
+ * pool at start-up, or a service whose device memory is planned once): no
+ * cudaMalloc/cudaFree, no context.  Its device scratch (input copies and the table)
+ * is one 32 MiB array inside the library, held by every GPU that loads it until the
+ * process exits.  Works on the current device and the legacy default stream,
+ * synchronously.  Every call looks up the array's device address on the current
+ * device; the first call on a device also loads the library's device code there, so
+ * make that first call before any stream capture.  Calls share the array (it keeps
+ * the last call's contents; nothing in it has to start at zero, since each call
+ * writes what it reads), so calls whose GPU work overlaps race.  Returns
+ * TRHEPD_ENOMEM when the inputs and the table need more than the 32 MiB, and
+ * TRHEPD_EINVAL for an int_method outside 1-7.
  * This entry point has no counterpart in the reference.
  */
 int trhepd_potential_table_noalloc(const trhepd_pot_state* pot, int int_method, int ns,
@@ -222,6 +236,14 @@ int trhepd_rocking_convolution(trhepd_context* ctx, const double* angle_deg, con
 int trhepd_problem_convolve(trhepd_context* ctx, trhepd_problem* pb, double omega_deg,
                             double* out);
 int trhepd_problem_fetch(trhepd_context* ctx, trhepd_problem* pb, double* f2, double* angle_deg);
+/* The curve-comparison metric of the reference's regression scripts
+   (test/test23/compare.py:50-67) between a solved resident problem's intensities
+   (the computed curves, compare.py's first file) and ref_f2 (nangles, nb) host
+   curves (its second file), reduced on the device: per angle row a,
+   out[2a] = ||I_a - ref_a||_2 / max_b ||I_b||_2 and out[2a+1] = ||I_a - ref_a||_2 /
+   ||I_a||_2 (a zero norm counts 1).  out: (nangles, 2) host buffer. */
+int trhepd_problem_compare(trhepd_context* ctx, trhepd_problem* pb, const double* ref_f2,
+                           double* out);
 int trhepd_problem_info(const trhepd_problem* pb, int64_t* out, int n);
 void trhepd_problem_destroy(trhepd_problem* pb);
 

@@ -8,6 +8,7 @@ path never does.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 from pathlib import Path
@@ -45,6 +46,12 @@ def lib():
         L.oracle_surface_solve.restype = ctypes.c_int
         L.oracle_surface_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_surface_solve_list.restype = ctypes.c_int
+        L.oracle_surface_solve_list.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_surface_kappa_max.restype = ctypes.c_double
+        L.oracle_surface_kappa_max.argtypes = [ctypes.c_void_p]
+        L.oracle_set_renorm_every.argtypes = [ctypes.c_int]
         L.oracle_surface_write.restype = ctypes.c_int
         L.oracle_surface_write.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.oracle_bulk_run.restype = ctypes.c_int
@@ -104,6 +111,22 @@ class Surface:
             raise RuntimeError(f"oracle solve failed rc={rc}")
         return f2, ang, ren
 
+    def solve_list(self, idx):
+        """Solve the listed angles (schedule indices) in parallel, one per thread."""
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        f2 = np.empty((len(idx), self.nb), dtype=np.float64)
+        ang = np.empty(len(idx), dtype=np.float64)
+        ren = np.empty(len(idx), dtype=np.int32)
+        rc = lib().oracle_surface_solve_list(self._h, idx.ctypes.data, len(idx), f2.ctypes.data,
+                                             ang.ctypes.data, ren.ctypes.data)
+        if rc:
+            raise RuntimeError(f"oracle solve failed rc={rc}")
+        return f2, ang, ren
+
+    def kappa_max(self) -> float:
+        """Largest evanescent decay constant over the beams and angles of the scan."""
+        return float(lib().oracle_surface_kappa_max(self._h))
+
     def write(self, path) -> None:
         rc = lib().oracle_surface_write(self._h, str(path).encode())
         if rc:
@@ -134,6 +157,18 @@ def set_bulk_scale(s: float) -> None:
     lib().oracle_set_bulk_scale(ctypes.c_double(s))
 
 
+def set_renorm_every(k: int) -> None:
+    """0: the reference's Gershgorin renormalisation test (default); k > 0:
+    renormalise after every k-th slice instead (a growth-bound schedule)."""
+    lib().oracle_set_renorm_every(int(k))
+
+
+def growth_interval(kappa_max: float, dz: float, tau: float = math.log(1e3)) -> int:
+    """Slices between renormalisations of the growth-bound schedule: the largest
+    L with exp((kappa_max + 1) L dz) <= exp(tau)."""
+    return max(1, int(math.floor(tau / ((kappa_max + 1.0) * dz))))
+
+
 def set_max_slices(n: int) -> None:
     """Integrate only the first n slices (0 = all); for bounded timing samples."""
     lib().oracle_set_max_slices(int(n))
@@ -159,3 +194,16 @@ def rocking_convolution(angle_deg, f2, omega: float = 0.5, scan: int | None = No
         g = (1.0 / (sigma * np.sqrt(2.0 * np.pi))) * np.exp(-0.5 * x ** 2 / sigma ** 2)
         out[b0:b0 + scan] = (g * d) @ f2[b0:b0 + scan]
     return out
+
+
+def compare_curves(comp, ref):
+    """The per-angle metric of the reference's regression scripts, restating
+    test/test23/compare.py:50-67: for each angle row, n0 = ||comp||_2 (1 when 0) and
+    e0 = ||comp - ref||_2; returns (nangles, 2) = (e0 / max_a n0, e0 / n0), the two
+    numbers the script prints after the angle."""
+    comp = np.asarray(comp, dtype=float)
+    ref = np.asarray(ref, dtype=float)
+    n0 = np.linalg.norm(comp, axis=1)
+    n0 = np.where(n0 == 0.0, 1.0, n0)
+    e0 = np.linalg.norm(comp - ref, axis=1)
+    return np.stack([e0 / n0.max(), e0 / n0], axis=1)

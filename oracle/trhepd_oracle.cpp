@@ -2208,6 +2208,51 @@ int oracle_surface_solve(void* hh, int first, int count, double* f2, double* ang
   return 0;
 }
 
+// Solve the listed angles (indices into the flattened schedule, any order) in
+// parallel; rows of f2 / angle_out / renorm_out follow the list.
+int oracle_surface_solve_list(void* hh, const int* idx, int count, double* f2, double* angle_out,
+                              int* renorm_out) {
+  auto* h = static_cast<OracleSurface*>(hh);
+  auto a = schedule(h->S);
+  const int total = a.nrep1 * a.nrep2, nb = h->S.nbd[0];
+  for (int q = 0; q < count; ++q)
+    if (idx[q] < 0 || idx[q] >= total) return -1;
+  int rc = 0;
+#pragma omp parallel for schedule(dynamic)
+  for (int q = 0; q < count; ++q) {
+    double ang = 0;
+    int ren = 0;
+    int r = oracle_surface_solve(hh, idx[q], 1, f2 + (size_t)q * nb, &ang, &ren);
+    if (r) rc = r;
+    if (angle_out) angle_out[q] = ang;
+    if (renorm_out) renorm_out[q] = ren;
+  }
+  return rc;
+}
+
+// Largest evanescent decay constant sqrt(-s) over every beam and angle of the
+// schedule (s = wn^2 - |k_par + G|^2 < 0, the gamma rule of solve_one); sets the
+// interval of a growth-bound renormalisation schedule.
+double oracle_surface_kappa_max(void* hh) {
+  auto& S = static_cast<OracleSurface*>(hh)->S;
+  auto a = schedule(S);
+  const int nb = S.nbd[0];
+  double km = 0.0;
+  for (int t = 0; t < a.nrep1 * a.nrep2; ++t) {
+    int irep1 = t / a.nrep2, irep2 = t % a.nrep2;
+    double ga = a.ng_outer ? S.gi + irep2 * S.dg : S.gi + irep1 * S.dg;
+    double az = a.ng_outer ? S.azi + irep1 * S.daz : S.azi + irep2 * S.daz;
+    double wnx = S.wn * std::cos(ga) * std::cos(az), wny = S.wn * std::cos(ga) * std::sin(az);
+    for (int i = 0; i < nb; ++i) {
+      double wgx = S.ghx * S.ih[i] + wnx;
+      double wgy = S.ghy * S.ih[i] + S.gky * S.ik[i] + wny;
+      double s = S.wn * S.wn - wgx * wgx - wgy * wgy;
+      if (s < 0) km = std::max(km, std::sqrt(-s));
+    }
+  }
+  return km;
+}
+
 // bulk.exe equivalent: bulk.txt -> bulkP.b.  Returns 0 on success.
 int oracle_bulk_run(const char* bulk_txt, const char* out_path, char* err, int errlen) {
   try {

@@ -1,7 +1,7 @@
 """Extract the reference's own regression data into small fixtures.
 
-Reads the reference checkout (path given as argv[1], default /root/reference)
-and writes, per test case (test23 / test47 / test521):
+Reads the reference checkout (its path is the required first argument) and
+writes, per test case (test23 / test47 / test521):
 
 * ``<case>/bulkP.b``, ``<case>/surf.txt``, ``<case>/bulk.txt`` — the inputs the
   reference's regression runs used (test/<case>/);
@@ -9,7 +9,11 @@ and writes, per test case (test23 / test47 / test521):
   outputs test/<case>/test-results/perf-<method>-<dz>.txt (E23.15, 15 digits),
   for the integrators and slice thicknesses listed below;
 * ``conv-<name>.npz`` — a sample's rocking curves (surf-bulkP.s) and the
-  convolution.txt the reference's make_convolution.py wrote from them.
+  convolution.txt the reference's make_convolution.py wrote from them;
+* ``test23/accurate.npz`` — the converged curves surf-bulkP-str-accurate.s (sp4,
+  dz 0.001, E23.15) and, per (method, dz) of the perf fixtures, the first
+  repetition of the per-angle rows compare.py printed against them
+  (test-results/perf-comp-acc.txt: angle, e0 / max n0, e0 / n0).
 
 Run once in a container that has the reference; the fixtures travel with the
 repository and nothing at test time reads the reference.
@@ -51,6 +55,22 @@ def main(ref: Path):
             ang, f2, hdr = parse_s(p)
             np.savez_compressed(dst / f"perf-{m}-{dz}.npz", angle=ang, f2=f2,
                                 beams=hdr["beams"], naz=hdr["naz"], ng=hdr["ng"])
+    # converged curves and the comparison metric printed against them
+    src = ref / "test" / "test23"
+    ang, f2, hdr = parse_s(src / "surf-bulkP-str-accurate.s")
+    rows = {}
+    for line in (src / "test-results" / "perf-comp-acc.txt").read_text().split("\n"):
+        t = line.split()
+        if len(t) != 7:
+            continue
+        key = f"comp-{t[2]}-{t[3]}"
+        if (int(t[2]), t[3]) not in SEL["test23"]:
+            continue
+        r = rows.setdefault(key, [])
+        if len(r) < len(ang):  # compare.py ran once per repetition; keep the first
+            r.append([float(t[4]), float(t[5]), float(t[6])])
+    np.savez_compressed(HERE / "test23" / "accurate.npz", angle=ang, f2=f2,
+                        beams=hdr["beams"], **{k: np.array(v) for k, v in rows.items()})
     # rocking-curve convolution samples: the reference's surf-bulkP.s and the
     # convolution.txt its make_convolution.py wrote from it (omega 0.5 deg)
     for name, tree, samp in CONV:
@@ -63,4 +83,6 @@ def main(ref: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the reference checkout>")
+    main(Path(sys.argv[1]))

@@ -1,0 +1,215 @@
+"""The benchmark's synthetic structures against the CPU oracle (FP64
+restatement of the reference path, pinned to the reference's outputs by
+test_oracle_golden.py).  Fixtures: tests/golden/synthetic/*.npz, written by
+tests/golden/make_fixtures.py; each test regenerates the same inputs with the
+seeded generator and checks their SHA-256 first.
+
+Bars (every call through the C ABI):
+
+* plain FP64 form, same renormalisation schedule as the oracle: 1e-9 relative on
+  spots >= 1e-6 of the row maximum and 1e-10 of the row maximum on every spot;
+  the raw every-spot relative maximum is reported beside it;
+* split forms (INT8 and BF16 digit slices, 4 per operand): every spot within
+  SPLIT_REL relative of the oracle, except where the FP64 rounding floor of the
+  case (the oracle under its two renormalisation schedules, which differ by
+  rounding only) is itself larger: there the bound is FLOOR_FACTOR x that floor
+  per spot.
+"""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, spot_errors
+
+pytestmark = pytest.mark.gpu
+
+SYN = GOLDEN / "synthetic"
+SPLIT_REL = 1e-6
+FLOOR_FACTOR = 4.0
+
+
+def every_spot_rel(got, ref):
+    """Relative error of every spot; a spot whose reference is exactly 0 counts 0
+    when the result is 0 too."""
+    got, ref = np.asarray(got), np.asarray(ref)
+    d = np.abs(got - ref)
+    m = np.abs(ref)
+    return np.where(m > 0, d / np.where(m > 0, m, 1.0), np.where(d > 0, np.inf, 0.0))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from trhepd_opt_b200 import build, native
+    build.build()
+    c = native.Context(0)
+    c.set_option(native.OPT_SPLIT_SLICES, 4)
+    yield c
+    c.close()
+
+
+def _structure(name):
+    from trhepd_opt_b200 import generator
+    if name == "batch47":
+        return generator.batch47(2)
+    if name == "dense521":
+        return generator.dense(521, seed=3)
+    n = int(name[len("uneven"):])
+    base = generator.dense(n, seed=20 + n, n_angles=61, region=15.0, dz=0.02)
+    return generator.jitter(base, 0.1, 1000 * n)
+
+
+_CACHE: dict = {}
+
+
+def resident(ctx, tmp_path_factory, name):
+    """(fixture, resident problem) for a synthetic case, inputs checked by hash."""
+    if name in _CACHE:
+        return _CACHE[name]
+    from trhepd_opt_b200 import bulkfile, surface
+    fx = np.load(SYN / f"{name}.npz")
+    d = tmp_path_factory.mktemp(name)
+    s = _structure(name)
+    s.write(d)
+    bulkfile.write_bulkp(s, d / "bulkP.b")
+    h = hashlib.sha256()
+    for f in ("bulk.txt", "surf.txt", "bulkP.b"):
+        h.update((d / f).read_bytes())
+    assert h.hexdigest() == str(fx["sha"]), "generator no longer reproduces the fixture inputs"
+    sp = surface.SurfaceProblem(ctx, d / "bulkP.b", d / "surf.txt", s.surface_dz, s.int_method)
+    rp = sp.resident()
+    assert rp.nb == int(fx["nb"]) and rp.ns == int(fx["ns"])
+    _CACHE[name] = (fx, sp, rp)
+    return _CACHE[name]
+
+
+def solve_rows(ctx, rp, fx, precision, policy):
+    from trhepd_opt_b200 import native
+    ctx.set_option(native.OPT_RENORM_POLICY, policy)
+    rp.solve(precision)
+    st = ctx.last_stats()
+    ang, f2 = rp.fetch()
+    idx = fx["idx"]
+    np.testing.assert_allclose(ang[idx], fx["angle"], atol=1e-9)
+    return f2[idx], st
+
+
+def report(tag, got, ref):
+    abs_err, rel_err = spot_errors(got, ref)
+    raw = float(every_spot_rel(got, ref).max())
+    print(f"{tag}: max err / row max {abs_err:.3e}, rel (spots >= 1e-6 row max) {rel_err:.3e},"
+          f" rel every spot {raw:.3e}")
+    return abs_err, rel_err, raw
+
+
+CASES_FP64 = [("batch47", 0), ("dense521", 0), ("dense521", 1), ("uneven23", 0),
+              ("uneven47", 0), ("uneven95", 0), ("uneven191", 0)]
+
+
+@pytest.mark.parametrize("name,policy", CASES_FP64,
+                         ids=[f"{n}-{'gershgorin' if p == 0 else 'growth'}" for n, p in CASES_FP64])
+def test_fp64_matches_oracle(ctx, tmp_path_factory, name, policy):
+    from trhepd_opt_b200 import native
+    fx, sp, rp = resident(ctx, tmp_path_factory, name)
+    ref = fx["f2"] if policy == 0 else fx["f2_growth"]
+    got, st = solve_rows(ctx, rp, fx, native.FP64, policy)
+    if policy == 1:  # the same schedule as the oracle's growth-bound run
+        assert st["renormalisations"] == int(fx["renorm_growth"][0])
+    abs_err, rel_err, _ = report(f"{name} fp64 policy {policy}", got, ref)
+    assert abs_err <= 1e-10, abs_err
+    assert rel_err <= 1e-9, rel_err
+
+
+def split_bound(fx):
+    """Per-spot bound of the split forms: SPLIT_REL, or FLOOR_FACTOR x the FP64
+    floor where the oracle's two schedules already differ by more."""
+    if "f2_growth" not in fx:
+        return np.full(fx["f2"].shape, SPLIT_REL)
+    floor = every_spot_rel(fx["f2_growth"], fx["f2"])
+    return np.maximum(SPLIT_REL, FLOOR_FACTOR * floor)
+
+
+CASES_SPLIT = [(n, p) for n in ("batch47", "dense521") for p in (1, 2)]
+CASES_SPLIT += [(f"uneven{n}", 2) for n in (95, 191)]
+
+
+@pytest.mark.parametrize("name,precision", CASES_SPLIT,
+                         ids=[f"{n}-{'bf16' if p == 1 else 'int8'}" for n, p in CASES_SPLIT])
+def test_split_every_spot_matches_oracle(ctx, tmp_path_factory, name, precision):
+    fx, sp, rp = resident(ctx, tmp_path_factory, name)
+    policy = 1 if "f2_growth" in fx else 0
+    ref = fx["f2_growth"] if policy == 1 else fx["f2"]
+    got, _ = solve_rows(ctx, rp, fx, precision, policy)
+    report(f"{name} split {precision} policy {policy}", got, ref)
+    rel = every_spot_rel(got, ref)
+    bound = split_bound(fx)
+    worst = np.unravel_index(np.argmax(rel / bound), rel.shape)
+    assert (rel <= bound).all(), (float(rel[worst]), float(bound[worst]), worst)
+
+
+def test_curve_errors_through_abi(ctx, tmp_path_factory):
+    """TRHEPD_OPT_VALIDATE: an INT8 solve of dense521 also runs the FP64 form and
+    reports each curve's errors; they equal the errors of the two fetched results,
+    and the FP64 leg equals the oracle within the FP64 bar."""
+    from trhepd_opt_b200 import native
+    fx, sp, rp = resident(ctx, tmp_path_factory, "dense521")
+    ctx.set_option(native.OPT_RENORM_POLICY, 1)
+    rp.solve(native.FP64)
+    _, f64 = rp.fetch()
+    ctx.set_option(native.OPT_VALIDATE, 1)
+    try:
+        rp.solve(native.SPLIT_INT8)
+        st = ctx.last_stats()
+        err = ctx.last_curve_errors(rp.nangles)
+    finally:
+        ctx.set_option(native.OPT_VALIDATE, 0)
+    _, f8 = rp.fetch()
+    assert st["stage_products"] > 0
+    rel = every_spot_rel(f8, f64).max(axis=1)
+    rowmax = np.abs(f64).max(axis=1)
+    np.testing.assert_allclose(err[:, 0], rel, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(err[:, 2], rowmax, rtol=1e-15)
+    np.testing.assert_allclose(err[:, 1], np.abs(f8 - f64).max(axis=1) / rowmax, rtol=1e-12)
+    print(f"dense521 int8 per-curve max rel err: max {err[:, 0].max():.3e}, "
+          f"median {np.median(err[:, 0]):.3e}")
+    # the FP64 leg of a validated solve is the plain FP64 solve
+    abs_err, rel_err, _ = report("dense521 fp64 (validation leg)", f64[fx["idx"]],
+                                 fx["f2_growth"])
+    assert abs_err <= 1e-10 and rel_err <= 1e-9
+    # an unvalidated solve leaves no curve errors behind
+    rp.solve(native.SPLIT_INT8)
+    with pytest.raises(native.TrhepdError):
+        ctx.last_curve_errors(rp.nangles)
+
+
+@pytest.mark.parametrize("precision", [1, 2], ids=["bf16", "int8"])
+def test_split_on_reference_n521(ctx, golden, precision):
+    """The split forms on the reference's own N=521 case (test521, sp4, 0.33 A
+    slices, one angle) against its committed output."""
+    from trhepd_opt_b200 import native
+    d = golden / "test521"
+    ref = np.load(d / "perf-5-0.33.npz")["f2"]
+    ctx.set_option(native.OPT_RENORM_POLICY, 0)
+    f2, _ = ctx.surf_run(d / "bulkP.b", d / "surf.txt", 0.33, 5, precision)
+    abs_err, rel_err, raw = report(f"test521 split {precision}", f2, ref)
+    assert abs_err <= 1e-8, abs_err
+    assert rel_err <= SPLIT_REL, rel_err
+
+
+@pytest.mark.parametrize("name", ["uneven95", "uneven191"])
+def test_stacked_batch_matches_oracle(ctx, tmp_path_factory, name):
+    """A stacked INT8 batch of a candidate and a copy of it equals the oracle."""
+    from trhepd_opt_b200 import native, surface
+    fx, sp, rp = resident(ctx, tmp_path_factory, name)
+    rp2 = sp.resident()
+    try:
+        ctx.set_option(native.OPT_RENORM_POLICY, 0)
+        surface.solve_batch(ctx, [rp, rp2], native.SPLIT_INT8)
+        for p in (rp, rp2):
+            ang, f2 = p.fetch()
+            rel = every_spot_rel(f2[fx["idx"]], fx["f2"])
+            assert (rel <= SPLIT_REL).all(), float(rel.max())
+    finally:
+        rp2.close()

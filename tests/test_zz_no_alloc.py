@@ -37,14 +37,21 @@ def test_noalloc_tables_match_regular_entry_point(golden):
             scale = np.abs(v_ref).max()
             assert np.abs(v - v_ref).max() <= 1e-14 * scale, call
             assert np.abs(vi - vi_ref).max() <= 1e-14 * scale, call
-        # a different integrator through the same scratch
-        v6_ref, _ = sp.potential_table(6)
-        v6 = np.zeros_like(v6_ref)
+        # the other integrators' tables through the same scratch
+        for method in (6, 1, 2, 4, 7):
+            vm_ref, _ = sp.potential_table(method)
+            vm = np.zeros_like(vm_ref)
+            nc = ctypes.c_int(0)
+            rc = L.trhepd_potential_table_noalloc(ctypes.byref(sp.pot), method, sp.args.ns,
+                                                   sp.args.dz, vm.ctypes.data, None,
+                                                   ctypes.byref(nc))
+            assert rc == 0 and nc.value == vm_ref.shape[0], (method, rc)
+            assert np.abs(vm - vm_ref).max() <= 1e-14 * np.abs(vm_ref).max(), method
+        # an int_method the reference does not define
         nc = ctypes.c_int(0)
-        rc = L.trhepd_potential_table_noalloc(ctypes.byref(sp.pot), 6, sp.args.ns, sp.args.dz,
-                                               v6.ctypes.data, None, ctypes.byref(nc))
-        assert rc == 0 and nc.value == v6_ref.shape[0]
-        assert np.abs(v6 - v6_ref).max() <= 1e-14 * np.abs(v6_ref).max()
+        rc = L.trhepd_potential_table_noalloc(ctypes.byref(sp.pot), 9, sp.args.ns, sp.args.dz,
+                                               None, None, ctypes.byref(nc))
+        assert rc == 1  # TRHEPD_EINVAL
 
 
 def test_noalloc_rejects_tables_beyond_its_scratch(golden):

@@ -25,6 +25,7 @@
 
 #include "bulk.h"
 #include "kernels.h"
+#include "launch_attr.h"
 
 namespace trhepd {
 
@@ -147,11 +148,8 @@ __global__ void __launch_bounds__(128, 2)
 
 void launch_zgemm_batched(const BatchedGemm& g, cudaStream_t st) {
   using namespace bgemm;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_zgemm_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    attr = true;
-  }
+  static SmemOptIn attr;
+  attr.ensure((const void*)k_zgemm_batched, SMEM);
   dim3 grid(ceil_div(g.N, BN), ceil_div(g.M, BM), g.batch);
   k_zgemm_batched<<<grid, 128, SMEM, st>>>(g);
 }

@@ -13,6 +13,7 @@
 #include <cstdio>
 
 #include "kernels.h"
+#include "launch_attr.h"
 
 namespace trhepd {
 
@@ -368,11 +369,8 @@ void launch_stage_gemm_f64(const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
                            int ld, int kpad, double cb, double ca, cudaStream_t st,
                            StackedRows sr) {
   using namespace f64gemm;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_stage_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    attr = true;
-  }
+  static SmemOptIn attr;
+  attr.ensure((const void*)k_stage_gemm_f64, SMEM);
   int rows = nang * n;
   if (sr.rows_b <= 0) sr = StackedRows{rows, 0};
   const int nprob = ceil_div(rows, sr.rows_b);
@@ -726,11 +724,8 @@ template <int kW, bool kF>
 static void gauss_jordan_panels(cd* Q, cd* P, const int* flag, int nang, int n, int ld,
                                 const GJScratch& sc, unsigned* status, cudaStream_t st) {
   const size_t smem = (size_t)n * kW * sizeof(cd);
-  static size_t attr = 0;
-  if (smem > attr) {
-    cudaFuncSetAttribute(k_gj_panel<kW, kF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = smem;
-  }
+  static SmemOptIn attr;
+  attr.ensure((const void*)k_gj_panel<kW, kF>, smem);
   for (int c0 = 0; c0 < n; c0 += kW) {
     int w = (n - c0 < kW) ? n - c0 : kW;
     k_gj_panel<kW, kF><<<nang, 256, smem, st>>>(Q, flag, n, ld, c0, w, sc, status);

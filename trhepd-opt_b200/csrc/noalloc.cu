@@ -16,11 +16,12 @@
 
 #include <algorithm>
 #include <cstring>
-#include <mutex>
+#include <stdexcept>
 #include <vector>
 
 #include "../../include/trhepd_b200.h"
 #include "host_model.h"
+#include "integrators.h"
 #include "kernels.h"
 
 namespace {
@@ -30,61 +31,38 @@ using namespace trhepd;
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_setup_mu;
-void* g_scratch_addr[128] = {};  // device address of the array, per device ordinal
-
-// Once per device, with that device current: the device address of the array.
-// (In host code the array's name is only a host-side stand-in.)
-void* scratch_address(int dev) {
-  std::lock_guard<std::mutex> lock(g_setup_mu);
-  if (dev < 0 || dev >= 128) return nullptr;
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return nullptr;
-    g_scratch_addr[dev] = p;
-  }
-  return g_scratch_addr[dev];
+// The device address of the array on the current device.  In host code the
+// array's name is only a host-side stand-in, so every call asks the runtime for
+// the address on the device that is current for it (the lookup is cheap next to
+// the call's synchronous copies, and stays right after a cudaDeviceReset reloads
+// the module).
+void* scratch_address() {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return nullptr;
+  return p;
 }
 
 size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
-
-const double kRkn46[13] = {
-    0.0829844064174052,  0.245298957184271,  0.396309801498368,  0.604872665711080,
-    -0.0390563049223486, -0.350171622895351, 0.1195241940131508, -0.350171622895351,
-    -0.0390563049223486, 0.604872665711080,  0.396309801498368,  0.245298957184271,
-    0.0829844064174052};
-const double kRkn611[23] = {
-    0.0414649985182624,  0.123229775946271,  0.198128671918067,  0.290553797799558,
-    -0.0400061921041533, -0.127049212625417, 0.0752539843015807, -0.246331761062075,
-    -0.0115113874206879, 0.357208872795928,  0.2366699247869311, 0.20477705429147,
-    0.2366699247869311,  0.357208872795928,  -0.0115113874206879, -0.246331761062075,
-    0.0752539843015807,  -0.127049212625417, -0.0400061921041533, 0.290553797799558,
-    0.198128671918067,   0.123229775946271,  0.0414649985182624};
 
 }  // namespace
 
 extern "C" int trhepd_potential_table_noalloc(const trhepd_pot_state* pot, int int_method,
                                               int ns, double dz, double* v, double* vi,
                                               int* ncol_out) {
-  if (!pot || ns < 1 || (int_method != 5 && int_method != 6)) return TRHEPD_EINVAL;
+  if (!pot || ns < 1) return TRHEPD_EINVAL;
+  Integrator I;
+  try {
+    I = integrator_for(int_method);
+  } catch (const std::invalid_argument&) {
+    return TRHEPD_EINVAL;
+  }
   if (pot->nv < 1 || pot->nelm < 1 || pot->nabr < 1 || pot->nabr + pot->nabi > kMab)
     return TRHEPD_EINVAL;
   if (pot->natms < 0 || pot->natmb < 0 || pot->natms + 2 * pot->natmb > 512)
     return TRHEPD_EINVAL;
   const int nv = pot->nv, nelm = pot->nelm;
-  // stage depths of hp_int_init (surf_prkn.f90:184-196)
-  const int s = (int_method == 5) ? 6 : 11;
-  const double* bab = (int_method == 5) ? kRkn46 : kRkn611;
-  std::vector<double> depth;
-  depth.reserve((size_t)s * ns + 1);
-  for (int l = 1; l <= ns; ++l) {
-    double iz = dz * (l - 1);
-    for (int k = 1; k <= s; ++k) {
-      depth.push_back(iz);
-      iz = iz + dz * bab[2 * k - 1];
-    }
-  }
-  depth.push_back(dz * ns);
+  // the stage depths of the integrator's init routine, as trhepd_potential_table
+  const std::vector<double> depth = stage_depths(I, ns, dz);
   const int ncol = (int)depth.size();
 
   // layout of the scratch: inputs, depths, table
@@ -118,9 +96,7 @@ extern "C" int trhepd_potential_table_noalloc(const trhepd_pot_state* pot, int i
   off = up256(off + (size_t)ncol * nv * sizeof(TableEntry));
   if (off > kNoAllocScratchBytes) return TRHEPD_ENOMEM;  // beyond the static scratch
 
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return TRHEPD_ECUDA;
-  unsigned char* base = static_cast<unsigned char*>(scratch_address(dev));
+  unsigned char* base = static_cast<unsigned char*>(scratch_address());
   if (!base) return TRHEPD_ECUDA;
 
   auto put = [&](size_t o, const void* src, size_t bytes) {

@@ -25,6 +25,7 @@
 #include <stdexcept>
 
 #include "small.h"
+#include "launch_attr.h"
 
 namespace trhepd {
 namespace fused {
@@ -341,12 +342,8 @@ __global__ void __launch_bounds__(Cfg<NP>::THREADS)
 template <int NP>
 void launch(const FusedLaunch& L, cudaStream_t st) {
   using C = Cfg<NP>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_fused_rkn<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)C::SMEM);
-    attr = true;
-  }
+  static SmemOptIn attr;
+  attr.ensure((const void*)k_fused_rkn<NP>, C::SMEM);
   k_fused_rkn<NP><<<L.total_ctas, C::THREADS, C::SMEM, st>>>(L);
 }
 

@@ -20,7 +20,9 @@
 #include "bulk.h"
 #include "magnus.h"
 #include "bulk_model.h"
+#include "curves.h"
 #include "host_model.h"
+#include "integrators.h"
 #include "kernels.h"
 #include "small.h"
 #include "split_gemm.h"
@@ -28,20 +30,6 @@
 using namespace trhepd;
 
 namespace {
-
-// Blanes-Moan RKN coefficient tables (surf_prkn.f90:11-52).
-const double kRkn46[13] = {
-    0.0829844064174052,  0.245298957184271,  0.396309801498368,  0.604872665711080,
-    -0.0390563049223486, -0.350171622895351, 0.1195241940131508, -0.350171622895351,
-    -0.0390563049223486, 0.604872665711080,  0.396309801498368,  0.245298957184271,
-    0.0829844064174052};
-const double kRkn611[23] = {
-    0.0414649985182624,  0.123229775946271,  0.198128671918067,  0.290553797799558,
-    -0.0400061921041533, -0.127049212625417, 0.0752539843015807, -0.246331761062075,
-    -0.0115113874206879, 0.357208872795928,  0.2366699247869311, 0.20477705429147,
-    0.2366699247869311,  0.357208872795928,  -0.0115113874206879, -0.246331761062075,
-    0.0752539843015807,  -0.127049212625417, -0.0400061921041533, 0.290553797799558,
-    0.198128671918067,   0.123229775946271,  0.0414649985182624};
 
 struct CudaError : std::runtime_error {
   int code;
@@ -94,76 +82,6 @@ T* upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
   return b.as<T>();
 }
 
-// Integrator families of srfref (surflf.f90:118-140) on the GPU path.
-enum Family { kRkn = 0, kLeapfrog = 1, kRk4 = 2, kMagnus2 = 3, kMagnus4 = 4, kMagnus6 = 5 };
-
-struct Integrator {
-  int method = 5;
-  Family family = kRkn;
-  int s = 6;                   // RKN stages per slice
-  const double* bab = nullptr; // RKN coefficients (b1, a1, b2, a2, ...)
-};
-
-Integrator integrator_for(int method) {
-  switch (method) {
-    case 1: return {1, kMagnus2, 1, nullptr};
-    case 2: return {2, kMagnus4, 3, nullptr};
-    case 3: return {3, kMagnus6, 3, nullptr};
-    case 4: return {4, kLeapfrog, 1, nullptr};
-    case 5: return {5, kRkn, 6, kRkn46};
-    case 6: return {6, kRkn, 11, kRkn611};
-    case 7: return {7, kRk4, 2, nullptr};
-    default:
-      throw std::invalid_argument(
-          "int_method must be 1-3 (Magnus 2/4/6), 4 (leapfrog), 5 (RKN-4), 6 (RKN-6) or 7 (RK4)"
-          " on the GPU path");
-  }
-}
-
-// Depths of the stage potential table, same arithmetic order as the reference's
-// init routines: hp_int_init4/6 (surf_prkn.f90:184-196), m2_int_init
-// (surf_magnus.f90:4-20, used by m2 and leapfrog), m4_int_init (:24-42, m4 and m6),
-// rk4_int_init (surf_rk.f90:4-25).
-std::vector<double> stage_depths(const Integrator& I, int ns, double dz) {
-  std::vector<double> d;
-  switch (I.family) {
-    case kRkn:
-      d.reserve((size_t)I.s * ns + 1);
-      for (int l = 1; l <= ns; ++l) {
-        double iz = dz * (l - 1);
-        for (int k = 1; k <= I.s; ++k) {
-          d.push_back(iz);
-          iz = iz + dz * I.bab[2 * k - 1];
-        }
-      }
-      d.push_back(dz * ns);
-      break;
-    case kLeapfrog:
-    case kMagnus2:
-      for (int l = 1; l <= ns; ++l) d.push_back(dz * (l - 0.5));
-      break;
-    case kMagnus4:
-    case kMagnus6: {  // m4_int_init (surf_magnus.f90:24-42): the three Gauss points
-      const double c0 = (5.0 - std::sqrt(15.0)) / 10, c1 = 0.5, c2 = (5.0 + std::sqrt(15.0)) / 10;
-      for (int l = 1; l <= ns; ++l) {
-        d.push_back(dz * ((l - 1) + c0));
-        d.push_back(dz * ((l - 1) + c1));
-        d.push_back(dz * ((l - 1) + c2));
-      }
-      break;
-    }
-    case kRk4:
-      for (int l = 1; l <= ns; ++l) {
-        const double iz = dz * (l - 1);
-        d.push_back(iz);
-        d.push_back(iz + 0.5 * dz);
-      }
-      d.push_back(dz * ns);
-      break;
-  }
-  return d;
-}
-
 }  // namespace
 
 struct trhepd_context {
@@ -178,7 +96,9 @@ struct trhepd_context {
   int profile = 0;               // 1: time every stage-product launch with events
   int graphs = 1;                // 1: replay resident solves from a captured CUDA graph
   int fused_max_n = kFusedMaxBeams;  // FP64 RKN solves with n <= this run fused (0: never)
+  int validate = 0;              // 1: split solves also run the FP64 form (per-curve errors)
   double stats[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  std::vector<double> curve_err; // 3 per angle of the last validated solve (curves.h)
   std::vector<cudaEvent_t> evpool;
   std::vector<cudaEvent_t> rnpool;  // profile mode: pairs around renormalisations
   // device buffers (grown on demand, reused across calls)
@@ -186,6 +106,7 @@ struct trhepd_context {
   DevBuf Q0, Q1, P, V, D, gam, F, flags, dval, gj, f2, wnsga2, status, split;
   DevBuf sgh, sgk, simg, snimg, sst;
   DevBuf cva, cvf, cvo;  // rocking-curve convolution of host curves
+  DevBuf cerr, cref;     // per-curve errors / distances, reference curves of a comparison
   DevBuf bk[24];  // bulk-solve work arrays
   DevBuf rk[5];   // RK4 / Magnus stage buffers
   DevBuf mg[9];   // Magnus shared matrices
@@ -335,25 +256,49 @@ struct trhepd_problem {
   int ncol = 0;
   DevBuf table, pair, gam, D, F, wnsga2, f2, dang, conv;
   std::vector<double> angle_deg;
-  // CUDA graph of the whole solve, valid for `graph_key` and the context buffers
-  // in `graph_sig`; `last_sig` holds the buffers of the last uncaptured solve.
-  cudaGraphExec_t graph = nullptr;
+  // CUDA graphs of the whole solve, one per option set (`key`: precision form and
+  // the options the launch sequence depends on), each valid for the context
+  // buffers in its `sig`; `last_sig` holds the buffers of the slot's last
+  // uncaptured solve.  A validated split solve alternates two option sets.
+  struct GraphSlot {
+    std::vector<double> key;
+    std::vector<void*> sig, last_sig;
+    cudaGraphExec_t exec = nullptr;
+    RunState run;
+    void drop() {
+      if (exec) cudaGraphExecDestroy(exec);
+      exec = nullptr;
+      sig.clear();
+    }
+  };
+  static constexpr size_t kGraphSlots = 4;
+  std::vector<GraphSlot> graphs;
   OwnWorkspace own;            // buffers of batch solves (trhepd_batch_solve)
-  std::vector<double> graph_key;
-  std::vector<void*> graph_sig, last_sig;
-  RunState graph_run;
+  DevBuf f2ref;                // FP64 intensities of a validated split solve
   void drop_graph() {
-    if (graph) cudaGraphExecDestroy(graph);
-    graph = nullptr;
-    graph_sig.clear();
+    for (GraphSlot& g : graphs) g.drop();
+    graphs.clear();
+  }
+  // The slot of `key`, made (evicting the oldest) if there is none.
+  GraphSlot& slot(const std::vector<double>& key) {
+    for (GraphSlot& g : graphs)
+      if (g.key == key) return g;
+    if (graphs.size() >= kGraphSlots) {
+      graphs.front().drop();
+      graphs.erase(graphs.begin());
+    }
+    graphs.emplace_back();
+    graphs.back().key = key;
+    return graphs.back();
   }
   size_t bytes() const {
-    return table.n + pair.n + gam.n + D.n + F.n + wnsga2.n + f2.n;
+    return table.n + pair.n + gam.n + D.n + F.n + wnsga2.n + f2.n + f2ref.n;
   }
   void release() {
     drop_graph();
     own.release();
-    for (DevBuf* b : {&table, &pair, &gam, &D, &F, &wnsga2, &f2, &dang, &conv}) b->release();
+    for (DevBuf* b : {&table, &pair, &gam, &D, &F, &wnsga2, &f2, &dang, &conv, &f2ref})
+      b->release();
   }
 };
 
@@ -932,14 +877,14 @@ void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
     return;
   }
   const std::vector<void*> sig = buffer_signature(C);
-  if (!Pb.graph || Pb.graph_key != key || Pb.graph_sig != sig) {
-    Pb.drop_graph();
-    if (Pb.last_sig != sig || Pb.graph_key != key) {
+  trhepd_problem::GraphSlot& gs = Pb.slot(key);
+  if (!gs.exec || gs.sig != sig) {
+    gs.drop();
+    if (gs.last_sig != sig) {
       // buffers may grow on this solve: run it directly, capture the next one
       RunState R;
-      Pb.graph_key = key;
       run_device(C, Pb, precision, R);
-      Pb.last_sig = buffer_signature(C);
+      gs.last_sig = buffer_signature(C);
       finish_host(C, Pb, R);
       return;
     }
@@ -960,15 +905,38 @@ void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
     cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
     cudaGraphDestroy(g);
     CK(e);
-    Pb.graph = ex;
-    Pb.graph_sig = sig;
-    Pb.graph_run = R;
+    gs.exec = ex;
+    gs.sig = sig;
+    gs.run = R;
   }
-  RunState R = Pb.graph_run;
+  RunState R = gs.run;
   CK(cudaEventRecord(C->ev0, C->stream));
-  CK(cudaGraphLaunch(Pb.graph, C->stream));
+  CK(cudaGraphLaunch(gs.exec, C->stream));
   CK(cudaEventRecord(C->ev1, C->stream));
   finish_host(C, Pb, R);
+}
+
+// A solve in `precision`; with TRHEPD_OPT_VALIDATE set, a split-form solve is
+// preceded by the FP64 solve of the same resident problem and followed by a
+// per-curve comparison on the device (the statistics stay those of the split solve).
+void run_checked(trhepd_context* C, trhepd_problem& Pb, int precision) {
+  C->curve_err.clear();
+  if (!C->validate || precision == TRHEPD_FP64) {
+    run(C, Pb, precision);
+    return;
+  }
+  const size_t bytes = (size_t)Pb.nang * Pb.n * sizeof(double);
+  run(C, Pb, TRHEPD_FP64);
+  double* ref = (double*)Pb.f2ref.ensure(bytes);
+  CK(cudaMemcpyAsync(ref, Pb.f2.p, bytes, cudaMemcpyDeviceToDevice, C->stream));
+  run(C, Pb, precision);
+  double* e = (double*)C->cerr.ensure((size_t)3 * Pb.nang * sizeof(double));
+  launch_curve_errors(Pb.f2.as<double>(), ref, Pb.nang, Pb.n, e, C->stream);
+  CK(cudaGetLastError());
+  C->curve_err.resize((size_t)3 * Pb.nang);
+  CK(cudaMemcpyAsync(C->curve_err.data(), e, C->curve_err.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, C->stream));
+  CK(cudaStreamSynchronize(C->stream));
 }
 
 // Problems that can be integrated as one stacked solve: same beams and beam-pair
@@ -1161,7 +1129,7 @@ void solve(trhepd_context* C, const SolveArgs& A, int precision, double* f2_out,
   trhepd_problem Pb;
   try {
     prepare(C, A, Pb);
-    run(C, Pb, precision);
+    run_checked(C, Pb, precision);
     fetch(C, Pb, f2_out, angle_out);
   } catch (...) {
     cudaStreamSynchronize(C->stream);
@@ -1580,7 +1548,8 @@ void trhepd_destroy(trhepd_context* c) {
   DevBuf* all[] = {&c->asf, &c->b, &c->dchg, &c->ghk, &c->depth, &c->table, &c->pair,
                    &c->Q0, &c->Q1, &c->P, &c->V, &c->D, &c->gam, &c->F, &c->flags, &c->dval,
                    &c->gj, &c->f2, &c->wnsga2, &c->status, &c->split, &c->sgh, &c->sgk,
-                   &c->simg, &c->snimg, &c->sst, &c->cva, &c->cvf, &c->cvo};
+                   &c->simg, &c->snimg, &c->sst, &c->cva, &c->cvf, &c->cvo, &c->cerr,
+                   &c->cref};
   for (DevBuf* b : all) b->release();
   for (int p = 0; p < 3; ++p) {
     c->z[p].release();
@@ -1643,6 +1612,9 @@ int trhepd_set_option(trhepd_context* c, int option, double value) {
     case TRHEPD_OPT_FUSED_MAX_N:
       if (value < 0) return fail(c, TRHEPD_EINVAL, "fused beam limit must be >= 0");
       c->fused_max_n = (int)value;
+      return TRHEPD_OK;
+    case TRHEPD_OPT_VALIDATE:
+      c->validate = value != 0.0;
       return TRHEPD_OK;
   }
   return fail(c, TRHEPD_EINVAL, "unknown option");
@@ -1757,7 +1729,37 @@ int trhepd_problem_solve(trhepd_context* ctx, trhepd_problem* pb, int precision)
     if (!pb) throw std::invalid_argument("null problem");
     if (!valid_precision(precision))
       throw std::invalid_argument("unknown precision form");
-    run(ctx, *pb, precision);
+    run_checked(ctx, *pb, precision);
+  });
+}
+
+int trhepd_last_curve_errors(const trhepd_context* ctx, double* out, int n) {
+  if (!ctx || !out) return TRHEPD_EINVAL;
+  if (ctx->curve_err.empty() || (size_t)n < ctx->curve_err.size()) return TRHEPD_EINVAL;
+  std::copy(ctx->curve_err.begin(), ctx->curve_err.end(), out);
+  return TRHEPD_OK;
+}
+
+int trhepd_problem_compare(trhepd_context* ctx, trhepd_problem* pb, const double* ref_f2,
+                           double* out) {
+  return guarded(ctx, [&] {
+    if (!pb || !ref_f2 || !out) throw std::invalid_argument("null argument");
+    cudaStream_t st = ctx->stream;
+    const size_t rows = (size_t)pb->nang, nb = (size_t)pb->n;
+    double* dref = (double*)ctx->cref.ensure(rows * nb * sizeof(double));
+    CK(cudaMemcpyAsync(dref, ref_f2, rows * nb * sizeof(double), cudaMemcpyHostToDevice, st));
+    double* e = (double*)ctx->cerr.ensure(2 * rows * sizeof(double));
+    launch_curve_distance(pb->f2.as<double>(), dref, (int)rows, (int)nb, e, st);
+    CK(cudaGetLastError());
+    std::vector<double> h(2 * rows);
+    CK(cudaMemcpyAsync(h.data(), e, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double mm = 0.0;
+    for (size_t a = 0; a < rows; ++a) mm = std::max(mm, h[2 * a + 1]);
+    for (size_t a = 0; a < rows; ++a) {
+      out[2 * a] = h[2 * a] / mm;
+      out[2 * a + 1] = h[2 * a] / h[2 * a + 1];
+    }
   });
 }
 

@@ -245,13 +245,10 @@ def jitter(base: Structure, sigma: float, seed: int) -> Structure:
     """A candidate surface: the base structure with surface atoms moved by N(0, sigma) A."""
     rng = np.random.default_rng(seed)
     s = dataclasses.replace(base)
-    cell_x = s.msa if s.msa else 1
-    cell_y = s.nsb if s.nsb else 1
     s.surf_atoms = [dataclasses.replace(
         a, x=a.x + float(rng.normal(0, sigma)) / (s.aa),
         y=a.y + float(rng.normal(0, sigma)) / (s.bb),
         z=a.z + float(rng.normal(0, sigma))) for a in base.surf_atoms]
-    del cell_x, cell_y
     return s
 
 

@@ -26,6 +26,7 @@ OPT_SPLIT_KERNEL = 5
 OPT_GRAPHS = 6
 OPT_FUSED_MAX_N = 7
 OPT_STREAM_PRIORITY = 8
+OPT_VALIDATE = 9
 
 # every symbol include/trhepd_b200.h declares
 EXPORTS = [
@@ -34,7 +35,8 @@ EXPORTS = [
     "trhepd_potential_table", "trhepd_srfref", "trhepd_surf_run", "trhepd_surf_load",
     "trhepd_surf_free", "trhepd_surf_views", "trhepd_problem_create", "trhepd_problem_solve", "trhepd_batch_solve", "trhepd_rocking_convolution", "trhepd_problem_convolve",
     "trhepd_problem_fetch", "trhepd_problem_info", "trhepd_problem_destroy",
-    "trhepd_potential_table_noalloc", "trhepd_bulk_run",
+    "trhepd_potential_table_noalloc", "trhepd_bulk_run", "trhepd_last_curve_errors",
+    "trhepd_problem_compare",
 ]
 
 
@@ -115,6 +117,8 @@ def load():
     L.trhepd_rocking_convolution.argtypes = [_P, _P, _P, _I, _I, _I, _D, _P]
     L.trhepd_problem_convolve.argtypes = [_P, _P, _D, _P]
     L.trhepd_problem_fetch.argtypes = [_P, _P, _P, _P]
+    L.trhepd_last_curve_errors.argtypes = [_P, _P, _I]
+    L.trhepd_problem_compare.argtypes = [_P, _P, _P, _P]
     L.trhepd_problem_info.argtypes = [_P, _P, _I]
     L.trhepd_potential_table_noalloc.argtypes = [_P, _I, _I, _D, _P, _P, _P]
     L.trhepd_bulk_run.argtypes = [_P, ctypes.c_char_p, ctypes.c_char_p, _P]
@@ -166,6 +170,13 @@ class Context:
                 "stage_kernel_ms": float(out[4]), "launches": int(out[5]),
                 "renorm_launches": int(out[6]), "tensor_kernel_ms": float(out[7]),
                 "renorm_ms": float(out[8])}
+
+    def last_curve_errors(self, nangles: int) -> np.ndarray:
+        """(nangles, 3) per-curve errors of the last validated split solve: max relative
+        error over every spot, max error over the curve maximum, the curve maximum."""
+        out = np.zeros(3 * nangles)
+        self._check(self._L.trhepd_last_curve_errors(self._h, out.ctypes.data, out.size))
+        return out.reshape(nangles, 3)
 
     def surf_run(self, bulkp, surf, dz2: float, int_method: int = 5, precision: int = FP64,
                  out_path=None):

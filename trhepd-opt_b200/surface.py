@@ -114,6 +114,17 @@ class ResidentProblem:
                                                      ang.ctypes.data))
         return ang, f2
 
+    def compare(self, ref_f2):
+        """compare.py's per-angle metric between the solved curves and `ref_f2`
+        (nangles, nb), reduced on the device: (nangles, 2) = (e0 / max n0, e0 / n0)."""
+        ref = np.ascontiguousarray(ref_f2, dtype=np.float64)
+        if ref.shape != (self.nangles, self.nb):
+            raise ValueError(f"reference curves must be {(self.nangles, self.nb)}")
+        out = np.zeros((self.nangles, 2))
+        self.ctx._check(self._L.trhepd_problem_compare(self.ctx._h, self._h, ref.ctypes.data,
+                                                       out.ctypes.data))
+        return out
+
     def convolve(self, omega: float = 0.5):
         """The solved intensities convolved on the device (make_convolution.py)."""
         out = np.zeros((self.nangles, self.nb))
