@@ -38,7 +38,7 @@ enum trhepd_precision {
   TRHEPD_SPLIT_BF16 = 1,  /* stage products from BF16 slices on tcgen05 (FP32 accumulators),
                              FP64 elsewhere */
   TRHEPD_SPLIT_INT8 = 2   /* stage products from signed 8-bit digit slices on tcgen05
-                             (exact INT32 accumulators, 3 or 4 slices), FP64 elsewhere */
+                             (exact INT32 accumulators, 3 to 6 slices), FP64 elsewhere */
 };
 
 /* options (trhepd_set_option) */
@@ -47,7 +47,8 @@ enum trhepd_option {
                                    1: growth bound: every floor(tau / ((kappa_max + 1) dz))
                                       slices, kappa_max the largest evanescent decay constant */
   TRHEPD_OPT_RENORM_TAU = 2,    /* growth bound ln(cond) between renormalisations (policy 1) */
-  TRHEPD_OPT_SPLIT_SLICES = 3,  /* slices per operand in the split forms (BF16 3..5, INT8 3..4) */
+  TRHEPD_OPT_SPLIT_SLICES = 3,  /* slices per operand in the split forms (BF16 3..5, INT8 3..6;
+                                   each INT8 slice adds 8 bits: 31 at 4, 47 at 6) */
   TRHEPD_OPT_PROFILE = 4,       /* nonzero: time every stage-product launch with CUDA events */
   TRHEPD_OPT_SPLIT_KERNEL = 5,  /* BF16 split kernel: 0 persistent, one CTA per SM, epilogue of
                                    a tile overlapped with the next tile's MMAs (default);

@@ -1,9 +1,12 @@
 """Split-precision forms (BF16 or INT8 digit slices on tcgen05, FP64 elsewhere)
-against the plain FP64 form and the oracle.  Target: every spot within 1e-6 of its row
-maximum and within 1e-5 relative on spots >= 1e-3 of the row maximum, with 4
-slices.  (At 2000 chained slices the FP64 result itself moves by ~4e-7 relative
-on weak spots when only the renormalisation points change, so weaker spots are
-bounded relative to the row maximum.)"""
+against the plain FP64 form and the reference's output, 5 slices per operand.
+
+Bars, relative on every spot (a spot that is exactly zero in FP64 must be zero):
+* INT8 (exact INT32 accumulation of 39-bit digit products): 1e-6, the target of
+  the split form;
+* BF16 (its slice pairs of weight below 2^-16 accumulate in FP32, which caps it
+  near 5e-6 at N = 521): 1e-5.
+"""
 from __future__ import annotations
 
 import numpy as np
@@ -12,6 +15,15 @@ import pytest
 from conftest import spot_errors
 
 pytestmark = pytest.mark.gpu
+
+EVERY_SPOT = {1: 1e-5, 2: 1e-6}   # precision form -> every-spot relative bound
+
+
+def every_spot_rel(got, ref):
+    got, ref = np.asarray(got), np.asarray(ref)
+    d = np.abs(got - ref)
+    m = np.abs(ref)
+    return float(np.where(m > 0, d / np.where(m > 0, m, 1.0), np.where(d > 0, np.inf, 0.0)).max())
 
 
 @pytest.fixture(scope="module")
@@ -50,17 +62,15 @@ def test_split_matches_fp64(ctx, tmp_path, case, form):
     rp.solve(native.FP64)
     _, ref = rp.fetch()
     precision, variant = FORMS[form]
-    ctx.set_option(native.OPT_SPLIT_SLICES, 4)
+    ctx.set_option(native.OPT_SPLIT_SLICES, 5)
     ctx.set_option(native.OPT_SPLIT_KERNEL, variant)
     try:
         rp.solve(precision)
         _, got = rp.fetch()
     finally:
         ctx.set_option(native.OPT_SPLIT_KERNEL, 0)
-    abs_err, _ = spot_errors(got, ref)
-    _, rel_big = spot_errors(got, ref, floor=1e-3)
-    assert abs_err <= 1e-6, abs_err
-    assert rel_big <= 1e-5, rel_big
+    rel = every_spot_rel(got, ref)
+    assert rel <= EVERY_SPOT[precision], rel
 
 
 @pytest.mark.parametrize("precision", [1, 2], ids=["bf16", "int8"])
@@ -69,13 +79,13 @@ def test_split_against_reference_output(ctx, golden, precision):
     from trhepd_opt_b200 import native
     d = golden / "test47"
     ref = np.load(d / "perf-5-0.22.npz")
-    ctx.set_option(native.OPT_SPLIT_SLICES, 4)
+    ctx.set_option(native.OPT_SPLIT_SLICES, 5)
     f2, _ = ctx.surf_run(d / "bulkP.b", d / "surf.txt", 0.22, 5, precision)
-    abs_err, _ = spot_errors(f2, ref["f2"])
-    assert abs_err <= 1e-6, abs_err
+    rel = every_spot_rel(f2, ref["f2"])
+    assert rel <= EVERY_SPOT[precision], rel
 
 
-@pytest.mark.parametrize("precision,slices", [(1, (3, 4, 5)), (2, (3, 4))],
+@pytest.mark.parametrize("precision,slices", [(1, (3, 4, 5)), (2, (3, 4, 5, 6))],
                          ids=["bf16", "int8"])
 def test_more_slices_is_more_accurate(ctx, tmp_path, precision, slices):
     from trhepd_opt_b200 import generator, native
@@ -92,15 +102,18 @@ def test_more_slices_is_more_accurate(ctx, tmp_path, precision, slices):
     assert all(a > b for a, b in zip(errs, errs[1:])), errs
 
 
-def test_int8_rejects_five_slices(ctx, tmp_path):
-    """Five INT8 levels would need 640 tensor-memory columns: a clear error, and
-    the context stays usable."""
+def test_split_slice_limits(ctx, tmp_path):
+    """INT8 takes 3 to 6 digit slices, BF16 3 to 5 (its FP32 accumulators gain
+    nothing from a sixth): clear errors outside, and the context stays usable."""
     from trhepd_opt_b200 import generator, native
     sp, rp = _resident(ctx, tmp_path, generator.small23())
-    ctx.set_option(native.OPT_SPLIT_SLICES, 5)
+    with pytest.raises(native.TrhepdError):
+        ctx.set_option(native.OPT_SPLIT_SLICES, 7)
+    ctx.set_option(native.OPT_SPLIT_SLICES, 6)
     try:
         with pytest.raises(native.TrhepdError):
-            rp.solve(native.SPLIT_INT8)
+            rp.solve(native.SPLIT_BF16)
+        rp.solve(native.SPLIT_INT8)
     finally:
         ctx.set_option(native.OPT_SPLIT_SLICES, 4)
     rp.solve(native.SPLIT_INT8)
@@ -116,8 +129,8 @@ def test_split_other_integrators(ctx, tmp_path, method, precision):
     sp, rp = _resident(ctx, tmp_path, s)
     rp.solve(native.FP64)
     _, ref = rp.fetch()
-    ctx.set_option(native.OPT_SPLIT_SLICES, 4)
+    ctx.set_option(native.OPT_SPLIT_SLICES, 5)
     rp.solve(precision)
     _, got = rp.fetch()
-    abs_err, _ = spot_errors(got, ref)
-    assert abs_err <= 1e-6, abs_err
+    rel = every_spot_rel(got, ref)
+    assert rel <= EVERY_SPOT[precision], rel

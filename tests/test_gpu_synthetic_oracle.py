@@ -9,11 +9,13 @@ Bars (every call through the C ABI):
 * plain FP64 form, same renormalisation schedule as the oracle: 1e-9 relative on
   spots >= 1e-6 of the row maximum and 1e-10 of the row maximum on every spot;
   the raw every-spot relative maximum is reported beside it;
-* split forms (INT8 and BF16 digit slices, 4 per operand): every spot within
-  SPLIT_REL relative of the oracle, except where the FP64 rounding floor of the
-  case (the oracle under its two renormalisation schedules, which differ by
-  rounding only) is itself larger: there the bound is FLOOR_FACTOR x that floor
-  per spot.
+* split forms, 5 digit slices per operand: every spot within SPLIT_REL[form]
+  relative of the oracle (INT8 1e-6, the target of the split form; BF16 1e-5,
+  its FP32 accumulators cap it near 5e-6), except where the FP64 rounding floor
+  of the case (the oracle under its two renormalisation schedules, which differ
+  by rounding only) is itself larger: there the bound is FLOOR_FACTOR x that
+  floor per spot (the floor measured on dense521 is 1.5e-11, so the bound stays
+  SPLIT_REL there).
 """
 from __future__ import annotations
 
@@ -27,7 +29,7 @@ from conftest import GOLDEN, spot_errors
 pytestmark = pytest.mark.gpu
 
 SYN = GOLDEN / "synthetic"
-SPLIT_REL = 1e-6
+SPLIT_REL = {1: 1e-5, 2: 1e-6}   # precision form (BF16, INT8) -> every-spot bound
 FLOOR_FACTOR = 4.0
 
 
@@ -45,7 +47,7 @@ def ctx():
     from trhepd_opt_b200 import build, native
     build.build()
     c = native.Context(0)
-    c.set_option(native.OPT_SPLIT_SLICES, 4)
+    c.set_option(native.OPT_SPLIT_SLICES, 5)
     yield c
     c.close()
 
@@ -122,13 +124,13 @@ def test_fp64_matches_oracle(ctx, tmp_path_factory, name, policy):
     assert rel_err <= 1e-9, rel_err
 
 
-def split_bound(fx):
-    """Per-spot bound of the split forms: SPLIT_REL, or FLOOR_FACTOR x the FP64
+def split_bound(fx, precision):
+    """Per-spot bound of a split form: SPLIT_REL, or FLOOR_FACTOR x the FP64
     floor where the oracle's two schedules already differ by more."""
     if "f2_growth" not in fx:
-        return np.full(fx["f2"].shape, SPLIT_REL)
+        return np.full(fx["f2"].shape, SPLIT_REL[precision])
     floor = every_spot_rel(fx["f2_growth"], fx["f2"])
-    return np.maximum(SPLIT_REL, FLOOR_FACTOR * floor)
+    return np.maximum(SPLIT_REL[precision], FLOOR_FACTOR * floor)
 
 
 CASES_SPLIT = [(n, p) for n in ("batch47", "dense521") for p in (1, 2)]
@@ -144,7 +146,7 @@ def test_split_every_spot_matches_oracle(ctx, tmp_path_factory, name, precision)
     got, _ = solve_rows(ctx, rp, fx, precision, policy)
     report(f"{name} split {precision} policy {policy}", got, ref)
     rel = every_spot_rel(got, ref)
-    bound = split_bound(fx)
+    bound = split_bound(fx, precision)
     worst = np.unravel_index(np.argmax(rel / bound), rel.shape)
     assert (rel <= bound).all(), (float(rel[worst]), float(bound[worst]), worst)
 
@@ -174,6 +176,7 @@ def test_curve_errors_through_abi(ctx, tmp_path_factory):
     np.testing.assert_allclose(err[:, 1], np.abs(f8 - f64).max(axis=1) / rowmax, rtol=1e-12)
     print(f"dense521 int8 per-curve max rel err: max {err[:, 0].max():.3e}, "
           f"median {np.median(err[:, 0]):.3e}")
+    assert err[:, 0].max() <= SPLIT_REL[2]  # every curve meets the split form's bar
     # the FP64 leg of a validated solve is the plain FP64 solve
     abs_err, rel_err, _ = report("dense521 fp64 (validation leg)", f64[fx["idx"]],
                                  fx["f2_growth"])
@@ -187,15 +190,16 @@ def test_curve_errors_through_abi(ctx, tmp_path_factory):
 @pytest.mark.parametrize("precision", [1, 2], ids=["bf16", "int8"])
 def test_split_on_reference_n521(ctx, golden, precision):
     """The split forms on the reference's own N=521 case (test521, sp4, 0.33 A
-    slices, one angle) against its committed output."""
+    slices, one angle) against its committed output: thick slices with
+    evanescent growth of ~1e3 per stage make this the hardest case for the digit
+    products (INT8 every spot 9.4e-7 at 5 slices, 4e-9 at 6)."""
     from trhepd_opt_b200 import native
     d = golden / "test521"
     ref = np.load(d / "perf-5-0.33.npz")["f2"]
     ctx.set_option(native.OPT_RENORM_POLICY, 0)
     f2, _ = ctx.surf_run(d / "bulkP.b", d / "surf.txt", 0.33, 5, precision)
     abs_err, rel_err, raw = report(f"test521 split {precision}", f2, ref)
-    assert abs_err <= 1e-8, abs_err
-    assert rel_err <= SPLIT_REL, rel_err
+    assert raw <= SPLIT_REL[precision], raw
 
 
 @pytest.mark.parametrize("name", ["uneven95", "uneven191"])
@@ -210,6 +214,6 @@ def test_stacked_batch_matches_oracle(ctx, tmp_path_factory, name):
         for p in (rp, rp2):
             ang, f2 = p.fetch()
             rel = every_spot_rel(f2[fx["idx"]], fx["f2"])
-            assert (rel <= SPLIT_REL).all(), float(rel.max())
+            assert (rel <= SPLIT_REL[2]).all(), float(rel.max())
     finally:
         rp2.close()

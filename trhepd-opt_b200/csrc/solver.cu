@@ -91,7 +91,7 @@ struct trhepd_context {
   std::string err;
   int renorm_policy = 0;
   double renorm_tau = std::log(1e3);
-  int split_slices = 4;
+  int split_slices = 5;           // 5 INT8 digits (39 bits) meet 1e-6 per spot at N = 521
   int split_variant = kSplitPersistent;
   int profile = 0;               // 1: time every stage-product launch with events
   int graphs = 1;                // 1: replay resident solves from a captured CUDA graph
@@ -444,8 +444,8 @@ void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_m
   R.status = (unsigned*)W.status->ensure(16);
   R.split = precision == TRHEPD_SPLIT_BF16 || precision == TRHEPD_SPLIT_INT8;
   R.split_variant = (precision == TRHEPD_SPLIT_INT8) ? kSplitInt8 : C->split_variant;
-  if (precision == TRHEPD_SPLIT_INT8 && C->split_slices > 4)
-    throw std::invalid_argument("the INT8 split form takes 3 or 4 slices");
+  if (precision == TRHEPD_SPLIT_BF16 && C->split_slices > 5)
+    throw std::invalid_argument("the BF16 split form takes 3 to 5 slices");
   if (R.split)
     R.sw = split_workspace_carve(
         W.split->ensure(split_workspace_bytes(nang, n, C->split_slices, R.nprob)), nang, n,
@@ -1578,7 +1578,7 @@ int trhepd_set_option(trhepd_context* c, int option, double value) {
       c->renorm_tau = value;
       return TRHEPD_OK;
     case TRHEPD_OPT_SPLIT_SLICES:
-      if (value < 3 || value > 5) return fail(c, TRHEPD_EINVAL, "split slices must be 3..5");
+      if (value < 3 || value > 6) return fail(c, TRHEPD_EINVAL, "split slices must be 3..6");
       c->split_slices = (int)value;
       return TRHEPD_OK;
     case TRHEPD_OPT_PROFILE:

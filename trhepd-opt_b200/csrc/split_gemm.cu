@@ -34,6 +34,7 @@
 #include <string>
 
 #include "kernels.h"
+#include "launch_attr.h"
 #include "split_gemm.h"
 
 namespace trhepd {
@@ -728,28 +729,75 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 // and written in balanced base 256, X = sum_s d_s 256^(S-1-s), d_s in [-128, 127]
 // for s >= 1; the headroom keeps |d_0| <= 127.  So x = 2^(e-7) sum_s d_s 2^-8s up
 // to half a unit of the last digit.  The slice pairs with s + t = L go to INT32
-// accumulator L (L < S, S*128 TMEM columns); every sum is exact (|acc_L| <=
-// S * 2^14 * K, below 2^31 for K < 32768), and the epilogue forms
-// sum_L 2^-8L acc_L in FP64 and scales it by 2^(e_r + f_j - 14).
+// accumulator L (L < S, S x NT(S) TMEM columns); every sum is exact (|acc_L| <=
+// S * 2^14 * K, below 2^31 for K < 16384), and the epilogue forms
+// sum_L 2^-8L acc_L in FP64 and scales it by 2^(e_r + f_j - 14).  S = 3..6: each
+// digit adds 8 bits (31 bits at S = 4, 47 at S = 6); tiles narrow from 128 to 96
+// and 80 real columns at S = 5, 6 so that the S levels fit the TMEM.
 namespace i8 {
 constexpr int BK = 64;                     // int8 k per pipeline stage (64-byte rows)
+constexpr int STAGES = 2;                  // pipeline stages of S A- and S B-slices
 constexpr int A_SLICE_BYTES = BM * BK;     // 8 KB
-constexpr int B_SLICE_BYTES = NT * BK;     // 8 KB
-// Two 64 KB stages at S = 4: the third stage's 64 KB serve better as L1 cache for
-// the epilogue's state loads (measured at N = 521: 0.52 vs 0.56 ms per launch
-// together with the L1-bypassing loads below).
-__host__ __device__ constexpr int stages_for(int S) { return S <= 3 ? 4 : 2; }
+// Real output columns per tile: the S accumulator levels of a tile must fit the
+// 512 TMEM columns (S * NT <= 512), and NT is a multiple of 16 for M = 128.
+__host__ __device__ constexpr int nt_for(int S) { return S <= 4 ? 128 : (S == 5 ? 96 : 80); }
+__host__ __device__ constexpr int nc_for(int S) { return nt_for(S) / 2; }
+__host__ __device__ constexpr int b_slice_bytes(int S) { return nt_for(S) * BK; }
 __host__ __device__ constexpr size_t stage_bytes(int S) {
-  return (size_t)S * (A_SLICE_BYTES + B_SLICE_BYTES);
+  return (size_t)S * (A_SLICE_BYTES + b_slice_bytes(S));
 }
-inline size_t smem_bytes(int S) { return 1024 + stages_for(S) * stage_bytes(S); }
+// Epilogue tables: the per-angle diagonal D of the angles a tile's rows belong to,
+// at most kDTabBytes per tile (two buffers, so that filling the next tile's table
+// never overlaps reads of the current one).
+constexpr int kDTabBytes = 4096;
+// Epilogue load ring: the RKN update reads every state entry (Q and P) once, so the
+// epilogue warps stream them from HBM into shared memory with cp.async several
+// update steps ahead of their use, across tile boundaries, holding no registers for
+// the loads in flight.  One slot = Q and P of each epilogue lane's two rows of one
+// step (16 bytes each): 16 KB.  As many slots as the shared memory left beside
+// the pipeline allows.
+constexpr int kRingItems = 4;
+constexpr size_t kSlotBytes = (size_t)kRingItems * 8 /* epilogue warps */ * 32 * 16;
+constexpr size_t kSmemCap = 232448 - 512;  // per-block opt-in limit, less static shared
+__host__ __device__ constexpr int ring_slots(int S) {
+  return (int)((kSmemCap - 1024 - STAGES * stage_bytes(S) - 2 * kDTabBytes) / kSlotBytes) > 6
+             ? 6
+             : (int)((kSmemCap - 1024 - STAGES * stage_bytes(S) - 2 * kDTabBytes) / kSlotBytes);
+}
+inline size_t smem_bytes(int S) {
+  return 1024 + STAGES * stage_bytes(S) + 2 * kDTabBytes + ring_slots(S) * kSlotBytes;
+}
+// Steps ahead at which the epilogue loads the stage matrix entries it needs
+// (registers: the narrower tiles of S = 5, 6 leave room for more).
+__host__ __device__ constexpr int v_ahead(int S) { return S <= 4 ? 1 : (S == 5 ? 2 : 3); }
+static_assert(ring_slots(3) >= 3 && ring_slots(4) >= 3 && ring_slots(5) >= 3 &&
+                  ring_slots(6) >= 3,
+              "epilogue ring needs at least three slots");
 }  // namespace i8
 
-// Instruction descriptor: S8 x S8 -> S32, both K-major, M = 128, N = NT.
-__host__ __device__ constexpr uint32_t instr_desc_i8() {
+// 16-byte global -> shared copy, cached in L2 only (the state is read once).
+__device__ __forceinline__ void cp_async_16(uint32_t saddr, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+// An INT32 accumulator value as a double without the conversion unit: the bits
+// 0x43380000:(a + 2^31) form 2^52 + 2^51 + 2^31 + a exactly, from which the
+// constant is subtracted exactly (magic-number conversion).
+__device__ __forceinline__ double i32_to_f64(uint32_t a) {
+  return __hiloint2double(0x43380000, (int)(a ^ 0x80000000u)) - 6755401588539392.0;
+}
+
+// Instruction descriptor: S8 x S8 -> S32, both K-major, M = 128, N = NT(S).
+__host__ __device__ constexpr uint32_t instr_desc_i8(int nt) {
   return (2u << 4)                      // D format S32
          | (1u << 7) | (1u << 10)       // A, B format S8
-         | ((uint32_t)(NT >> 3) << 17)  // N
+         | ((uint32_t)(nt >> 3) << 17)  // N
          | ((uint32_t)(BM >> 4) << 24); // M
 }
 __device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
@@ -763,18 +811,30 @@ __device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint6
 }
 
 // Balanced base-256 digits of X = rint(x * scale), scale = 2^(7 - e + 8(S-1)),
-// most significant first.  |X| < 2^(7 + 8(S-1)) fits 32 bits for S <= 4.
+// most significant first.  |X| < 2^(7 + 8(S-1)): 32-bit arithmetic for S <= 4,
+// 64-bit for S = 5, 6 (|X| < 2^47, exact in double before the rounding).
 template <int S>
 __device__ __forceinline__ void digits_i8(double x, double scale, int* d) {
-  static_assert(S <= 4, "32-bit digit arithmetic");
-  int X = __double2int_rn(x * scale);
+  static_assert(S <= 6, "at most six digits");
+  if constexpr (S <= 4) {
+    int X = __double2int_rn(x * scale);
 #pragma unroll
-  for (int s = S - 1; s >= 1; --s) {
-    const int lo = ((X + 128) & 255) - 128;
-    d[s] = lo;
-    X = (X - lo) >> 8;
+    for (int s = S - 1; s >= 1; --s) {
+      const int lo = ((X + 128) & 255) - 128;
+      d[s] = lo;
+      X = (X - lo) >> 8;
+    }
+    d[0] = X;
+  } else {
+    long long X = __double2ll_rn(x * scale);
+#pragma unroll
+    for (int s = S - 1; s >= 1; --s) {
+      const int lo = (int)((X + 128) & 255) - 128;
+      d[s] = lo;
+      X = (X - lo) >> 8;
+    }
+    d[0] = (int)X;
   }
-  d[0] = X;
 }
 __device__ __forceinline__ double digit_scale(int e, int S) {
   return pow2(7 - e + 8 * (S - 1));
@@ -861,21 +921,28 @@ __global__ void __launch_bounds__(128) k_slice_cols_i8(const cd* __restrict__ V,
   }
 }
 
-// Streaming load of one state entry, cached in L2 only: every entry is read once.
-__device__ __forceinline__ cd ldcg_cd(const cd* a) {
-  const double2 v = __ldcg(reinterpret_cast<const double2*>(a));
-  return cd{v.x, v.y};
-}
-
-// Persistent INT8 stage product: the warp roles, barriers, register split and the
-// register-held drain of k_split_gemm_p, with S INT32 accumulators.
+// Persistent INT8 stage product: one CTA per SM walks the tiles (static stride);
+// warp 0 issues TMA, warp 1 the MMAs of every slice pair (s, t) with s + t < S into
+// accumulator level s + t, warps 2-3 idle; eight epilogue warps (two per TMEM lane
+// quadrant, one per column half) drain a finished tile into registers, give the
+// TMEM back at once (the next tile's MMAs start) and perform the FP64 RKN update
+// from registers.  Tile: 128 stacked rows x NT(S) real columns; S levels x NT(S)
+// TMEM columns.  setmaxnreg splits the registers (control 40, epilogue 232).
 template <int S>
 __global__ void __launch_bounds__(P_THREADS, 1)
     k_split_gemm_i8(const __grid_constant__ CUtensorMap tmA,
                     const __grid_constant__ CUtensorMap tmB, EpiArgs ep, int nkb, int tiles_n,
-                    int tiles) {
-  static_assert(S * NT <= TMEM_COLS, "INT8 levels exceed the tensor memory");
-  constexpr int STAGES = i8::stages_for(S);
+                    int tiles, int dpitch) {
+  constexpr int NTS = i8::nt_for(S);          // real columns per tile
+  constexpr int NCS = NTS / 2;                // complex columns per tile
+  constexpr int G = NCS / 8;                  // 4-column groups per epilogue warp
+  constexpr int STEPS = 2 * G;                // update steps (g, h) per tile
+  constexpr int STAGES = i8::STAGES;
+  constexpr int RING = i8::ring_slots(S);
+  constexpr int AHEAD = RING - 1;             // ring steps in flight
+  constexpr int VA = i8::v_ahead(S);          // stage-matrix steps in flight
+  static_assert(S * NTS <= TMEM_COLS, "INT8 levels exceed the tensor memory");
+  static_assert(NCS % 8 == 0 && NTS % 16 == 0, "tile width");
   if (*(volatile unsigned*)ep.status & kStatusTimeout) return;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -885,6 +952,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
   __shared__ int abort_sh, issued_sh, consumed_sh;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t sbytes = i8::stage_bytes(S);
+  constexpr int BSL = i8::b_slice_bytes(S);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -920,7 +988,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
         bool stop = false;
         for (int tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x) {
           const int rt = tile / tiles_n, pb = rt / ep.tpp;
-          const int m0 = pb * ep.rows_b + (rt - pb * ep.tpp) * BM, n0 = (tile % tiles_n) * NT;
+          const int m0 = pb * ep.rows_b + (rt - pb * ep.tpp) * BM, n0 = (tile % tiles_n) * NTS;
           for (int kb = 0; kb < nkb; ++kb, ++g) {
             const int st = g % STAGES, round = g / STAGES;
             if (round > 0 && !mbar_wait(&empty_bar[st], (round - 1) & 1)) {
@@ -939,8 +1007,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 #pragma unroll
             for (int s = 0; s < S; ++s) {
               tma_load_3d(&tmA, &full_bar[st], sa + s * i8::A_SLICE_BYTES, kb * i8::BK, m0, s);
-              tma_load_3d(&tmB, &full_bar[st], sb + s * i8::B_SLICE_BYTES, kb * i8::BK, n0,
-                          pb * S + s);
+              tma_load_3d(&tmB, &full_bar[st], sb + s * BSL, kb * i8::BK, n0, pb * S + s);
             }
           }
         }
@@ -949,7 +1016,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     } else if (warp == 1) {
       // ---------------- MMA issuer
       if (lane == 0) {
-        const uint32_t idesc = instr_desc_i8();
+        const uint32_t idesc = instr_desc_i8(NTS);
         int g = 0, it = 0;
         bool stop = false;
         for (int tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x, ++it) {
@@ -981,8 +1048,8 @@ __global__ void __launch_bounds__(P_THREADS, 1)
                 for (int t = 0; t < S - s; ++t) {
                   const int L = s + t;
                   const uint64_t ad = sw64_desc(sa + s * i8::A_SLICE_BYTES + kk * 32);
-                  const uint64_t bd = sw64_desc(sb + t * i8::B_SLICE_BYTES + kk * 32);
-                  tc_mma_i8(tmem + L * NT, ad, bd, idesc, started[L] ? 1u : 0u);
+                  const uint64_t bd = sw64_desc(sb + t * BSL + kk * 32);
+                  tc_mma_i8(tmem + L * NTS, ad, bd, idesc, started[L] ? 1u : 0u);
                   started[L] = true;
                 }
               }
@@ -1000,18 +1067,83 @@ __global__ void __launch_bounds__(P_THREADS, 1)
   } else {
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(P_REG_EPI));
     // ---------------- epilogue warps 4..11
+    // Warp w (q4 = w & 3: TMEM lane quadrant, rows q4*32..+31 of the tile; half:
+    // complex columns half*NCS/2..+NCS/2-1) holds per lane rows t1, t1 + 8 of its
+    // 16-row blocks h = 0, 1 and complex column t0 of its 4-column groups g < G.
+    // Update step ls = 2g + h, STEPS per tile.
     const int q4 = warp & 3;
-    const int half = (warp - 4) >> 2;
+    const int ew = warp - 4;
+    const int half = ew >> 2;
     const int t0 = lane & 3, t1 = lane >> 2;
+    unsigned char* dtab_base = smem + STAGES * sbytes;
+    double2* ring = reinterpret_cast<double2*>(dtab_base + 2 * i8::kDTabBytes) + ew * 32 + lane;
+    const uint32_t ring_s = smem_u32(ring);
+    constexpr int kItem = P_EPI_WARPS * 32;               // double2 entries between items
+    constexpr uint32_t kItemBytes = kItem * 16;
+    // Row block of a tile for this warp: first row, end of its problem's rows,
+    // first complex column (rend = 0 past the last tile: nothing to load).
+    struct Geo {
+      int m0, rend, jh;
+    };
+    auto geometry = [&](int tile) {
+      Geo Gt{0, 0, 0};
+      if (tile < tiles) {
+        const int rt = tile / tiles_n, pb = rt / ep.tpp;
+        Gt.m0 = pb * ep.rows_b + (rt - pb * ep.tpp) * BM + q4 * 32;
+        Gt.rend = min(ep.rows, (pb + 1) * ep.rows_b);
+        Gt.jh = (tile % tiles_n) * NCS + half * (NCS / 2);
+      }
+      return Gt;
+    };
+    // cp.async the Q and P entries of step ls of the tile with geometry Gt into ring
+    // slot `slot` (one commit group per step, empty outside the matrix)
+    auto issue = [&](const Geo& Gt, int ls, int slot) {
+      const int g = ls >> 1, h = ls & 1;
+      const int j = Gt.jh + 4 * g + t0;
+      const uint32_t sa = ring_s + (uint32_t)slot * i8::kRingItems * kItemBytes;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int r = Gt.m0 + 16 * h + 8 * u + t1;
+        if (r < Gt.rend && j < ep.n) {
+          const size_t o = (size_t)r * ep.ld + j;
+          cp_async_16(sa + u * kItemBytes, ep.Q + o);
+          cp_async_16(sa + (2 + u) * kItemBytes, ep.P + o);
+        }
+      }
+      cp_async_commit();
+    };
+    int slot_rd = 0, slot_wr = 0;
+    auto next_slot = [](int s) { return s + 1 == RING ? 0 : s + 1; };
+    {
+      const Geo G0 = geometry(blockIdx.x);
+#pragma unroll
+      for (int q = 0; q < AHEAD; ++q) {
+        // the first tile of a CTA always has at least AHEAD steps
+        issue(G0, q, slot_wr);
+        slot_wr = next_slot(slot_wr);
+      }
+    }
     int it = 0;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
       const int rt = tile / tiles_n, pb = rt / ep.tpp;
       const int m0 = pb * ep.rows_b + (rt - pb * ep.tpp) * BM + q4 * 32;
       const int rend = min(ep.rows, (pb + 1) * ep.rows_b);  // this problem's rows end here
-      const int jh = (tile % tiles_n) * NC + half * (NC / 2);
+      const int j0 = (tile % tiles_n) * NCS;                 // first column of the tile
+      const int jh = j0 + half * (NCS / 2);
       const cd* Vb = ep.V + (size_t)pb * ep.vstride;
       const int* fcb = ep.fcol + (size_t)pb * ep.fstride;
       const cd vd = Vb[(size_t)ep.kpad * ep.ld];
+      const Geo Gc{m0, rend, jh}, Gn = geometry(tile + gridDim.x);
+      // D table of this tile: angles a0.. of its rows, columns j0 .. j0 + dpitch - 1
+      const int tm0 = m0 - q4 * 32;
+      const int a0 = tm0 / ep.n;
+      const int na = (min(tm0 + BM, rend) - 1) / ep.n - a0 + 1;
+      cd* dtab = reinterpret_cast<cd*>(dtab_base + (it & 1) * i8::kDTabBytes);
+      for (int e = (warp - 4) * 32 + lane; e < na * dpitch; e += P_EPI_WARPS * 32) {
+        const int a = e / dpitch, jl = e - a * dpitch;
+        const int j = j0 + jl;
+        dtab[e] = (j < ep.n) ? ep.D[(size_t)(a0 + a) * ep.ld + j] + vd : cd{0.0, 0.0};
+      }
       int er[2][2], ra[2][2], ri[2][2];
 #pragma unroll
       for (int h = 0; h < 2; ++h)
@@ -1027,37 +1159,59 @@ __global__ void __launch_bounds__(P_THREADS, 1)
             ri[h][u] = r - ra[h][u] * ep.n;
           }
         }
-      int fc[8];
+      int fc[G];
 #pragma unroll
-      for (int g = 0; g < 8; ++g) {
+      for (int g = 0; g < G; ++g) {
         const int j = jh + 4 * g + t0;
         fc[g] = (j < ep.n) ? fcb[j] : 0;
       }
+      cd qd[2][2];  // diagonal of each of this lane's rows (read while the MMAs run)
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int r = m0 + 16 * h + 8 * u + t1;
+          qd[h][u] = (r < rend) ? ep.Q[(size_t)r * ep.ld + ri[h][u]] : cd{0.0, 0.0};
+        }
+      // the stage matrix entries of the first VA steps
+      cd vq[VA][2];
+#pragma unroll
+      for (int ls = 0; ls < VA; ++ls) {
+        const int g = ls >> 1, h = ls & 1, j = jh + 4 * g + t0;
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int r = m0 + 16 * h + 8 * u + t1;
+          vq[ls][u] = (r < rend && j < ep.n) ? Vb[(size_t)ri[h][u] * ep.ld + j] : cd{0.0, 0.0};
+        }
+      }
       const bool ok = mbar_wait(&tfull, it & 1);
+      // also the barrier after which every epilogue warp sees this tile's D table
       if (epi_any(!ok)) {
         if (!ok) atomicOr(ep.status, kStatusTimeout);
         abort_sh = 1;
         break;
       }
       tc_fence_after();
-      cd vals[8][2][2];
+      // drain: each level's INT32 sums as exact doubles, combined by Horner in
+      // powers of 2^-8, then scaled by 2^(e_r + f_j - 14)
+      cd vals[G][2][2];
 #pragma unroll
-      for (int g = 0; g < 8; ++g)
+      for (int g = 0; g < G; ++g)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const uint32_t taddr = tmem + ((uint32_t)(q4 * 32 + 16 * h) << 16) +
-                                 (uint32_t)(2 * (half * (NC / 2) + 4 * g));
+                                 (uint32_t)(2 * (half * (NCS / 2) + 4 * g));
           uint32_t a[S][4];
 #pragma unroll
-          for (int L = 0; L < S; ++L) tmem_ld_16x256(taddr + L * NT, a[L]);
+          for (int L = 0; L < S; ++L) tmem_ld_16x256(taddr + L * NTS, a[L]);
           tmem_wait_ld();
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
-            double re = (double)(int)a[S - 1][2 * u], im = (double)(int)a[S - 1][2 * u + 1];
+            double re = i32_to_f64(a[S - 1][2 * u]), im = i32_to_f64(a[S - 1][2 * u + 1]);
 #pragma unroll
             for (int L = S - 2; L >= 0; --L) {
-              re = fma(re, 0.00390625, (double)(int)a[L][2 * u]);
-              im = fma(im, 0.00390625, (double)(int)a[L][2 * u + 1]);
+              re = fma(re, 0.00390625, i32_to_f64(a[L][2 * u]));
+              im = fma(im, 0.00390625, i32_to_f64(a[L][2 * u + 1]));
             }
             const double sc = pow2(er[h][u] + fc[g] - 14);
             vals[g][h][u] = cd{re * sc, im * sc};
@@ -1066,45 +1220,50 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&tempty);
-      cd qd[2][2];  // diagonal of each of this lane's rows
 #pragma unroll
-      for (int h = 0; h < 2; ++h)
+      for (int ls = 0; ls < STEPS; ++ls) {
+        const int g = ls >> 1, h = ls & 1;
+        const int j = jh + 4 * g + t0;
+        cp_async_wait<AHEAD - 1>();  // this step's group has landed
+        const double2* sl = ring + slot_rd * (i8::kRingItems * kItem);
+        cd qv[2], pv[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const double2 x = sl[u * kItem], y = sl[(2 + u) * kItem];
+          qv[u] = cd{x.x, x.y};
+          pv[u] = cd{y.x, y.y};
+        }
+        slot_rd = next_slot(slot_rd);
+        // the slot refilled now is the one read (and used) by the previous step
+        if (ls + AHEAD < STEPS)
+          issue(Gc, ls + AHEAD, slot_wr);
+        else
+          issue(Gn, ls + AHEAD - STEPS, slot_wr);
+        slot_wr = next_slot(slot_wr);
+        const cd vv[2] = {vq[ls % VA][0], vq[ls % VA][1]};
+        if (ls + VA < STEPS) {  // the stage-matrix entries VA steps ahead
+          const int g2 = (ls + VA) >> 1, h2 = (ls + VA) & 1, j2 = jh + 4 * g2 + t0;
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int r = m0 + 16 * h2 + 8 * u + t1;
+            if (r < rend && j2 < ep.n) vq[ls % VA][u] = Vb[(size_t)ri[h2][u] * ep.ld + j2];
+          }
+        }
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
           const int r = m0 + 16 * h + 8 * u + t1;
-          qd[h][u] = (r < rend) ? ep.Q[(size_t)r * ep.ld + ri[h][u]] : cd{0.0, 0.0};
-        }
-#pragma unroll
-      for (int g = 0; g < 8; ++g) {
-        const int j = jh + 4 * g + t0;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          cd qv[2], pv[2], vv[2], dv[2];
-#pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            const int r = m0 + 16 * h + 8 * u + t1;
-            if (r < rend && j < ep.n) {
-              const size_t ro = (size_t)r * ep.ld;
-              qv[u] = ldcg_cd(ep.Q + ro + j);
-              pv[u] = ldcg_cd(ep.P + ro + j);
-              vv[u] = Vb[(size_t)ri[h][u] * ep.ld + j];
-              dv[u] = ep.D[(size_t)ra[h][u] * ep.ld + j];
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            const int r = m0 + 16 * h + 8 * u + t1;
-            if (r < rend && j < ep.n) {
-              const size_t ro = (size_t)r * ep.ld;
-              const cd acc = vals[g][h][u] + qd[h][u] * vv[u] + qv[u] * (dv[u] + vd);
-              const cd p = pv[u] + ep.cb * acc;
-              ep.P[ro + j] = p;
-              ep.Qo[ro + j] = qv[u] + ep.ca * p;
-            }
+          if (r < rend && j < ep.n) {
+            const size_t ro = (size_t)r * ep.ld;
+            const cd dv = dtab[(ra[h][u] - a0) * dpitch + (j - j0)];
+            const cd acc = vals[g][h][u] + qd[h][u] * vv[u] + qv[u] * dv;
+            const cd p = pv[u] + ep.cb * acc;
+            ep.P[ro + j] = p;
+            ep.Qo[ro + j] = qv[u] + ep.ca * p;
           }
         }
       }
     }
+    cp_async_wait<0>();
   }
   tc_fence_before();
   __syncthreads();
@@ -1138,11 +1297,12 @@ size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 // Workspace layout: A slices, B^T slices (`cbytes` bytes per complex entry: 4 for
 // BF16 pairs, 2 for INT8 pairs; one set per problem of a stacked group), row and
 // column exponents.
-Carve carve(void* base, int nang, int n, int S, int cbytes = 4, int nprob = 1) {
+Carve carve(void* base, int nang, int n, int S, int cbytes = 4, int nprob = 1,
+            int nc = split::NC) {
   Carve c;
   c.rows = nang * n;
   c.kc = round_up(n, 16);                 // complex k (= ld of the state)
-  c.npad = round_up(n, split::NC);
+  c.npad = round_up(n, nc);               // complex columns of the tiles
   c.nrows = 2 * c.npad;
   char* p = reinterpret_cast<char*>(base);
   size_t o = 0;
@@ -1176,12 +1336,12 @@ EncodeTiled encoder() {
 }
 
 // 3-D map over [S][rows][kr] elements of `esize` bytes (BF16 or INT8) with a
-// (64 bytes x 128 x 1) box and 64-byte swizzle; out-of-range boxes read zeros.
-CUtensorMap make_map(void* base, int kr, int rows, int S, int esize = 2) {
+// (64 bytes x box_rows x 1) box and 64-byte swizzle; out-of-range boxes read zeros.
+CUtensorMap make_map(void* base, int kr, int rows, int S, int esize = 2, int box_rows = split::BM) {
   CUtensorMap m;
   cuuint64_t dims[3] = {(cuuint64_t)kr, (cuuint64_t)rows, (cuuint64_t)S};
   cuuint64_t strides[2] = {(cuuint64_t)kr * esize, (cuuint64_t)kr * esize * rows};
-  cuuint32_t box[3] = {(cuuint32_t)(64 / esize), split::BM, 1};
+  cuuint32_t box[3] = {(cuuint32_t)(64 / esize), (cuuint32_t)box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   const CUtensorMapDataType dt =
       (esize == 2) ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
@@ -1190,6 +1350,12 @@ CUtensorMap make_map(void* base, int kr, int rows, int S, int esize = 2) {
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
   return m;
+}
+
+int current_device() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return dev;
 }
 
 int sm_count() {
@@ -1219,8 +1385,8 @@ void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V,
   const int tiles_n = c.nrows / split::NT, tiles_m = ceil_div(c.rows, split::BM);
   if (variant == kSplitPersistent) {
     const size_t smem = split::psmem_bytes(S);
-    static bool attr[6] = {false, false, false, false, false, false};
-    if (!attr[S]) {
+    static SmemOptIn attr;
+    if (!attr.bytes_on(current_device())) {
       // setmaxnreg redistributes the registers the block was launched with: the
       // kernel must have been built with the count the split assumes
       cudaFuncAttributes fa{};
@@ -1229,10 +1395,8 @@ void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V,
         throw std::runtime_error("persistent split kernel built with " +
                                  std::to_string(fa.numRegs) + " registers per thread, needs " +
                                  std::to_string(split::P_REG_LAUNCH));
-      cudaFuncSetAttribute(split::k_split_gemm_p<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      attr[S] = true;
     }
+    attr.ensure((const void*)split::k_split_gemm_p<S>, smem);
     const int tiles = tiles_n * tiles_m;
     const int grid = std::min(tiles, sm_count());
     if (ev) cudaEventRecord(ev[0], st);
@@ -1241,12 +1405,8 @@ void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V,
     if (ev) cudaEventRecord(ev[1], st);
   } else {
     const size_t smem = split::smem_bytes(S);
-    static bool attr[6] = {false, false, false, false, false, false};
-    if (!attr[S]) {
-      cudaFuncSetAttribute(split::k_split_gemm<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      attr[S] = true;
-    }
+    static SmemOptIn attr;
+    attr.ensure((const void*)split::k_split_gemm<S>, smem);
     dim3 grid(tiles_n, tiles_m);
     if (ev) cudaEventRecord(ev[0], st);
     split::k_split_gemm<S><<<grid, split::THREADS, smem, st>>>(ta, tb, ep, kr / split::BK);
@@ -1258,51 +1418,61 @@ template <int S>
 void run_split_i8(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
                   int nang, int n, int ld, double cb, double ca, const cudaEvent_t* ev,
                   StackedRows sr, cudaStream_t st) {
+  constexpr int NTS = split::i8::nt_for(S), NCS = NTS / 2;
   const int rows = nang * n;
   if (sr.rows_b <= 0) sr = StackedRows{rows, 0};
   const int nprob = ceil_div(rows, sr.rows_b);
-  Carve c = carve(w.base, nang, n, S, 2, nprob);
+  Carve c = carve(w.base, nang, n, S, 2, nprob, NCS);
   const int kr = 2 * c.kc;
+  if (kr > 16384) throw std::invalid_argument("INT8 split form: k beyond the exact INT32 range");
   uint16_t* B = reinterpret_cast<uint16_t*>(c.B);
   uint32_t* A = reinterpret_cast<uint32_t*>(c.A);
   split::k_slice_cols_i8<S><<<dim3(n, nprob), 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, B,
                                                             sr.vstride, c.npad);
   split::k_slice_rows_i8<S><<<ceil_div(c.rows, 8), 256, 0, st>>>(Q, c.rows, n, ld, kr, A, c.erow);
   CUtensorMap ta = make_map(c.A, kr, c.rows, S, 1);
-  CUtensorMap tb = make_map(c.B, kr, c.nrows, S * nprob, 1);
+  CUtensorMap tb = make_map(c.B, kr, c.nrows, S * nprob, 1, NTS);
   split::EpiArgs ep{Q, P, Qo, V, D, c.erow, c.fcol, w.status, c.rows, n, ld, c.kc, S, cb, ca};
   const int tpp = ceil_div(sr.rows_b, split::BM);
   ep.rows_b = sr.rows_b;
   ep.vstride = sr.vstride;
   ep.fstride = c.npad;
   ep.tpp = tpp;
-  const int tiles_n = c.nrows / split::NT, tiles_m = nprob * tpp;
+  // the epilogue's per-tile table of D: the angles of 128 rows x min(NC, n) columns
+  const int dpitch = std::min(NCS, n);
+  if ((size_t)((split::BM - 1) / n + 2) * dpitch * sizeof(cd) > (size_t)split::i8::kDTabBytes)
+    throw std::invalid_argument("INT8 split form: diagonal table exceeds its shared memory");
+  const int tiles_n = c.nrows / NTS, tiles_m = nprob * tpp;
   const size_t smem = split::i8::smem_bytes(S);
-  static bool attr[6] = {false, false, false, false, false, false};
-  if (!attr[S]) {
+  static SmemOptIn attr;
+  if (!attr.bytes_on(current_device())) {
     cudaFuncAttributes fa{};
     if (cudaFuncGetAttributes(&fa, split::k_split_gemm_i8<S>) != cudaSuccess ||
         fa.numRegs < split::P_REG_LAUNCH)
       throw std::runtime_error("INT8 split kernel built with " + std::to_string(fa.numRegs) +
                                " registers per thread, needs " +
                                std::to_string(split::P_REG_LAUNCH));
-    cudaFuncSetAttribute(split::k_split_gemm_i8<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    attr[S] = true;
   }
+  attr.ensure((const void*)split::k_split_gemm_i8<S>, smem);
   const int tiles = tiles_n * tiles_m;
   const int grid = std::min(tiles, sm_count());
   if (ev) cudaEventRecord(ev[0], st);
   split::k_split_gemm_i8<S><<<grid, split::P_THREADS, smem, st>>>(
-      ta, tb, ep, ceil_div(kr, split::i8::BK), tiles_n, tiles);
+      ta, tb, ep, ceil_div(kr, split::i8::BK), tiles_n, tiles, dpitch);
   if (ev) cudaEventRecord(ev[1], st);
 }
 
 }  // namespace
 
 size_t split_workspace_bytes(int nang, int n, int slices, int nprob) {
-  Carve c = carve(nullptr, nang, n, slices, 4, nprob);
-  return reinterpret_cast<size_t>(c.fcol) + align256((size_t)nprob * c.npad * sizeof(int)) + 256;
+  // large enough for every tile width (BF16: 64 complex columns; INT8: 64, 48, 40)
+  size_t b = 0;
+  for (int nc : {split::NC, split::i8::nc_for(5), split::i8::nc_for(6)}) {
+    Carve c = carve(nullptr, nang, n, slices, 4, nprob, nc);
+    b = std::max(b, reinterpret_cast<size_t>(c.fcol) +
+                        align256((size_t)nprob * c.npad * sizeof(int)) + 256);
+  }
+  return b;
 }
 
 SplitWorkspace split_workspace_carve(void* base, int nang, int n, int slices, unsigned* status,
@@ -1329,8 +1499,14 @@ int split_stage(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V
       case 4:
         run_split_i8<4>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, sr, st);
         break;
+      case 5:
+        run_split_i8<5>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, sr, st);
+        break;
+      case 6:
+        run_split_i8<6>(w, Q, P, Qo, V, D, nang, n, ld, cb, ca, ev, sr, st);
+        break;
       default:
-        throw std::invalid_argument("INT8 split slices must be 3 or 4");
+        throw std::invalid_argument("INT8 split slices must be 3 to 6");
     }
     return 4;
   }

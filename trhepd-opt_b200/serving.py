@@ -187,7 +187,7 @@ class Server:
         ld = -(-n // 16) * 16
         state = 3 * n_angles * n * ld * 16
         table = ncol * nv * 32
-        split = 4 * n_angles * n * 2 * ld * 2
+        split = 6 * n_angles * n * 2 * ld * 4  # digit slices, up to 6 per operand
         return state + table + split + n_angles * n * n * 16
 
     # ---- scheduling
