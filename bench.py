@@ -274,8 +274,8 @@ def serve_leg(device: int, seconds: float, load: float, precision: int, seed: in
                 "isolated_s": {f"{n}x{g}": t for (n, g), t in iso.items()},
                 "mix": {str(k): v for k, v in serving.DEFAULT_MIX.items()},
                 "grids": list(serving.GRIDS),
-                "slots": [{"n_min": lo, "n_max": hi, "stream_priority": p}
-                          for lo, hi, p in serving.DEFAULT_SLOTS],
+                "slots": [{"n_min": lo, "n_max": hi, "stream_priority": p, "max_ctas": cap}
+                          for lo, hi, p, cap in serving.DEFAULT_SLOTS],
                 "hbm_budget_gb": 120.0,
                 "structures": "dense(N) base per (N, grid), 15 A region in 0.02 A slices, "
                               "surface atoms jittered by sigma in [0.05, 0.2] A per request"})
@@ -320,6 +320,31 @@ def uneven_leg(ctx, precision: int, per_n: int = 8, seed: int = 0) -> dict:
             "note": "N <= 64 in fused FP64 launches, N = 95, 191 in the requested form"}
 
 
+def bulk_leg(ctx, cpu: bool) -> dict:
+    """The bulk boundary solve (bulk.exe: bulk.txt -> bulkP.b) timed on its own, as
+    the reference runs it in a separate program: the reference's N = 23 structure
+    (69 angles x 7 beam groups) and N = 521 structure (1 angle x 49 groups), GPU
+    device time of the second run, beside the oracle on the host cores."""
+    out = {}
+    for case in ("test23", "test521"):
+        d = ROOT / "tests" / "golden" / case
+        tmp = Path(tempfile.mkdtemp(prefix="trhepd_bulk_"))
+        ctx.bulk_run(d / "bulk.txt", tmp / "bulkP.b")
+        st = ctx.bulk_run(d / "bulk.txt", tmp / "bulkP.b")
+        e = {"device_ms": st["device_ms"], "items": st["items"], "layers": st["layers"],
+             "item_solves_per_s": st["items"] / (st["device_ms"] / 1e3)}
+        if cpu:
+            from oracle import oracle as O
+            O.build()
+            t0 = time.perf_counter()
+            O.bulk_run(d / "bulk.txt", tmp / "oracle.b")
+            e["oracle_host_s"] = time.perf_counter() - t0
+        out[case] = e
+    out["note"] = ("(angle, beam group) items; GPU: slice propagators from matrix cos/sin "
+                   "series, layer recursion with the reference's convergence exit")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -337,13 +362,14 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven candidate batch")
+    ap.add_argument("--no-bulk", action="store_true", help="skip the bulk boundary solve leg")
     ap.add_argument("--uneven-per-n", type=int, default=8,
                     help="candidates per beam count in the uneven batch (64: 256 structures)")
-    ap.add_argument("--serve-seconds", type=float, default=40.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-load", type=float, default=0.5,
                     help="arrival rate as a fraction of the isolated-solve throughput")
-    ap.add_argument("--serve-fp64", action="store_true",
-                    help="also run the serving stream with the plain FP64 form")
+    ap.add_argument("--no-serve-fp64", action="store_true",
+                    help="skip the serving stream in the plain FP64 form")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     pg = None
@@ -464,17 +490,50 @@ def main():
         kernel, unit = "k_stage_gemm_f64 (FP64 DMMA)", "TFLOP/s"
     fp64_equiv_tflops = fp64_equiv / (tensor_ms * 1e-3) / 1e12
     form = args.precision if args.precision != "auto" else "int8"
-    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": unit,
+    # the two rooflines of the stage kernel: issued tensor work and algorithmic HBM
+    # bytes (state Q, P read; P, Q' written; digit slices A and B read once)
+    ld = -(-n // 16) * 16
+    kc = ld
+    hbm_bytes = 4 * 16.0 * nang * n * n
+    if split:
+        hbm_bytes += (slices if prec == native.SPLIT_INT8 else 2 * slices) * nang * n * 2 * kc
+    hbm_peak = peaks.get("hbm_gbs") or 6650.0
+    hbm_ms = hbm_bytes / (hbm_peak * 1e9) * 1e3
+    # INT8: the tcgen05 kind::i8 issue rate measured by a back-to-back MMA probe on
+    # this part, 8192 MAC per clock per SM, at the median SM clock of the timed region
+    mma_issue = None
+    if prec == native.SPLIT_INT8 and clk.get("sm_mhz"):
+        try:
+            import torch
+            sms = torch.cuda.get_device_properties(local).multi_processor_count
+        except Exception:
+            sms = 148
+        mma_issue = 2 * 8192 * sms * clk["sm_mhz"] * 1e6 / 1e12   # TOP/s
+    traffic = NCU_TRAFFIC.get((args.workload, form, slices))
+    tensor_floor_ms = issued / (peak * 1e12) * 1e3 if peak else 0.0
+    roof = {"bound": "tensor" if tensor_floor_ms >= hbm_ms else "hbm",
+            "achieved": achieved, "peak": peak, "unit": unit,
             "frac": (achieved / peak) if peak else None,
-            "traffic": NCU_TRAFFIC.get((args.workload, form)),
+            "traffic": (traffic * nang / 16.0) if traffic else None,
             "kernel": kernel, "peak_source": peak_src, "library_peak": pk,
             "avg_launch_ms": tensor_ms, "stage_product_ms": stage_ms, "ops_per_launch": issued,
             "slice_pairs": pairs, "fp64_equivalent_tflops": fp64_equiv_tflops,
             "fp64_library_peak_tflops": f64_peak,
             "frac_of_fp64_peak": (fp64_equiv_tflops / f64_peak["sustained"]) if f64_peak else None,
+            "frac_of_mma_issue_rate": (achieved / mma_issue) if mma_issue else None,
+            "mma_issue_rate": mma_issue,
+            "hbm": {"algorithmic_bytes_per_launch": hbm_bytes, "peak_gbs": hbm_peak,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if
+                    peaks.get("hbm_gbs") else "fallback 6.65 TB/s",
+                    "achieved_gbs": hbm_bytes / (tensor_ms * 1e-3) / 1e9,
+                    "frac": hbm_ms / tensor_ms, "time_at_peak_ms": hbm_ms},
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                              "on the 16-angle profiling case, scaled by angles "
+                              "(profiles/k_split_gemm_i8_dense521s.md)" if traffic else None,
             "note": "ops per launch = slice pairs x 8*nangles*N^3 (complex N^3 as a real "
                     "(nangles*N) x 2N x 2N product per slice pair); stage_product_ms adds "
-                    "the slicing and exponent kernels of the same stage"}
+                    "the slicing and exponent kernels of the same stage; the kernel is "
+                    "bound by shared-memory operand bandwidth (see frac_of_mma_issue_rate)"}
     # where the device time of one solve goes (the profiled solve; events between
     # launches make it slightly longer than an unprofiled one)
     breakdown = {"solve_ms": stp["device_ms"], "stage_products_ms": stp["stage_kernel_ms"],
@@ -493,8 +552,11 @@ def main():
     def errors(got, ref):
         rowmax = np.maximum(np.abs(ref).max(axis=1, keepdims=True), 1e-300)
         d = np.abs(got - ref)
-        big = np.abs(ref) >= 1e-3 * rowmax
-        return {"max_err_vs_rowmax": float((d / rowmax).max()),
+        m = np.abs(ref)
+        big = m >= 1e-3 * rowmax
+        every = np.where(m > 0, d / np.where(m > 0, m, 1.0), np.where(d > 0, np.inf, 0.0))
+        return {"max_rel_err_all_spots": float(every.max()),
+                "max_err_vs_rowmax": float((d / rowmax).max()),
                 "max_rel_err_spots_ge_1e-3_rowmax":
                     float((d / np.where(big, np.abs(ref), np.inf)).max())}
 
@@ -541,13 +603,16 @@ def main():
     uneven = None
     if rank == 0 and ws == 1 and not args.no_uneven:
         uneven = uneven_leg(ctx, prec, per_n=args.uneven_per_n)
+    bulk = None
+    if rank == 0 and ws == 1 and not args.no_bulk:
+        bulk = bulk_leg(ctx, cpu=not args.no_cpu_baseline)
     ctx.close()
 
     serve = None
     if rank == 0 and ws == 1 and not args.no_serve:
         serve = {"split" if split else "fp64":
                  serve_leg(local, args.serve_seconds, args.serve_load, prec)}
-        if args.serve_fp64 and prec != native.FP64:
+        if not args.no_serve_fp64 and prec != native.FP64:
             serve["fp64"] = serve_leg(local, args.serve_seconds, args.serve_load, native.FP64)
 
     if rank == 0:
@@ -567,13 +632,27 @@ def main():
                            "stage_products_per_solve": stp["stage_products"],
                            "bulk_boundary": "non-reflecting bulk records (f = 0)",
                            "l2": "inputs larger than L2 (state + stage table > 1 GB)",
-                           "parallelism": f"replicas x{ws}"},
-                "roofline": roof, "breakdown": breakdown, "fp64": fp64, "bf16_split": bf16,
-                "uneven_batch": uneven,
+                           "parallelism": f"replicas x{ws}",
+                           "serving_stream": None if not serve else (
+                               f"Poisson {next(iter(serve.values()))['arrival_rate_req_s']:.2f} "
+                               f"req/s for {args.serve_seconds:g} s: the serving workload's "
+                               "200 req/s scaled to {:g} of the throughput its isolated solve "
+                               "times allow".format(args.serve_load))},
+                "roofline": roof,
                 "e2e": e2e,
                 "cpu_baseline": cpu,
                 "gpu_launches": launches, "clocks": clk, "wall_seconds_timed": t_wall,
-                "serving": serve}
+                "serving": serve, "uneven_batch": uneven, "bulk_boundary": bulk,
+                "breakdown": breakdown,
+                "bf16_split": bf16, "fp64": fp64,
+                # last, so that a truncated view of the line still shows them
+                "split_vs_fp64": None if not fp64 else {
+                    "speedup": fp64["split_speedup"],
+                    "max_rel_err_all_spots": fp64["split_max_rel_err_all_spots"],
+                    "fp64_value": fp64["value"], "split_value": value,
+                    "renormalisation": "growth bound ln(1e3) for both forms; Gauss-Jordan "
+                                       "with fused complex multiply-adds (split) and with "
+                                       "products formed first (FP64, reference rounding)"}}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()

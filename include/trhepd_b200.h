@@ -62,11 +62,20 @@ enum trhepd_option {
   TRHEPD_OPT_STREAM_PRIORITY = 8, /* 0 (default, lowest) .. 1 (highest): priority of the
                                    context's stream; the block scheduler starts pending work of
                                    higher-priority streams first when several contexts share a GPU */
-  TRHEPD_OPT_VALIDATE = 9       /* nonzero: every split-form solve (trhepd_srfref,
+  TRHEPD_OPT_VALIDATE = 9,      /* nonzero: every split-form solve (trhepd_srfref,
                                    trhepd_problem_solve) is checked against the plain FP64 form
                                    of the same problem, solved first with the same options; the
                                    per-curve errors are read with trhepd_last_curve_errors.  Costs
-                                   one FP64 solve (about 3.5x the INT8 solve at N = 521) */
+                                   one FP64 solve (about 3x the INT8 solve at N = 521) */
+  TRHEPD_OPT_PARTICLE = 10,     /* trhepd_bulk_run: 0 positrons (TRHEPD, default), 1 electrons
+                                   (RHEED): the program-level switch ep = 'P' / 'E' of bulk.exe
+                                   (bulkm.f90:21-24), written to bulkP.b as inegpos; the surface
+                                   solve follows the inegpos of the file it reads
+                                   (surfio.f90:152) */
+  TRHEPD_OPT_MAX_CTAS = 11      /* 0 (default): the stage-product kernels use every SM; k > 0:
+                                   the persistent split kernels run at most k CTAs and the FP64
+                                   stage kernel at most 2k blocks, leaving the other SMs to
+                                   kernels of other contexts (streams) on the same GPU */
 };
 
 typedef struct trhepd_context trhepd_context;
@@ -250,7 +259,8 @@ void trhepd_problem_destroy(trhepd_problem* pb);
 
 /*
  * bulk.exe (sim-trhepd-rheed/src/bulkm.f90:207-256 + bulkio.f90:10-223 + blkref
- * bulk.f90:7-128) for one domain, positron mode: reads bulk.txt, computes every
+ * bulk.f90:7-128) for one domain, positrons or electrons (TRHEPD_OPT_PARTICLE):
+ * reads bulk.txt, computes every
  * (angle, beam group) reflection matrix on the GPU and writes bulkP.b in the
  * reference's record layout.  stats (optional): out[0] device ms, out[1] layers
  * iterated, out[2] double-angle steps, out[3] (angle, group) items.

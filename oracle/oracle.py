@@ -157,6 +157,11 @@ def set_bulk_scale(s: float) -> None:
     lib().oracle_set_bulk_scale(ctypes.c_double(s))
 
 
+def set_electron(on: bool) -> None:
+    """bulk_run for electrons (inegpos = 0, bulkm.f90:21-24) or positrons (default)."""
+    lib().oracle_set_electron(1 if on else 0)
+
+
 def set_renorm_every(k: int) -> None:
     """0: the reference's Gershgorin renormalisation test (default); k > 0:
     renormalise after every k-th slice instead (a growth-bound schedule)."""

@@ -1818,11 +1818,14 @@ static int blkref_group(int nbgm, int nbf, const int* ihg, const int* ikg, const
   return std::min(l, ml);
 }
 
+// Test knob: the particle of bulk_run, bulkm.f90:21-24 (1 positron, 0 electron).
+static int g_inegpos = 1;
+
 // bulk.exe (bulkm.f90:207-256 + bulkio.f90:10-223 + blkref): bulk.txt -> bulkP.b,
-// positron mode (bulkm.f90:222-225).
+// positrons (inegpos = 1) or electrons (0), bulkm.f90:21-24.
 static void bulk_run(const std::string& bulk_txt, const std::string& out_path) {
   ListReader T(bulk_txt);
-  const int inegpos = 1, idiag = 3, isym = 0, iabr = 0, iabp = 1, iabe = 0;
+  const int inegpos = g_inegpos, idiag = 3, isym = 0, iabr = 0, iabp = 1, iabe = 0;
   auto h3 = T.ints(3);
   int nh = h3[0], nk = h3[1], ndom = h3[2];
   if (nh < 1 || nk < 1 || ndom < 1) throw std::runtime_error("bulk.txt: bad NH/NK/NDOM");
@@ -2085,6 +2088,7 @@ struct OracleSurface {
 extern "C" {
 
 void oracle_set_renorm_every(int k) { g_renorm_every = k; }
+void oracle_set_electron(int e) { g_inegpos = e ? 0 : 1; }
 void oracle_set_bulk_scale(double s) { g_bulk_scale = s; }
 
 // Plane-group images in 1x1-lattice units (strfac.f90:15-64); returns the count.

@@ -10,6 +10,9 @@ writes, per test case (test23 / test47 / test521):
   for the integrators and slice thicknesses listed below;
 * ``conv-<name>.npz`` — a sample's rocking curves (surf-bulkP.s) and the
   convolution.txt the reference's make_convolution.py wrote from them;
+* ``ge001/`` — the Ge(001) sample's bulk.txt, surf.txt and the bulkP.b the
+  reference wrote from them (sim-trhepd-rheed/sample/Ge_001_c4x2), the only
+  reference output with a Z = 32 element;
 * ``test23/accurate.npz`` — the converged curves surf-bulkP-str-accurate.s (sp4,
   dz 0.001, E23.15) and, per (method, dz) of the perf fixtures, the first
   repetition of the per-angle rows compare.py printed against them
@@ -55,6 +58,13 @@ def main(ref: Path):
             ang, f2, hdr = parse_s(p)
             np.savez_compressed(dst / f"perf-{m}-{dz}.npz", angle=ang, f2=f2,
                                 beams=hdr["beams"], naz=hdr["naz"], ng=hdr["ng"])
+    # the Ge(001) sample: inputs and the bulkP.b the reference wrote from them
+    src = ref / "sim-trhepd-rheed" / "sample" / "Ge_001_c4x2"
+    dst = HERE / "ge001"
+    dst.mkdir(parents=True, exist_ok=True)
+    for f in ("bulk.txt", "surf.txt"):
+        shutil.copyfile(src / f, dst / f)
+    shutil.copyfile(src / "output" / "bulkP.b", dst / "bulkP.b")
     # converged curves and the comparison metric printed against them
     src = ref / "test" / "test23"
     ang, f2, hdr = parse_s(src / "surf-bulkP-str-accurate.s")

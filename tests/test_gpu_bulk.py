@@ -165,3 +165,81 @@ def test_bulk_then_surface(golden, ctx, oracle_mod, tmp_path):
     b.close()
     rowmax, _ = spot_errors(fa, fb)
     assert rowmax <= 1e-8, rowmax
+
+
+def test_bulk_ge_sample(golden, ctx, tmp_path):
+    """The reference's Ge(001) sample (Z = 32, one beam, 70 angles): header records
+    byte-identical to the bulkP.b the reference wrote, records to rounding."""
+    d = golden / "ge001"
+    out = tmp_path / "bulkP.b"
+    ctx.bulk_run(d / "bulk.txt", out)
+    mine, ref = records(out), records(d / "bulkP.b")
+    assert len(mine) == 16 + 70  # 70 glancing angles x 1 beam group
+    for i in range(16):
+        assert mine[i] == ref[i], f"header record {i}"
+    nnum, worst = compare(mine, ref)
+    assert worst <= 1e-10, worst
+
+
+def test_bulk_test521_within_sensitivity(golden, ctx, oracle_mod, tmp_path):
+    """The reference's N = 521 bulk (nh = nk = 7, 49 beam groups of up to 53 beams,
+    1 angle).  Its layer recursion is ill-conditioned in the reference's own
+    algorithm for the largest groups: a 2^-50 rescale of the slice potentials moves
+    the oracle's records for the groups of 53, 16 and 14 beams by O(1) of their
+    maximum, and the committed bulkP.b differs from the oracle there by as much, so
+    those records are rounding noise in any implementation.  Headers are
+    byte-identical; every record the rescale moves by less than 1e-3 of its maximum
+    (the meaningful ones, over 40) agrees with the oracle within 1e-8 plus 8x that
+    record's sensitivity; the others must be finite."""
+    d = golden / "test521"
+    ours = tmp_path / "gpu.b"
+    st = ctx.bulk_run(d / "bulk.txt", ours)
+    assert st["items"] == 49
+    ref, pert = sensitivity(oracle_mod, d / "bulk.txt", tmp_path)
+    mine, committed = records(ours), records(d / "bulkP.b")
+    assert len(mine) == len(ref) == len(committed) == 16 + 49
+    for i in range(16):
+        assert mine[i] == committed[i], f"header record {i}"
+    checked, worst = 0, 0.0
+    for i in range(16, len(mine)):
+        xa, ya, za = (np.frombuffer(v[i], np.complex128) for v in (mine, ref, pert))
+        assert np.isfinite(xa).all()
+        sc = max(np.abs(ya).max(), 1e-300)
+        sens = np.abs(za - ya).max() / sc
+        if sens > 1e-3:
+            continue
+        worst = max(worst, (np.abs(xa - ya).max() / sc) / (1e-8 + 8.0 * sens))
+        checked += 1
+    assert checked >= 40, checked
+    assert worst <= 1.0, worst
+
+
+def test_bulk_electron_matches_oracle(golden, ctx, oracle_mod, tmp_path):
+    """Electron mode (TRHEPD_OPT_PARTICLE = 1, bulk.exe with ep = 'E'): bulkP.b on the
+    GPU against the oracle's, then the surface solve on that file (which follows
+    its inegpos) against the oracle's surface solve."""
+    from trhepd_opt_b200 import native
+    d = golden / "test23"
+    ours, theirs = tmp_path / "bulkE.b", tmp_path / "oracleE.b"
+    ctx.set_option(native.OPT_PARTICLE, 1)
+    try:
+        ctx.bulk_run(d / "bulk.txt", ours)
+    finally:
+        ctx.set_option(native.OPT_PARTICLE, 0)
+    oracle_mod.set_electron(True)
+    try:
+        oracle_mod.bulk_run(d / "bulk.txt", theirs)
+    finally:
+        oracle_mod.set_electron(False)
+    nnum, worst = compare(records(ours), records(theirs))
+    assert nnum > 0 and worst <= 1e-9, worst
+    ctx.set_option(native.OPT_RENORM_POLICY, 0)
+    f2, _ = ctx.surf_run(theirs, d / "surf.txt", 0.1, 5, native.FP64)
+    S = oracle_mod.Surface(theirs, d / "surf.txt", 0.1, 5)
+    ref, _, _ = S.solve()
+    S.close()
+    abs_err, rel_err = spot_errors(f2, ref)
+    assert abs_err <= 1e-10 and rel_err <= 1e-9, (abs_err, rel_err)
+    # electrons and positrons scatter differently
+    fp, _ = ctx.surf_run(d / "bulkP.b", d / "surf.txt", 0.1, 5, native.FP64)
+    assert np.abs(fp - f2).max() > 1e-3 * np.abs(fp).max()

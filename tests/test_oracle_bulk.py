@@ -68,3 +68,52 @@ def test_bulk_conditioning(golden, oracle_mod, tmp_path):
     bulk_txt, _ = s.write(tmp_path / "s")
     assert sens(bulk_txt, tmp_path / "s") > 1e-4
 
+
+def test_bulk_ge_sample(golden, oracle_mod, tmp_path):
+    """The reference's Ge(001) sample (Z = 32, plane group 6, one beam, 70 angles):
+    the header records, which carry the element's scattering-factor coefficients,
+    are byte-identical and the records agree to rounding."""
+    d = golden / "ge001"
+    out = tmp_path / "bulkP.b"
+    oracle_mod.bulk_run(d / "bulk.txt", out)
+    mine, ref = records(out), records(d / "bulkP.b")
+    assert len(mine) == len(ref) == 16 + 70
+    for i in range(16):
+        assert mine[i] == ref[i], f"header record {i}"
+    for x, y in zip(mine[16:], ref[16:]):
+        xa, ya = np.frombuffer(x, np.complex128), np.frombuffer(y, np.complex128)
+        assert np.abs(xa - ya).max() <= 1e-12 * np.abs(ya).max()
+
+
+def test_bulk_electron_mode(golden, oracle_mod, tmp_path):
+    """Electrons (bulk.exe with ep = 'E', bulkm.f90:21-24): inegpos = 0 in the
+    header and the scattering-factor coefficients without the positron sign flip
+    (bulkio.f90:74); the Python header writer agrees byte for byte."""
+    import struct as st
+
+    from trhepd_opt_b200 import bulkfile, generator
+    d = golden / "test23"
+    oracle_mod.set_electron(True)
+    try:
+        oracle_mod.bulk_run(d / "bulk.txt", tmp_path / "e.b")
+    finally:
+        oracle_mod.set_electron(False)
+    oracle_mod.bulk_run(d / "bulk.txt", tmp_path / "p.b")
+    e, p = records(tmp_path / "e.b"), records(tmp_path / "p.b")
+    assert st.unpack("<10i", e[1])[0] == 0 and st.unpack("<10i", p[1])[0] == 1
+    ae, ap = np.frombuffer(e[8], np.float64), np.frombuffer(p[8], np.float64)
+    np.testing.assert_array_equal(ae[:4], -ap[:4])        # a(1:nabr), flipped for positrons
+    np.testing.assert_array_equal(ae[4:], ap[4:])         # sap, b
+    assert any(x != y for x, y in zip(e[16:], p[16:]))    # different reflection records
+    s = generator.small23()
+    bulk_txt, _ = s.write(tmp_path / "s")
+    oracle_mod.set_electron(True)
+    try:
+        oracle_mod.bulk_run(bulk_txt, tmp_path / "s" / "oracle.b")
+    finally:
+        oracle_mod.set_electron(False)
+    bulkfile.write_bulkp(s, tmp_path / "s" / "py.b", electron=True)
+    mine, ref = records(tmp_path / "s" / "py.b"), records(tmp_path / "s" / "oracle.b")
+    assert len(mine) == len(ref)
+    for i in range(16):
+        assert mine[i] == ref[i], f"header record {i}"

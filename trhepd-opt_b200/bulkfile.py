@@ -83,8 +83,9 @@ def zero_records(angle: int, group: int, nbf: int) -> np.ndarray:
     return np.zeros((nbf, nbf), dtype=np.complex128)
 
 
-def write_bulkp(s: Structure, path, records=zero_records) -> dict:
-    """Write bulkP.b for structure `s` (positron, one domain); returns header data."""
+def write_bulkp(s: Structure, path, records=zero_records, electron: bool = False) -> dict:
+    """Write bulkP.b for structure `s` (one domain; positrons, or electrons with
+    inegpos = 0 and no sign flip, bulkm.f90:21-24); returns header data."""
     ih = [h for h, _ in s.beams]
     ik = [k for _, k in s.beams]
     nb = len(ih)
@@ -99,7 +100,7 @@ def write_bulkp(s: Structure, path, records=zero_records) -> dict:
     nabr, nabi = 4, 1
     with open(path, "wb") as f:
         _rec(f, struct.pack("<i", 1))
-        _rec(f, struct.pack("<10i", 1, 0, s.nh, s.nk, 0, 1, 0, nabr, nabi, 3))
+        _rec(f, struct.pack("<10i", 0 if electron else 1, 0, s.nh, s.nk, 0, 1, 0, nabr, nabi, 3))
         _rec(f, struct.pack("<id", nb, 0.0))
         _rec(f, b"".join(struct.pack("<ii", h, k) for h, k in zip(ih, ik)))
         _rec(f, struct.pack("<dddiddi", s.energy_kev, s.azi[0] * RAD, s.azi[2] * RAD, naz,
@@ -112,7 +113,8 @@ def write_bulkp(s: Structure, path, records=zero_records) -> dict:
             a, b = scattering.params(e.z)
             a = list(a)
             a[0] -= e.da1
-            a = [-x for x in a]  # positron
+            if not electron:
+                a = [-x for x in a]  # positron (bulkio.f90:74)
             _rec(f, struct.pack("<10d", *a, e.sap, *b, 0.0))
             _rec(f, struct.pack("<5d", e.bh, e.bk, e.bz, scattering.mass(e.z), 0.0))
         for at in s.bulk_atoms:

@@ -45,7 +45,8 @@ class RecWriter {
 
 }  // namespace
 
-void load_bulk_inputs(const std::string& path, BulkInputs& B) {
+void load_bulk_inputs(const std::string& path, BulkInputs& B, int inegpos) {
+  B.inegpos = inegpos > 0 ? 1 : 0;
   ListInput T(path);
   auto h3 = T.values(3);
   B.nh = std::stoi(h3[0]);
@@ -104,7 +105,8 @@ void load_bulk_inputs(const std::string& path, BulkInputs& B) {
       b[(size_t)i * mab + j] = b4[j];
     }
     a[(size_t)i * mab] -= da1;                                     // bulkio.f90:73
-    for (int j = 0; j < B.nabr; ++j) a[(size_t)i * mab + j] *= -1.0;  // positron
+    if (B.inegpos > 0)                                             // positron: bulkio.f90:74
+      for (int j = 0; j < B.nabr; ++j) a[(size_t)i * mab + j] *= -1.0;
     B.nabi = 1;
     a[(size_t)i * mab + B.nabr] = sap;
     b[(size_t)i * mab + B.nabr] = 0.0;
@@ -278,7 +280,7 @@ void write_bulkp(const std::string& path, const BulkInputs& B,
   RecWriter W(path);
   W.put<int32_t>(1);
   W.end();
-  for (int v : {1, 0, B.nh, B.nk, B.iabr, 1, 0, B.nabr, B.nabi, 3}) W.put<int32_t>(v);
+  for (int v : {B.inegpos, 0, B.nh, B.nk, B.iabr, 1, 0, B.nabr, B.nabi, 3}) W.put<int32_t>(v);
   W.end();
   W.put<int32_t>(B.nb);
   W.put<double>(B.rdom);

@@ -1,6 +1,7 @@
 // Host-side setup of the bulk solve: a C++ equivalent of bulkio
-// (sim-trhepd-rheed/src/bulkio.f90:10-223) for one domain, positron mode
-// (bulkm.f90:222-225).  The reflection records themselves come from the GPU.
+// (sim-trhepd-rheed/src/bulkio.f90:10-223) for one domain, positrons or electrons
+// (bulkm.f90:21-24: inegpos = 1 or 0).  The reflection records themselves come
+// from the GPU.
 #pragma once
 #include <string>
 #include <vector>
@@ -14,6 +15,7 @@ struct BulkInputs {
   // ---- header records of bulkP.b (bulkio.f90:126-141), as written
   int nh = 1, nk = 1, nb = 0, naz = 1, ng = 1, ml = 100, nsg = 1, nelm = 0, natm = 0;
   int nabr = 4, nabi = 1, iabr = 0;
+  int inegpos = 1;                             // 1 positron, 0 electron
   double rdom = 0, be = 10, azi = 0, daz = 0, gi = 0, dg = 0, dz = 0, epsb = 1e-10;
   double aa = 0, bb = 0, gam = 0, cc = 0, dx = 0, dy = 0, zoffset = 0;
   std::vector<int> ih, ik;                     // original beam order
@@ -32,8 +34,9 @@ struct BulkInputs {
   StructureFactorJob stf[3];                   // st at zi (0,0), zi+cc (-dx,-dy), zi-cc (dx,dy)
 };
 
-// Parse bulk.txt and derive everything above.  Throws std::runtime_error.
-void load_bulk_inputs(const std::string& bulk_txt, BulkInputs& B);
+// Parse bulk.txt and derive everything above for positrons (inegpos = 1) or
+// electrons (0).  Throws std::runtime_error.
+void load_bulk_inputs(const std::string& bulk_txt, BulkInputs& B, int inegpos = 1);
 
 // Write bulkP.b: header records plus the reflection records t4 (per angle, per
 // group, nbf x nbf column-major, in the reference's order).

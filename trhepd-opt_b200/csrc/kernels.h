@@ -68,10 +68,11 @@ void launch_gather_stage_multi(const TableEntry* const* tables, size_t coloff, c
 void launch_stage_identity(cd* Q, cd* P, const cd* V, const cd* D, int nang, int n, int ld,
                            double cb, double ca, cudaStream_t st, StackedRows sr = {});
 
-// K5 (FP64 DMMA): P += cb*(Q V + Q o D_a);  Qo = Q + ca*P   (all angles, one launch)
+// K5 (FP64 DMMA): P += cb*(Q V + Q o D_a);  Qo = Q + ca*P   (all angles, one launch).
+// max_sms > 0: at most two blocks per SM on that many SMs, walking the tiles.
 void launch_stage_gemm_f64(const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D, int nang, int n,
                            int ld, int kpad, double cb, double ca, cudaStream_t st,
-                           StackedRows sr = {});
+                           StackedRows sr = {}, int max_sms = 0);
 
 // Q := I for angles whose flag is set (flag == nullptr: all angles).
 void launch_set_identity(cd* Q, const int* flag, int nang, int n, int ld, cudaStream_t st);

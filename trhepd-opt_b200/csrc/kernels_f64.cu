@@ -258,7 +258,7 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double& c2, double&
 __global__ void __launch_bounds__(128, 2)
     k_stage_gemm_f64(const cd* __restrict__ Q, cd* __restrict__ P, cd* __restrict__ Qo,
                      const cd* __restrict__ V, const cd* __restrict__ D, int rows, int n, int ld,
-                     int kpad, double cb, double ca, StackedRows sr) {
+                     int kpad, double cb, double ca, StackedRows sr, int tiles_x, int ntiles) {
   using namespace f64gemm;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd* As = reinterpret_cast<cd*>(smem_raw);
@@ -266,12 +266,19 @@ __global__ void __launch_bounds__(128, 2)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  // row tile -> problem: tiles of one problem never take rows of the next
   const int tpp = ceil_div(sr.rows_b, BM);
-  const int pb = blockIdx.y / tpp;
-  const int bm = pb * sr.rows_b + (blockIdx.y - pb * tpp) * BM, bn = blockIdx.x * BN;
-  rows = min(rows, (pb + 1) * sr.rows_b);
-  V += (size_t)pb * sr.vstride;
+  const int rows_all = rows;
+  const cd* const V_all = V;
+  // one tile per block (a grid of every tile), or a capped grid whose blocks walk the
+  // tiles (a context leaving SMs to other streams)
+  const int stride = gridDim.x * gridDim.y;
+  for (int tile = blockIdx.y * gridDim.x + blockIdx.x; tile < ntiles; tile += stride) {
+  const int tx = tile % tiles_x, ty = tile / tiles_x;
+  // row tile -> problem: tiles of one problem never take rows of the next
+  const int pb = ty / tpp;
+  const int bm = pb * sr.rows_b + (ty - pb * tpp) * BM, bn = tx * BN;
+  rows = min(rows_all, (pb + 1) * sr.rows_b);
+  V = V_all + (size_t)pb * sr.vstride;
 
   auto load_stage = [&](int s, int k0) {
     cd* a = As + s * A_TILE;
@@ -363,19 +370,29 @@ __global__ void __launch_bounds__(128, 2)
           Qo[o] = q + ca * p;
         }
       }
+  __syncthreads();  // the next tile's loads reuse the shared-memory stages
+  }
 }
 
 void launch_stage_gemm_f64(const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D, int nang, int n,
                            int ld, int kpad, double cb, double ca, cudaStream_t st,
-                           StackedRows sr) {
+                           StackedRows sr, int max_sms) {
   using namespace f64gemm;
   static SmemOptIn attr;
   attr.ensure((const void*)k_stage_gemm_f64, SMEM);
   int rows = nang * n;
   if (sr.rows_b <= 0) sr = StackedRows{rows, 0};
   const int nprob = ceil_div(rows, sr.rows_b);
-  dim3 grid(ceil_div(n, BN), nprob * ceil_div(sr.rows_b, BM));
-  k_stage_gemm_f64<<<grid, 128, SMEM, st>>>(Q, P, Qo, V, D, rows, n, ld, kpad, cb, ca, sr);
+  const int tiles_x = ceil_div(n, BN), tiles_y = nprob * ceil_div(sr.rows_b, BM);
+  const int ntiles = tiles_x * tiles_y;
+  if (max_sms > 0 && ntiles > 2 * max_sms) {  // two blocks per SM
+    k_stage_gemm_f64<<<2 * max_sms, 128, SMEM, st>>>(Q, P, Qo, V, D, rows, n, ld, kpad, cb, ca, sr,
+                                                     tiles_x, ntiles);
+  } else {
+    dim3 grid(tiles_x, tiles_y);
+    k_stage_gemm_f64<<<grid, 128, SMEM, st>>>(Q, P, Qo, V, D, rows, n, ld, kpad, cb, ca, sr,
+                                              tiles_x, ntiles);
+  }
 }
 
 // ============================================================ identity / flags

@@ -97,6 +97,8 @@ struct trhepd_context {
   int graphs = 1;                // 1: replay resident solves from a captured CUDA graph
   int fused_max_n = kFusedMaxBeams;  // FP64 RKN solves with n <= this run fused (0: never)
   int validate = 0;              // 1: split solves also run the FP64 form (per-curve errors)
+  int particle = 0;              // trhepd_bulk_run: 0 positrons, 1 electrons
+  int max_ctas = 0;              // persistent split kernels: CTA cap (0: one per SM)
   double stats[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<double> curve_err; // 3 per angle of the last validated solve (curves.h)
   std::vector<cudaEvent_t> evpool;
@@ -450,6 +452,7 @@ void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_m
     R.sw = split_workspace_carve(
         W.split->ensure(split_workspace_bytes(nang, n, C->split_slices, R.nprob)), nang, n,
         C->split_slices, R.status, st, R.nprob);
+  R.sw.max_ctas = C->max_ctas;
   R.gj_per = 2 * ceil_div(n, 16);
   if (C->profile && (int)C->evpool.size() < 4 * nprod_max) {
     while ((int)C->evpool.size() < 4 * nprod_max) {
@@ -503,7 +506,8 @@ void stage_product(trhepd_context* C, RunState& R, const cd* Q, cd* P, cd* Qo, d
                               C->split_slices, R.split_variant, ev ? ev + 1 : nullptr, R.st, R.sr);
   } else {
     if (ev) CK(cudaEventRecord(ev[1], R.st));
-    launch_stage_gemm_f64(Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, R.kpad, cb, ca, R.st, R.sr);
+    launch_stage_gemm_f64(Q, P, Qo, R.V, R.D, R.nang, R.n, R.ld, R.kpad, cb, ca, R.st, R.sr,
+                          C->max_ctas);
     if (ev) CK(cudaEventRecord(ev[2], R.st));
     R.launches += 1;
   }
@@ -868,7 +872,7 @@ std::vector<void*> buffer_signature(const trhepd_context* C) {
 void run(trhepd_context* C, trhepd_problem& Pb, int precision) {
   const std::vector<double> key = {(double)precision, (double)C->split_slices,
                                    (double)C->split_variant, (double)C->renorm_policy,
-                                   C->renorm_tau, (double)C->fused_max_n};
+                                   C->renorm_tau, (double)C->fused_max_n, (double)C->max_ctas};
   if (!C->graphs || C->profile) {
     Pb.drop_graph();
     RunState R;
@@ -1616,6 +1620,14 @@ int trhepd_set_option(trhepd_context* c, int option, double value) {
     case TRHEPD_OPT_VALIDATE:
       c->validate = value != 0.0;
       return TRHEPD_OK;
+    case TRHEPD_OPT_MAX_CTAS:
+      if (value < 0 || value > 1 << 20) return fail(c, TRHEPD_EINVAL, "CTA cap must be >= 0");
+      c->max_ctas = (int)value;
+      return TRHEPD_OK;
+    case TRHEPD_OPT_PARTICLE:
+      if (value != 0.0 && value != 1.0) return fail(c, TRHEPD_EINVAL, "particle must be 0 or 1");
+      c->particle = (int)value;
+      return TRHEPD_OK;
   }
   return fail(c, TRHEPD_EINVAL, "unknown option");
 }
@@ -1896,7 +1908,7 @@ int trhepd_bulk_run(trhepd_context* ctx, const char* bulk_txt, const char* out_p
   return guarded(ctx, [&] {
     if (!bulk_txt || !out_path) throw std::invalid_argument("null path");
     BulkInputs B;
-    load_bulk_inputs(bulk_txt, B);
+    load_bulk_inputs(bulk_txt, B, ctx->particle == 1 ? 0 : 1);
     std::vector<std::vector<cd>> records;
     bulk_solve(ctx, B, records, stats);
     write_bulkp(out_path, B, records);

@@ -173,6 +173,7 @@ struct EpiArgs {
   // tpp row tiles per problem
   int rows_b = 0, fstride = 0, tpp = 0;
   long long vstride = 0;
+  int* tile_counter = nullptr;  // INT8 kernel: {next tile, finished CTAs}, zero between launches
 };
 
 // ------------------------------------------------------------ slicing kernels
@@ -921,8 +922,20 @@ __global__ void __launch_bounds__(128) k_slice_cols_i8(const cd* __restrict__ V,
   }
 }
 
-// Persistent INT8 stage product: one CTA per SM walks the tiles (static stride);
-// warp 0 issues TMA, warp 1 the MMAs of every slice pair (s, t) with s + t < S into
+// Called once per CTA when it has claimed its last tile: the last CTA of the launch
+// re-arms the counter pair (next tile, finished CTAs) for the next launch on the
+// stream (kernel boundaries order the reset before that launch's claims).
+__device__ __forceinline__ void tile_counter_done(int* counter, unsigned ctas) {
+  __threadfence();
+  if (atomicAdd(&counter[1], 1) == (int)ctas - 1) {
+    counter[0] = 0;
+    counter[1] = 0;
+    __threadfence();
+  }
+}
+
+// Persistent INT8 stage product: one CTA per SM (or fewer) takes tiles from a
+// per-launch counter; warp 0 claims them and issues TMA, warp 1 the MMAs of every slice pair (s, t) with s + t < S into
 // accumulator level s + t, warps 2-3 idle; eight epilogue warps (two per TMEM lane
 // quadrant, one per column half) drain a finished tile into registers, give the
 // TMEM back at once (the next tile's MMAs start) and perform the FP64 RKN update
@@ -943,13 +956,22 @@ __global__ void __launch_bounds__(P_THREADS, 1)
   constexpr int VA = i8::v_ahead(S);          // stage-matrix steps in flight
   static_assert(S * NTS <= TMEM_COLS, "INT8 levels exceed the tensor memory");
   static_assert(NCS % 8 == 0 && NTS % 16 == 0, "tile width");
-  if (*(volatile unsigned*)ep.status & kStatusTimeout) return;
+  constexpr int TQ = 4;                       // tile-index queue slots
+  if (*(volatile unsigned*)ep.status & kStatusTimeout) {
+    if (threadIdx.x == 0) tile_counter_done(ep.tile_counter, gridDim.x);
+    return;
+  }
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], tfull, tempty, drain_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh, issued_sh, consumed_sh;
+  // Tiles are claimed dynamically from a per-launch counter by the TMA warp and
+  // handed to the MMA and epilogue warps through a queue of TQ slots (-1: no more):
+  // a CTA that starts late (its SM held by another kernel) takes what is left.
+  __shared__ int tq[TQ];
+  __shared__ __align__(8) uint64_t tq_full[TQ], tq_empty[TQ];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t sbytes = i8::stage_bytes(S);
   constexpr int BSL = i8::b_slice_bytes(S);
@@ -962,6 +984,10 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     mbar_init(&tfull, 1);
     mbar_init(&tempty, P_EPI_WARPS);
     mbar_init(&drain_bar, 1);
+    for (int q = 0; q < TQ; ++q) {
+      mbar_init(&tq_full[q], 1);
+      mbar_init(&tq_empty[q], 1 + P_EPI_WARPS);  // the MMA thread and every epilogue warp
+    }
     abort_sh = 0;
     issued_sh = 0;
     consumed_sh = 0;
@@ -986,7 +1012,19 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       if (lane == 0) {
         int g = 0;
         bool stop = false;
-        for (int tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x) {
+        for (int it = 0; !stop; ++it) {
+          // claim the next tile and publish it in queue slot it % TQ
+          const int qs = it % TQ;
+          if (it >= TQ && !mbar_wait(&tq_empty[qs], ((it / TQ) - 1) & 1)) {
+            atomicOr(ep.status, kStatusTimeout);
+            abort_sh = 1;
+            break;
+          }
+          int tile = ld_volatile(&abort_sh) ? tiles : atomicAdd(ep.tile_counter, 1);
+          if (tile >= tiles) tile = -1;
+          tq[qs] = tile;
+          mbar_arrive(&tq_full[qs]);
+          if (tile < 0) break;
           const int rt = tile / tiles_n, pb = rt / ep.tpp;
           const int m0 = pb * ep.rows_b + (rt - pb * ep.tpp) * BM, n0 = (tile % tiles_n) * NTS;
           for (int kb = 0; kb < nkb; ++kb, ++g) {
@@ -1019,7 +1057,16 @@ __global__ void __launch_bounds__(P_THREADS, 1)
         const uint32_t idesc = instr_desc_i8(NTS);
         int g = 0, it = 0;
         bool stop = false;
-        for (int tile = blockIdx.x; tile < tiles && !stop; tile += gridDim.x, ++it) {
+        for (;; ++it) {
+          const int qs = it % TQ;
+          if (!mbar_wait(&tq_full[qs], (it / TQ) & 1)) {
+            atomicOr(ep.status, kStatusTimeout);
+            abort_sh = 1;
+            break;
+          }
+          const int tile = tq[qs];
+          mbar_arrive(&tq_empty[qs]);
+          if (tile < 0) break;
           if (it > 0 && !mbar_wait(&tempty, (it - 1) & 1)) {
             atomicOr(ep.status, kStatusTimeout);
             abort_sh = 1;
@@ -1087,7 +1134,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     };
     auto geometry = [&](int tile) {
       Geo Gt{0, 0, 0};
-      if (tile < tiles) {
+      if (tile >= 0 && tile < tiles) {
         const int rt = tile / tiles_n, pb = rt / ep.tpp;
         Gt.m0 = pb * ep.rows_b + (rt - pb * ep.tpp) * BM + q4 * 32;
         Gt.rend = min(ep.rows, (pb + 1) * ep.rows_b);
@@ -1114,17 +1161,24 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     };
     int slot_rd = 0, slot_wr = 0;
     auto next_slot = [](int s) { return s + 1 == RING ? 0 : s + 1; };
+    // the first tile of this CTA (-1: none); each tile has more than AHEAD steps
+    bool qok = mbar_wait(&tq_full[0], 0);
+    int tile = qok ? tq[0] : -1;
     {
-      const Geo G0 = geometry(blockIdx.x);
+      const Geo G0 = geometry(tile);
 #pragma unroll
       for (int q = 0; q < AHEAD; ++q) {
-        // the first tile of a CTA always has at least AHEAD steps
         issue(G0, q, slot_wr);
         slot_wr = next_slot(slot_wr);
       }
     }
+    if (epi_any(!qok)) {
+      if (!qok) atomicOr(ep.status, kStatusTimeout);
+      abort_sh = 1;
+      tile = -1;
+    }
     int it = 0;
-    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
+    for (; tile >= 0; ++it) {
       const int rt = tile / tiles_n, pb = rt / ep.tpp;
       const int m0 = pb * ep.rows_b + (rt - pb * ep.tpp) * BM + q4 * 32;
       const int rend = min(ep.rows, (pb + 1) * ep.rows_b);  // this problem's rows end here
@@ -1133,7 +1187,12 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       const cd* Vb = ep.V + (size_t)pb * ep.vstride;
       const int* fcb = ep.fcol + (size_t)pb * ep.fstride;
       const cd vd = Vb[(size_t)ep.kpad * ep.ld];
-      const Geo Gc{m0, rend, jh}, Gn = geometry(tile + gridDim.x);
+      // the next tile of this CTA, published by the TMA warp before it loads that
+      // tile's operands (so before this tile's MMAs finish)
+      const int qn = (it + 1) % TQ;
+      const bool nok = mbar_wait(&tq_full[qn], ((it + 1) / TQ) & 1);
+      const int tile_next = nok ? tq[qn] : -1;
+      const Geo Gc{m0, rend, jh}, Gn = geometry(tile_next);
       // D table of this tile: angles a0.. of its rows, columns j0 .. j0 + dpitch - 1
       const int tm0 = m0 - q4 * 32;
       const int a0 = tm0 / ep.n;
@@ -1184,7 +1243,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
           vq[ls][u] = (r < rend && j < ep.n) ? Vb[(size_t)ri[h][u] * ep.ld + j] : cd{0.0, 0.0};
         }
       }
-      const bool ok = mbar_wait(&tfull, it & 1);
+      const bool ok = nok && mbar_wait(&tfull, it & 1);
       // also the barrier after which every epilogue warp sees this tile's D table
       if (epi_any(!ok)) {
         if (!ok) atomicOr(ep.status, kStatusTimeout);
@@ -1262,6 +1321,11 @@ __global__ void __launch_bounds__(P_THREADS, 1)
           }
         }
       }
+      // queue slot of this tile no longer read by this warp (the next one is kept
+      // until the end of the next tile)
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tq_empty[it % TQ]);
+      tile = tile_next;
     }
     cp_async_wait<0>();
   }
@@ -1277,6 +1341,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(TMEM_COLS));
   }
+  if (threadIdx.x == 0) tile_counter_done(ep.tile_counter, gridDim.x);
 }
 
 }  // namespace split
@@ -1289,6 +1354,7 @@ struct Carve {
   __nv_bfloat162* B;
   int* erow;
   int* fcol;
+  int* counter;  // the INT8 kernel's tile counter pair (zeroed with the workspace)
   int rows, kc, npad, nrows;
 };
 
@@ -1313,6 +1379,8 @@ Carve carve(void* base, int nang, int n, int S, int cbytes = 4, int nprob = 1,
   c.erow = reinterpret_cast<int*>(p + o);
   o = align256(o + (size_t)c.rows * sizeof(int));
   c.fcol = reinterpret_cast<int*>(p + o);
+  o = align256(o + (size_t)nprob * c.npad * sizeof(int));
+  c.counter = reinterpret_cast<int*>(p + o);  // in the 256 bytes split_workspace_bytes adds
   return c;
 }
 
@@ -1365,6 +1433,13 @@ int sm_count() {
   return n > 0 ? n : 148;
 }
 
+// CTAs of a persistent kernel: one per SM, or fewer when the context caps them (a
+// serving slot leaving SMs to concurrent requests of other slots).
+int persistent_grid(const SplitWorkspace& w) {
+  const int sms = sm_count();
+  return w.max_ctas > 0 ? std::min(sms, w.max_ctas) : sms;
+}
+
 template <int S>
 void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V, const cd* D,
                int nang, int n, int ld, double cb, double ca, int variant, const cudaEvent_t* ev,
@@ -1398,7 +1473,7 @@ void run_split(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd* V,
     }
     attr.ensure((const void*)split::k_split_gemm_p<S>, smem);
     const int tiles = tiles_n * tiles_m;
-    const int grid = std::min(tiles, sm_count());
+    const int grid = std::min(tiles, persistent_grid(w));
     if (ev) cudaEventRecord(ev[0], st);
     split::k_split_gemm_p<S><<<grid, split::P_THREADS, smem, st>>>(ta, tb, ep, kr / split::BK,
                                                                    tiles_n, tiles);
@@ -1438,6 +1513,7 @@ void run_split_i8(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd*
   ep.vstride = sr.vstride;
   ep.fstride = c.npad;
   ep.tpp = tpp;
+  ep.tile_counter = c.counter;
   // the epilogue's per-tile table of D: the angles of 128 rows x min(NC, n) columns
   const int dpitch = std::min(NCS, n);
   if ((size_t)((split::BM - 1) / n + 2) * dpitch * sizeof(cd) > (size_t)split::i8::kDTabBytes)
@@ -1455,7 +1531,7 @@ void run_split_i8(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd*
   }
   attr.ensure((const void*)split::k_split_gemm_i8<S>, smem);
   const int tiles = tiles_n * tiles_m;
-  const int grid = std::min(tiles, sm_count());
+  const int grid = std::min(tiles, persistent_grid(w));
   if (ev) cudaEventRecord(ev[0], st);
   split::k_split_gemm_i8<S><<<grid, split::P_THREADS, smem, st>>>(
       ta, tb, ep, ceil_div(kr, split::i8::BK), tiles_n, tiles, dpitch);

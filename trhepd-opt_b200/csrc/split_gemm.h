@@ -11,6 +11,7 @@ struct SplitWorkspace {
   void* base = nullptr;
   int nang = 0, n = 0, slices = 0;
   unsigned* status = nullptr;  // device status word (kStatus* bits)
+  int max_ctas = 0;            // persistent kernels: at most this many CTAs (0: one per SM)
 };
 
 size_t split_workspace_bytes(int nang, int n, int slices, int nprob = 1);

@@ -27,6 +27,8 @@ OPT_GRAPHS = 6
 OPT_FUSED_MAX_N = 7
 OPT_STREAM_PRIORITY = 8
 OPT_VALIDATE = 9
+OPT_PARTICLE = 10
+OPT_MAX_CTAS = 11
 
 # every symbol include/trhepd_b200.h declares
 EXPORTS = [

@@ -82,8 +82,14 @@ def poisson_stream(rate: float, duration: float, seed: int = 0, mix=None,
 
 
 FUSED_MAX_N = 64
-# slot layout: (smallest N, largest N, stream priority 0 lowest .. 1 highest)
-DEFAULT_SLOTS = ((0, 95, 1.0), (0, 95, 1.0), (96, 191, 0.5), (192, 1 << 30, 0.0))
+# slot layout: (smallest N, largest N, stream priority 0 lowest .. 1 highest, SM cap
+# of the stage-product kernels, 0 = every SM).  A large solve's stage kernels hold
+# their SMs for a whole launch (persistent split kernels) or a block's lifetime
+# (FP64), so a small request's kernels would queue for SMs behind every launch; the
+# large-N slot is capped at 48 of the 148 SMs and the other slots always find SMs
+# free.  Their own kernels are not capped: the split kernels' CTAs take tiles from a
+# shared counter, so the CTAs that start at once do the work.
+DEFAULT_SLOTS = ((0, 95, 1.0, 0), (0, 95, 1.0, 0), (96, 191, 0.5, 0), (192, 1 << 30, 0.0, 48))
 
 
 class _Pending:
@@ -134,14 +140,14 @@ class Server:
     def __init__(self, device: int = 0, slots=DEFAULT_SLOTS, mem_budget_gb: float = 120.0,
                  precision: int = native.FP64, region: float = 15.0, dz: float = 0.02,
                  renorm_policy: int = 1, schedules: dict | None = None):
-        """`slots`: a sequence of (smallest N, largest N, stream priority) per slot,
-        or an int k for k slots that take any request at the default priority.
+        """`slots`: a sequence of (smallest N, largest N, stream priority[, CTA cap])
+        per slot, or an int k for k slots that take any request at the default priority.
         `schedules`: an autotune table (N -> chosen schedules); a request uses the
         entry of the nearest tuned N, else the fixed rule of precision_for."""
         self.schedules = schedules
         if isinstance(slots, int):
             slots = tuple((0, 1 << 30, 0.0) for _ in range(slots))
-        self.layout = tuple(slots)
+        self.layout = tuple(tuple(s) + (0,) * (4 - len(s)) for s in slots)
         self.slots = len(self.layout)
         self.device, self.precision = device, precision
         self.region, self.dz = region, dz
@@ -154,11 +160,12 @@ class Server:
         self.bulk_lock = threading.Lock()
         self.t0 = time.perf_counter()
         self.ctxs = [native.Context(device) for _ in self.layout]
-        for c, (_, _, prio) in zip(self.ctxs, self.layout):
+        for c, (_, _, prio, cap) in zip(self.ctxs, self.layout):
             c.set_option(native.OPT_RENORM_POLICY, renorm_policy)
             c.set_option(native.OPT_STREAM_PRIORITY, prio)
+            c.set_option(native.OPT_MAX_CTAS, cap)
         self.workers = [threading.Thread(target=self._work, args=(c, lo, hi), daemon=True)
-                        for c, (lo, hi, _) in zip(self.ctxs, self.layout)]
+                        for c, (lo, hi, _, _) in zip(self.ctxs, self.layout)]
         self.done: list[Request] = []
         for w in self.workers:
             w.start()
