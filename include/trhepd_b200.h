@@ -259,8 +259,8 @@ void trhepd_problem_destroy(trhepd_problem* pb);
 
 /*
  * bulk.exe (sim-trhepd-rheed/src/bulkm.f90:207-256 + bulkio.f90:10-223 + blkref
- * bulk.f90:7-128) for one domain, positrons or electrons (TRHEPD_OPT_PARTICLE):
- * reads bulk.txt, computes every
+ * bulk.f90:7-128) for every domain (NDOM >= 1, each at azimuth azi + rdom), positrons
+ * or electrons (TRHEPD_OPT_PARTICLE): reads bulk.txt, computes every
  * (angle, beam group) reflection matrix on the GPU and writes bulkP.b in the
  * reference's record layout.  stats (optional): out[0] device ms, out[1] layers
  * iterated, out[2] double-angle steps, out[3] (angle, group) items.
@@ -269,11 +269,15 @@ int trhepd_bulk_run(trhepd_context* ctx, const char* bulk_txt, const char* out_p
                     double* stats);
 
 /*
- * surf.exe for the first domain (surfm.f90:6-97 + surfio.f90:60-381): reads
- * bulkP.b and surf.txt, slices the surface for dz2, solves on the GPU and, if
- * out_path is not NULL, writes the rocking-curve file in the reference format.
- * f2 (optional) receives (nb, nangles); dims (optional) receives
- * {nb, nangles, ns, nv}.
+ * surf.exe (surfm.f90:6-97 + surfio.f90:60-381): reads bulkP.b and surf.txt,
+ * slices the surface for dz2, solves on the GPU and, if out_path is not NULL,
+ * writes the rocking-curve file in the reference format.  With NDOM > 1 every
+ * domain is solved (azimuth azi + rdom(d)) and the weighted sum of the rotated
+ * domains (domainsum.f90:7-121) is formed on the device: out_path receives the
+ * summed file (E12.4 rows, the beams of the domain with the most beams) and the
+ * same path with the extension .md every domain's rows, as the reference writes
+ * them.  f2 (optional) receives (nb, nangles), the summed intensities for
+ * NDOM > 1; dims (optional) receives {nb, nangles, ns, nv}.
  */
 int trhepd_surf_run(trhepd_context* ctx, const char* bulkp, const char* surf, double dz2,
                     int int_method, int precision, const char* out_path, double* f2,

@@ -212,3 +212,96 @@ def compare_curves(comp, ref):
     n0 = np.where(n0 == 0.0, 1.0, n0)
     e0 = np.linalg.norm(comp - ref, axis=1)
     return np.stack([e0 / n0.max(), e0 / n0], axis=1)
+
+
+def _fortran_e_value(v: float, d: int) -> float:
+    """v as Fortran's E(w).d edit writes it (d significant digits, 0.ddd form) and
+    reads it back."""
+    if v == 0.0:
+        return 0.0
+    m, e = f"{abs(v):.{d - 1}e}".split("e")
+    digits = m.replace(".", "")
+    return float(("-" if v < 0 else "") + "0." + digits + "e" + str(int(e) + 1))
+
+
+def domain_curves(S: "Surface"):
+    """Every domain of a multi-domain problem solved by the oracle: list of
+    (angle_deg, f2[nangles, nb_d]) in domain order (surfio.f90:291-341)."""
+    L = lib()
+    L.oracle_surface_solve_domain.restype = ctypes.c_int
+    L.oracle_surface_solve_domain.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    hdr = domain_header(S)
+    out = []
+    for d, nb in enumerate(hdr["nbd"]):
+        f2 = np.empty((S.n_angles, nb))
+        ang = np.empty(S.n_angles)
+        if L.oracle_surface_solve_domain(S._h, d, 0, S.n_angles, f2.ctypes.data, ang.ctypes.data):
+            raise RuntimeError("oracle domain solve failed")
+        out.append((ang, f2))
+    return out
+
+
+def domain_header(S: "Surface") -> dict:
+    """nbd, rdom (rad), wdom, gam (rad), every domain's ih/ik, nh, nk of a problem."""
+    L = lib()
+    L.oracle_surface_domains.argtypes = [ctypes.c_void_p] * 8
+    nhnk = (ctypes.c_int * 3)()
+    L.oracle_surface_domains(S._h, None, None, None, None, None, None, nhnk)
+    ndom = nhnk[2]
+    nbd = np.zeros(ndom, dtype=np.int32)
+    rdom, wdom = np.zeros(ndom), np.zeros(ndom)
+    gam = ctypes.c_double()
+    L.oracle_surface_domains(S._h, nbd.ctypes.data, rdom.ctypes.data, wdom.ctypes.data,
+                             ctypes.byref(gam), None, None, nhnk)
+    ih = np.zeros(int(nbd.sum()), dtype=np.int32)
+    ik = np.zeros_like(ih)
+    L.oracle_surface_domains(S._h, None, None, None, None, ih.ctypes.data, ik.ctypes.data, nhnk)
+    return {"nbd": [int(x) for x in nbd], "rdom": rdom, "wdom": wdom, "gam": gam.value,
+            "ih": ih, "ik": ik, "nh": nhnk[0], "nk": nhnk[1]}
+
+
+def domain_sum(curves, hdr):
+    """Weighted sum of rotated-domain rocking curves, restating
+    sim-trhepd-rheed/src/domainsum.f90:7-121 on values as it reads them from the .md
+    header (domain angles and cell angle F10.3 degrees, weights E12.3): the reference
+    domain has the most beams (first such); a beam of another domain is added onto
+    the first reference beam within 1e-4 after rotation by rdom(ref) - rdom(d)
+    (reduced coordinates h/nh, k/nk, sheared for gam = 120 deg), sums in domain and
+    beam order.  Returns (angle_deg of the last domain, s2[nangles, mb], idomr)."""
+    rad = math.atan(1.0) / 45.0
+    deg = 1.0 / rad
+    nbd = hdr["nbd"]
+    ndom = len(nbd)
+    gam = float(f"{hdr['gam'] * deg:10.3f}")
+    rdom = [float(f"{r * deg:10.3f}") for r in hdr["rdom"]]
+    wdom = [_fortran_e_value(w, 3) for w in hdr["wdom"]]
+    idomr = int(np.argmax(nbd))
+    mb = nbd[idomr]
+    off = np.concatenate([[0], np.cumsum(nbd)])
+
+    def red(b):
+        gx, gy = hdr["ih"][b] / hdr["nh"], hdr["ik"][b] / hdr["nk"]
+        if abs(gam - 120.0) < 1e-4:
+            gx = (gx + gx + gy) / math.sqrt(3.0)
+        return gx, gy
+
+    nang = curves[0][1].shape[0]
+    s2 = np.zeros((nang, mb))
+    for d in range(ndom):
+        f2 = curves[d][1]
+        if d == idomr:
+            for ib in range(mb):
+                s2[:, ib] = s2[:, ib] + f2[:, ib] * wdom[d]
+            continue
+        dr = rdom[idomr] - rdom[d]
+        cdr, sdr = math.cos(dr * rad), math.sin(dr * rad)
+        for ib in range(nbd[d]):
+            gx, gy = red(off[d] + ib)
+            gxr, gyr = cdr * gx - sdr * gy, sdr * gx + cdr * gy
+            for ibr in range(mb):
+                hx, hy = red(off[idomr] + ibr)
+                if abs(gxr - hx) < 1e-4 and abs(gyr - hy) < 1e-4:
+                    s2[:, ibr] = s2[:, ibr] + f2[:, ib] * wdom[d]
+                    break
+    return curves[-1][0], s2, idomr

@@ -2212,6 +2212,72 @@ int oracle_surface_solve(void* hh, int first, int count, double* f2, double* ang
   return 0;
 }
 
+// Domain `domain` of a multi-domain problem (surfio.f90:291-341): its beams, its
+// bulk records and azimuth azi + rdom(domain); angles [first, first+count).
+int oracle_surface_solve_domain(void* hh, int domain, int first, int count, double* f2,
+                                double* angle_out) {
+  auto* h = static_cast<OracleSurface*>(hh);
+  auto& S = h->S;
+  if (domain < 0 || domain >= S.ndom) return -1;
+  auto& D = S.dom[domain];
+  auto a = schedule(S);
+  int ibt = 0;
+  for (int d = 0; d < domain; ++d) ibt += S.nbd[d];
+  const int nb = S.nbd[domain];
+  const int total = a.nrep1 * a.nrep2;
+  if (first < 0 || count < 0 || first + count > total) return -1;
+  // the stage potential of this domain (its beam-difference set)
+  std::vector<cplx> v, vi;
+  if (domain == 0) {
+    v = h->v;
+    vi = h->vi;
+  } else {
+    build_potential(S, D, h->method, v, vi);
+  }
+  const double azi = S.azi + S.rdom[domain];
+#pragma omp parallel for schedule(dynamic)
+  for (int t = first; t < first + count; ++t) {
+    int irep1 = t / a.nrep2, irep2 = t % a.nrep2;
+    double ga, az;
+    if (a.ng_outer) {
+      az = azi + irep1 * S.daz;
+      ga = S.gi + irep2 * S.dg;
+    } else {
+      ga = S.gi + irep1 * S.dg;
+      az = azi + irep2 * S.daz;
+    }
+    IntStats st;
+    solve_one(S, D, nb, S.ih.data() + ibt, S.ik.data() + ibt, h->method, v.data(), vi.data(), ga,
+              az, D.fbulk.data() + D.rec_off[t], f2 + (size_t)(t - first) * nb, st);
+    if (angle_out) angle_out[t - first] = (a.ng_outer ? ga : az) * 180.0 / 3.141592654;
+  }
+  return 0;
+}
+
+// Header data of every domain: out_i[0..] = nbd per domain; out_d = rdom (radians),
+// wdom per domain, then gam (radians); ih/ik of every domain, domain after domain.
+void oracle_surface_domains(void* hh, int* nbd, double* rdom, double* wdom, double* gam,
+                            int* ih, int* ik, int* nhnk) {
+  auto& S = static_cast<OracleSurface*>(hh)->S;
+  int nbt = 0;
+  for (int d = 0; d < S.ndom; ++d) {
+    if (nbd) nbd[d] = S.nbd[d];
+    if (rdom) rdom[d] = S.rdom[d];
+    if (wdom) wdom[d] = S.wdom[d];
+    nbt += S.nbd[d];
+  }
+  if (gam) *gam = S.gam;
+  for (int j = 0; j < nbt; ++j) {
+    if (ih) ih[j] = S.ih[j];
+    if (ik) ik[j] = S.ik[j];
+  }
+  if (nhnk) {
+    nhnk[0] = S.nh;
+    nhnk[1] = S.nk;
+    nhnk[2] = S.ndom;
+  }
+}
+
 // Solve the listed angles (indices into the flattened schedule, any order) in
 // parallel; rows of f2 / angle_out / renorm_out follow the list.
 int oracle_surface_solve_list(void* hh, const int* idx, int count, double* f2, double* angle_out,

@@ -45,25 +45,46 @@ class RecWriter {
 
 }  // namespace
 
-void load_bulk_inputs(const std::string& path, BulkInputs& B, int inegpos) {
+void load_bulk_inputs(const std::string& path, BulkInputs& B, int inegpos, int domain) {
   B.inegpos = inegpos > 0 ? 1 : 0;
   ListInput T(path);
   auto h3 = T.values(3);
   B.nh = std::stoi(h3[0]);
   B.nk = std::stoi(h3[1]);
-  int ndom = std::stoi(h3[2]);
+  B.ndom = std::stoi(h3[2]);
   if (B.nh < 1 || B.nk < 1) throw std::runtime_error("bulk.txt: NH, NK must be >= 1");
-  if (ndom != 1) throw std::runtime_error("bulk.txt: only NDOM = 1 is supported on the GPU path");
-  B.nb = T.integer();
-  if (B.nb < 1) throw std::runtime_error("bulk.txt: NB < 1");
-  B.rdom = ListInput::real(T.values(1)[0]) * (kPi / 180.0);
-  auto bk = T.values(2 * B.nb);
-  B.ih.resize(B.nb);
-  B.ik.resize(B.nb);
-  for (int j = 0; j < B.nb; ++j) {
-    B.ih[j] = std::stoi(bk[2 * j]);
-    B.ik[j] = std::stoi(bk[2 * j + 1]);
+  if (B.ndom < 1) throw std::runtime_error("bulk.txt: NDOM < 1");
+  if (domain < 0 || domain >= B.ndom) throw std::runtime_error("domain index out of range");
+  B.domain = domain;
+  // bulkio.f90:34-50: beams per domain, domain angles, each domain's beams
+  auto nbv = T.values(B.ndom);
+  B.nbd.resize(B.ndom);
+  for (int d = 0; d < B.ndom; ++d) {
+    B.nbd[d] = std::stoi(nbv[d]);
+    if (B.nbd[d] < 1) throw std::runtime_error("bulk.txt: NB < 1");
   }
+  auto rv = T.values(B.ndom);
+  B.rdom_all.resize(B.ndom);
+  std::vector<double> rdom_deg(B.ndom);
+  for (int d = 0; d < B.ndom; ++d) {
+    rdom_deg[d] = ListInput::real(rv[d]);
+    B.rdom_all[d] = rdom_deg[d] * (kPi / 180.0);
+  }
+  B.ih_all.clear();
+  B.ik_all.clear();
+  for (int d = 0; d < B.ndom; ++d) {
+    auto bk = T.values(2 * B.nbd[d]);
+    for (int j = 0; j < B.nbd[d]; ++j) {
+      B.ih_all.push_back(std::stoi(bk[2 * j]));
+      B.ik_all.push_back(std::stoi(bk[2 * j + 1]));
+    }
+  }
+  int ibt = 0;
+  for (int d = 0; d < domain; ++d) ibt += B.nbd[d];
+  B.nb = B.nbd[domain];
+  B.rdom = B.rdom_all[domain];
+  B.ih.assign(B.ih_all.begin() + ibt, B.ih_all.begin() + ibt + B.nb);
+  B.ik.assign(B.ik_all.begin() + ibt, B.ik_all.begin() + ibt + B.nb);
   auto sc = T.values(7);
   double be = ListInput::real(sc[0]), azi = ListInput::real(sc[1]), azf = ListInput::real(sc[2]);
   double daz = ListInput::real(sc[3]), gi = ListInput::real(sc[4]), gf = ListInput::real(sc[5]);
@@ -130,6 +151,17 @@ void load_bulk_inputs(const std::string& path, BulkInputs& B, int inegpos) {
   B.cc = ListInput::real(st[4]);
   B.dx = ListInput::real(st[5]);
   B.dy = ListInput::real(st[6]);
+  if (B.ndom > 1) {  // rotated domains need a square or hexagonal cell (bulkio.f90:87-99)
+    const double gdeg = ListInput::real(st[3]);
+    if (std::fabs(B.aa - B.bb) > 1e-4)
+      throw std::runtime_error("bulk.txt: NDOM > 1 needs AA = BB");
+    const double step = std::fabs(gdeg - 90.0) < 1e-4 ? 90.0
+                        : std::fabs(gdeg - 120.0) < 1e-4 ? 60.0 : 0.0;
+    if (step == 0.0) throw std::runtime_error("bulk.txt: NDOM > 1 needs GAM = 90 or 120");
+    for (int d = 0; d < B.ndom; ++d)
+      if (std::fabs(rdom_deg[d] / step - std::nearbyint(rdom_deg[d] / step)) > 1e-4)
+        throw std::runtime_error("bulk.txt: domain angle not a multiple of the cell symmetry");
+  }
   B.natm = T.integer();
   if (B.natm < 1) throw std::runtime_error("bulk.txt: NATM < 1");
   B.ielm.resize(B.natm);
@@ -275,19 +307,22 @@ void load_bulk_inputs(const std::string& path, BulkInputs& B, int inegpos) {
   }
 }
 
-void write_bulkp(const std::string& path, const BulkInputs& B,
-                 const std::vector<std::vector<cd>>& records) {
+void write_bulkp(const std::string& path, const std::vector<BulkInputs>& Bd,
+                 const std::vector<std::vector<std::vector<cd>>>& records) {
+  const BulkInputs& B = Bd.at(0);
   RecWriter W(path);
-  W.put<int32_t>(1);
+  W.put<int32_t>(B.ndom);
   W.end();
   for (int v : {B.inegpos, 0, B.nh, B.nk, B.iabr, 1, 0, B.nabr, B.nabi, 3}) W.put<int32_t>(v);
   W.end();
-  W.put<int32_t>(B.nb);
-  W.put<double>(B.rdom);
+  for (int d = 0; d < B.ndom; ++d) {
+    W.put<int32_t>(B.nbd[d]);
+    W.put<double>(B.rdom_all[d]);
+  }
   W.end();
-  for (int i = 0; i < B.nb; ++i) {
-    W.put<int32_t>(B.ih[i]);
-    W.put<int32_t>(B.ik[i]);
+  for (size_t i = 0; i < B.ih_all.size(); ++i) {
+    W.put<int32_t>(B.ih_all[i]);
+    W.put<int32_t>(B.ik_all[i]);
   }
   W.end();
   W.put<double>(B.be);
@@ -324,24 +359,27 @@ void write_bulkp(const std::string& path, const BulkInputs& B,
     for (double v : {B.ocr[i], B.x[i], B.y[i], B.z[i]}) W.put<double>(v);
     W.end();
   }
-  for (int i = 0; i < B.nb; ++i) W.put<int32_t>(B.iord[i]);
-  W.end();
-  W.put<int32_t>(B.ngr);
-  W.put<int32_t>(B.nv);
-  W.end();
-  for (int g = 0; g < B.ngr; ++g) W.put<int32_t>(B.nbg[g]);
-  W.end();
-  for (int i = 0; i < B.nv; ++i) {
-    W.put<int32_t>(B.igh[i]);
-    W.put<int32_t>(B.igk[i]);
-  }
-  W.end();
-  for (const auto& r : records) {
-    for (const cd& v : r) {
-      W.put<double>(v.x);
-      W.put<double>(v.y);
+  for (size_t d = 0; d < Bd.size(); ++d) {
+    const BulkInputs& D = Bd[d];
+    for (int i = 0; i < D.nb; ++i) W.put<int32_t>(D.iord[i]);
+    W.end();
+    W.put<int32_t>(D.ngr);
+    W.put<int32_t>(D.nv);
+    W.end();
+    for (int g = 0; g < D.ngr; ++g) W.put<int32_t>(D.nbg[g]);
+    W.end();
+    for (int i = 0; i < D.nv; ++i) {
+      W.put<int32_t>(D.igh[i]);
+      W.put<int32_t>(D.igk[i]);
     }
     W.end();
+    for (const auto& r : records.at(d)) {
+      for (const cd& v : r) {
+        W.put<double>(v.x);
+        W.put<double>(v.y);
+      }
+      W.end();
+    }
   }
 }
 

@@ -86,7 +86,27 @@ __global__ void __launch_bounds__(256) k_curve_distance(const double* __restrict
   }
 }
 
+// domainsum.f90:58-106: s2[a][ibr] = sum over domains d (in order) and over the
+// beams ib of d that rotate onto beam ibr of the reference domain (in order) of
+// f2_d[a][ib] * w_d, each product rounded before the addition as the reference
+// forms it.  One thread per (angle, reference beam).
+__global__ void k_domain_sum(const DomainSumArgs args, int nang, int mb, double* __restrict__ s2) {
+  const int ibr = blockIdx.x * blockDim.x + threadIdx.x, a = blockIdx.y;
+  if (ibr >= mb || a >= nang) return;
+  double s = 0.0;
+  for (int d = 0; d < args.ndom; ++d) {
+    const double* f = args.f2[d] + (size_t)a * args.nb[d];
+    const int b0 = args.start[d * (mb + 1) + ibr], b1 = args.start[d * (mb + 1) + ibr + 1];
+    for (int q = b0; q < b1; ++q) s = __dadd_rn(s, __dmul_rn(f[args.list[q]], args.w[d]));
+  }
+  s2[(size_t)a * mb + ibr] = s;
+}
+
 }  // namespace
+
+void launch_domain_sum(const DomainSumArgs& args, int nang, int mb, double* s2, cudaStream_t st) {
+  if (nang > 0 && mb > 0) k_domain_sum<<<dim3((mb + 127) / 128, nang), 128, 0, st>>>(args, nang, mb, s2);
+}
 
 void launch_curve_errors(const double* got, const double* ref, int nang, int nb, double* out,
                          cudaStream_t st) {

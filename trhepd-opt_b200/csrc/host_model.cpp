@@ -186,10 +186,13 @@ int plane_group_images(int nsg, int ma, int mb, int na, int nb, double x, double
 }
 
 void load_surface_inputs(const std::string& bulkp, const std::string& surf, double dz2,
-                         int int_method, SurfaceInputs& S) {
+                         int int_method, SurfaceInputs& S, int domain) {
   Records R(bulkp);
   R.begin();
   S.ndom = R.i4();
+  if (S.ndom < 1) throw std::runtime_error("bulkP.b: NDOM < 1");
+  if (domain < 0 || domain >= S.ndom) throw std::runtime_error("domain index out of range");
+  S.domain = domain;
   R.begin();
   int inegpos = R.i4();
   R.i4();  // isym
@@ -201,12 +204,16 @@ void load_surface_inputs(const std::string& bulkp, const std::string& surf, doub
   R.i4();  // idiag
   R.begin();
   std::vector<int> nbd(S.ndom);
+  S.rdom.assign(S.ndom, 0.0);
   int nbt = 0;
   for (int i = 0; i < S.ndom; ++i) {
     nbd[i] = R.i4();
-    R.r8();  // rdom
+    S.rdom[i] = R.r8();
     nbt += nbd[i];
   }
+  S.nbd = nbd;
+  S.nh = nh;
+  S.nk = nk;
   R.begin();
   std::vector<int> ih(nbt), ik(nbt);
   for (int j = 0; j < nbt; ++j) {
@@ -229,6 +236,7 @@ void load_surface_inputs(const std::string& bulkp, const std::string& surf, doub
   int nsgb = R.i4();
   R.i4();  // mp
   double aa = R.r8(), bb = R.r8(), gam = R.r8();
+  S.gam = gam;
   S.cc = R.r8();
   double dxb = R.r8(), dyb = R.r8(), zoffset = R.r8();
   R.begin();
@@ -313,6 +321,14 @@ void load_surface_inputs(const std::string& bulkp, const std::string& surf, doub
     else
       throw std::runtime_error("surf.txt: atom element index out of range");
   }
+  // domain weights (surfio.f90:186-190)
+  S.wdom.assign(S.ndom, 1.0);
+  if (S.ndom > 1) {
+    auto w = T.values(S.ndom);
+    for (int i = 0; i < S.ndom; ++i) S.wdom[i] = ListInput::real(w[i]);
+  }
+  S.ih_all = ih;
+  S.ik_all = ik;
   // surface slices (surfio.f90:198-210)
   if (nsgs < 1) {
     S.ns = 0;
@@ -364,10 +380,24 @@ void load_surface_inputs(const std::string& bulkp, const std::string& surf, doub
     S.ghy = -(pi + pi) / (aa * std::tan(gam) * nh);
     S.gky = (pi + pi) / (bb * std::sin(gam) * nk);
   }
-  // first domain: beam tables and bulk records
-  S.nb = nbd[0];
-  S.ih.assign(ih.begin(), ih.begin() + S.nb);
-  S.ik.assign(ik.begin(), ik.begin() + S.nb);
+  // the records of the domains before `domain` (surfio.f90:291-300 and the bulk
+  // records srfref reads, surflf.f90:65-72), skipped
+  int ibt = 0;
+  for (int d = 0; d < domain; ++d) {
+    R.begin();  // iord
+    R.begin();
+    const int ngr = R.i4();
+    R.i4();     // nvb
+    R.begin();  // nbg
+    R.begin();  // igh, igk
+    for (int r = 0; r < S.naz * S.ng * ngr; ++r) R.begin();
+    ibt += nbd[d];
+  }
+  S.azi += S.rdom[domain];
+  // this domain: beam tables and bulk records
+  S.nb = nbd[domain];
+  S.ih.assign(ih.begin() + ibt, ih.begin() + ibt + S.nb);
+  S.ik.assign(ik.begin() + ibt, ik.begin() + ibt + S.nb);
   R.begin();
   S.iord.resize(S.nb);
   for (int i = 0; i < S.nb; ++i) S.iord[i] = R.i4();

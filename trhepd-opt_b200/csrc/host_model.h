@@ -51,15 +51,22 @@ struct SurfaceInputs {
   double wn = 0, ghx = 0, ghy = 0, gky = 0, azi = 0, daz = 0, gi = 0, dg = 0;
   int naz = 1, ng = 1, int_method = 5;
   std::vector<cd> t1rec;          // bulk records: nrep1*nrep2 angles x sum(nbg^2), file order
-  // ---- output header data (surfio.f90:270-288) for the rocking-curve writer
-  int ndom = 1;
+  // ---- output header data (surfio.f90:270-288) for the rocking-curve writer and the
+  // domain sum (domainsum.f90): every domain's beams, angle and weight
+  int ndom = 1, domain = 0;       // domains in the files; the one these inputs describe
+  int nh = 1, nk = 1;
+  double gam = 0;                 // cell angle (radians)
+  std::vector<int> nbd;           // beams per domain
+  std::vector<double> rdom, wdom; // domain angles (radians) and weights
+  std::vector<int> ih_all, ik_all;  // every domain's beams, domain after domain
 };
 
-// surfio (surfio.f90:60-381) for the first domain: parse bulkP.b and surf.txt,
-// apply the surface slicing rule for dz2, and fill every field above.
+// surfio (surfio.f90:60-381) for domain `domain` (0-based; srfref is called with
+// azimuth azi + rdom(domain), surfio.f90:340): parse bulkP.b and surf.txt, apply the
+// surface slicing rule for dz2, and fill every field above.
 // Throws std::runtime_error on malformed input.
 void load_surface_inputs(const std::string& bulkp, const std::string& surf, double dz2,
-                         int int_method, SurfaceInputs& out);
+                         int int_method, SurfaceInputs& out, int domain = 0);
 
 // Write the rocking-curve file (surfio.f90:270-274 header, surflf.f90:154-165 rows).
 void write_rocking_curves(const std::string& path, const SurfaceInputs& in, const double* f2,

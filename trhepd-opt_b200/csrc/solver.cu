@@ -1475,41 +1475,250 @@ std::string fortran_e(double v, int w, int d) {
 
 }  // namespace
 
+namespace {
+// '(400I4)' beam list of the header lines (surfio.f90:273, 284-287).
+void write_beams(FILE* o, const int* ih, const int* ik, int nb) {
+  int cnt = 0;
+  for (int j = 0; j < nb; ++j) {
+    for (int v : {ih[j], ik[j]}) {
+      std::fprintf(o, "%4d", v);
+      if (++cnt % 400 == 0 && cnt < 2 * nb) std::fprintf(o, "\n");
+    }
+  }
+  std::fprintf(o, "\n");
+}
+
+// One domain's rows (surflf.f90:154-165, domainsum.f90:113-119): per outer scan
+// index a block of '(E12.4,200(",",Ew.d))' rows with format reversion after 200
+// values, then an empty line.
+void write_rows(FILE* o, int naz, int ng, const double* f2, const double* angle_deg, int nb,
+                int w, int d) {
+  const bool ng_outer = ng > naz;
+  const int nrep1 = ng_outer ? naz : ng, nrep2 = ng_outer ? ng : naz;
+  for (int r1 = 0; r1 < nrep1; ++r1) {
+    for (int r2 = 0; r2 < nrep2; ++r2) {
+      const int t = r1 * nrep2 + r2;
+      std::string line = fortran_e(angle_deg[t], 12, 4);
+      for (int i = 0; i < nb; ++i) {
+        if (i > 0 && i % 200 == 0) {
+          std::fprintf(o, "%s\n", line.c_str());
+          line.clear();
+        }
+        line += ",";
+        line += fortran_e(f2[(size_t)t * nb + i], w, d);
+      }
+      std::fprintf(o, "%s,\n", line.c_str());
+    }
+    std::fprintf(o, "\n");
+  }
+}
+}  // namespace
+
 namespace trhepd {
 void write_rocking_curves(const std::string& path, const SurfaceInputs& S, const double* f2,
                           const double* angle_deg) {
   FILE* o = std::fopen(path.c_str(), "w");
   if (!o) throw std::runtime_error("cannot write " + path);
   std::fprintf(o, "#azimuths,g-angles,beams\n%4d%4d%4d\n#ih,ik\n", S.naz, S.ng, S.nb);
-  int cnt = 0;
-  for (int j = 0; j < S.nb; ++j) {
-    for (int v : {S.ih[j], S.ik[j]}) {
-      std::fprintf(o, "%4d", v);
-      if (++cnt % 400 == 0 && cnt < 2 * S.nb) std::fprintf(o, "\n");
-    }
+  write_beams(o, S.ih.data(), S.ik.data(), S.nb);
+  write_rows(o, S.naz, S.ng, f2, angle_deg, S.nb, 23, 15);
+  std::fclose(o);
+}
+
+// The .md file of a multi-domain run (surfio.f90:276-287 header, then each domain's
+// srfref rows in domain order): f2[d] (nangles x nbd[d]) and angle_deg[d].
+void write_domain_curves(const std::string& path, const SurfaceInputs& S,
+                         const std::vector<std::vector<double>>& f2,
+                         const std::vector<std::vector<double>>& angle_deg) {
+  const double deg = 45.0 / std::atan(1.0);
+  FILE* o = std::fopen(path.c_str(), "w");
+  if (!o) throw std::runtime_error("cannot write " + path);
+  std::fprintf(o, "#azimuths,g-angles,domains,nh,nk,gam\n%4d%4d%4d%4d%4d%10.3f\n", S.naz, S.ng,
+               S.ndom, S.nh, S.nk, S.gam * deg);
+  std::fprintf(o, "#beams,domain angle,domain weight\n");
+  for (int i = 0; i < S.ndom; ++i)
+    std::fprintf(o, "%4d%10.3f%s\n", S.nbd[i], S.rdom[i] * deg, fortran_e(S.wdom[i], 12, 3).c_str());
+  std::fprintf(o, "#ih,ik\n");
+  int ibt = 0;
+  for (int i = 0; i < S.ndom; ++i) {
+    write_beams(o, S.ih_all.data() + ibt, S.ik_all.data() + ibt, S.nbd[i]);
+    ibt += S.nbd[i];
   }
-  std::fprintf(o, "\n");
-  const bool ng_outer = S.ng > S.naz;
-  const int nrep1 = ng_outer ? S.naz : S.ng, nrep2 = ng_outer ? S.ng : S.naz;
-  for (int r1 = 0; r1 < nrep1; ++r1) {
-    for (int r2 = 0; r2 < nrep2; ++r2) {
-      int t = r1 * nrep2 + r2;
-      std::string line = fortran_e(angle_deg[t], 12, 4);
-      for (int i = 0; i < S.nb; ++i) {
-        if (i > 0 && i % 200 == 0) {
-          std::fprintf(o, "%s\n", line.c_str());
-          line.clear();
-        }
-        line += ",";
-        line += fortran_e(f2[(size_t)t * S.nb + i], 23, 15);
-      }
-      std::fprintf(o, "%s,\n", line.c_str());
-    }
-    std::fprintf(o, "\n");
-  }
+  for (int i = 0; i < S.ndom; ++i)
+    write_rows(o, S.naz, S.ng, f2[i].data(), angle_deg[i].data(), S.nbd[i], 23, 15);
+  std::fclose(o);
+}
+
+// The single-domain file domainsum writes (domainsum.f90:108-119): the reference
+// domain's beams, '(E12.4,200(",",E12.4))' rows.
+void write_domain_sum(const std::string& path, const SurfaceInputs& S, int idomr,
+                      const double* s2, const double* angle_deg) {
+  FILE* o = std::fopen(path.c_str(), "w");
+  if (!o) throw std::runtime_error("cannot write " + path);
+  int ibt = 0;
+  for (int i = 0; i < idomr; ++i) ibt += S.nbd[i];
+  const int mb = S.nbd[idomr];
+  std::fprintf(o, "#azimuths,g-angles,beams\n%4d%4d%4d\n#ih,ik\n", S.naz, S.ng, mb);
+  write_beams(o, S.ih_all.data() + ibt, S.ik_all.data() + ibt, mb);
+  write_rows(o, S.naz, S.ng, s2, angle_deg, mb, 12, 4);
   std::fclose(o);
 }
 }  // namespace trhepd
+
+namespace trhepd {
+void write_domain_curves(const std::string& path, const SurfaceInputs& S,
+                         const std::vector<std::vector<double>>& f2,
+                         const std::vector<std::vector<double>>& angle_deg);
+void write_domain_sum(const std::string& path, const SurfaceInputs& S, int idomr,
+                      const double* s2, const double* angle_deg);
+}  // namespace trhepd
+
+namespace {
+// A value as it reads back from the Fortran-formatted .md header domainsum parses.
+double reread(const std::string& text) { return std::stod(text); }
+
+// surf.exe for NDOM > 1 (surfm.f90:72-90): every domain's srfref (surfio.f90:291-341,
+// azimuth azi + rdom(idom)) into its own resident problem, then the weighted sum of
+// the rotated domains' curves on the device (domainsum.f90:7-121) with the angles,
+// weights and cell angle as domainsum reads them back from the .md header.  Writes
+// the .md file (out_path with its extension replaced by .md) and the summed .s file
+// (out_path).  f2 receives the summed intensities (nangles x the reference domain's
+// beams).
+void surf_run_domains(trhepd_context* C, const char* bulkp, const char* surf, double dz2,
+                      int int_method, int precision, const SurfaceInputs& S0,
+                      const char* out_path, double* f2_out, int max_f2, int* dims) {
+  const int ndom = S0.ndom;
+  if (ndom > kMaxDomains) throw std::invalid_argument("more domains than the domain sum takes");
+  const double rad = std::atan(1.0) / 45.0, deg = 45.0 / std::atan(1.0);
+  cudaStream_t st = C->stream;
+  std::vector<trhepd_problem*> probs;
+  std::vector<SurfaceInputs> Sd(ndom);
+  DevBuf dstart, dlist, ds2;
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(st);
+    for (trhepd_problem* p : probs) {
+      p->release();
+      delete p;
+    }
+    dstart.release();
+    dlist.release();
+    ds2.release();
+  };
+  try {
+    for (int d = 0; d < ndom; ++d) {
+      load_surface_inputs(bulkp, surf, dz2, int_method, Sd[d], d);
+      structure_factors(C, Sd[d]);
+      trhepd_pot_state pot = pot_view(Sd[d]);
+      const SurfaceInputs& S = Sd[d];
+      SolveArgs a{&pot, S.nb, S.ns, S.iv.data(), S.dz, S.ngr, S.nbg.data(), S.iord.data(),
+                  S.ih.data(), S.ik.data(), S.wn, S.ghx, S.ghy, S.gky, S.azi, S.daz, S.gi,
+                  S.dg, S.naz, S.ng, int_method, reinterpret_cast<const double*>(S.t1rec.data())};
+      probs.push_back(new trhepd_problem());
+      prepare(C, a, *probs.back());
+      run_checked(C, *probs.back(), precision);
+    }
+    // domainsum.f90:43-56: the reference domain has the most beams (the first such)
+    int idomr = 0;
+    for (int d = 1; d < ndom; ++d)
+      if (S0.nbd[d] > S0.nbd[idomr]) idomr = d;
+    const int mb = S0.nbd[idomr];
+    const int nang = probs[0]->nang;
+    // values as the .md header carries them (F10.3 degrees, E12.3 weights)
+    char buf[64];
+    auto f103 = [&](double v) {
+      std::snprintf(buf, sizeof buf, "%10.3f", v);
+      return reread(buf);
+    };
+    const double gam = f103(S0.gam * deg);
+    std::vector<double> rdom(ndom), wdom(ndom);
+    for (int d = 0; d < ndom; ++d) {
+      rdom[d] = f103(S0.rdom[d] * deg);
+      wdom[d] = reread(fortran_e(S0.wdom[d], 12, 3));
+    }
+    std::vector<int> off(ndom + 1, 0);
+    for (int d = 0; d < ndom; ++d) off[d + 1] = off[d] + S0.nbd[d];
+    auto reduced = [&](int b, double& gx, double& gy) {  // domainsum.f90:82-86
+      gx = (double)S0.ih_all[b] / S0.nh;
+      gy = (double)S0.ik_all[b] / S0.nk;
+      if (std::fabs(gam - 120.0) < 1e-4) gx = (gx + gx + gy) / std::sqrt(3.0);
+    };
+    // per domain and reference beam, the domain's beams rotating onto it (:76-101)
+    std::vector<int> start((size_t)ndom * (mb + 1), 0), list;
+    for (int d = 0; d < ndom; ++d) {
+      std::vector<std::vector<int>> onto(mb);
+      const double dr = rdom[idomr] - rdom[d];
+      const double cdr = std::cos(dr * rad), sdr = std::sin(dr * rad);
+      for (int ib = 0; ib < S0.nbd[d]; ++ib) {
+        if (d == idomr) {
+          onto[ib].push_back(ib);
+          continue;
+        }
+        double gx, gy;
+        reduced(off[d] + ib, gx, gy);
+        const double gxr = cdr * gx - sdr * gy, gyr = sdr * gx + cdr * gy;
+        for (int ibr = 0; ibr < mb; ++ibr) {
+          double hx, hy;
+          reduced(off[idomr] + ibr, hx, hy);
+          if (std::fabs(gxr - hx) < 1e-4 && std::fabs(gyr - hy) < 1e-4) {
+            onto[ibr].push_back(ib);
+            break;
+          }
+        }
+      }
+      for (int ibr = 0; ibr < mb; ++ibr) {
+        start[(size_t)d * (mb + 1) + ibr] = (int)list.size();
+        list.insert(list.end(), onto[ibr].begin(), onto[ibr].end());
+      }
+      start[(size_t)d * (mb + 1) + mb] = (int)list.size();
+    }
+    if (list.empty()) list.push_back(0);
+    DomainSumArgs A{};
+    A.ndom = ndom;
+    for (int d = 0; d < ndom; ++d) {
+      A.f2[d] = probs[d]->f2.as<double>();
+      A.nb[d] = probs[d]->n;
+      A.w[d] = wdom[d];
+    }
+    A.start = upload(dstart, start, st);
+    A.list = upload(dlist, list, st);
+    double* s2 = (double*)ds2.ensure((size_t)nang * mb * sizeof(double));
+    launch_domain_sum(A, nang, mb, s2, st);
+    CK(cudaGetLastError());
+    std::vector<double> hs2((size_t)nang * mb);
+    CK(cudaMemcpyAsync(hs2.data(), s2, hs2.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    std::vector<std::vector<double>> f2d(ndom), angd(ndom);
+    for (int d = 0; d < ndom; ++d) {
+      f2d[d].resize((size_t)probs[d]->nang * probs[d]->n);
+      angd[d].resize(probs[d]->nang);
+      fetch(C, *probs[d], f2d[d].data(), angd[d].data());
+    }
+    if (out_path) {
+      std::string s_path = out_path, md_path = s_path;
+      const size_t dot = md_path.find_last_of('.'), slash = md_path.find_last_of('/');
+      if (dot != std::string::npos && (slash == std::string::npos || dot > slash))
+        md_path.resize(dot);
+      md_path += ".md";
+      write_domain_curves(md_path, S0, f2d, angd);
+      // domainsum reads every domain's angles into one array: the last domain's stay
+      write_domain_sum(s_path, S0, idomr, hs2.data(), angd[ndom - 1].data());
+    }
+    if (f2_out) {
+      if ((size_t)max_f2 < hs2.size()) throw std::invalid_argument("f2 buffer too small");
+      std::memcpy(f2_out, hs2.data(), hs2.size() * sizeof(double));
+    }
+    if (dims) {
+      dims[0] = mb;
+      dims[1] = nang;
+      dims[2] = Sd[idomr].ns;
+      dims[3] = Sd[idomr].nv;
+    }
+  } catch (...) {
+    cleanup();
+    throw;
+  }
+  cleanup();
+}
+}  // namespace
 
 // =============================================================================
 // C ABI
@@ -1907,10 +2116,23 @@ int trhepd_bulk_run(trhepd_context* ctx, const char* bulk_txt, const char* out_p
                     double* stats) {
   return guarded(ctx, [&] {
     if (!bulk_txt || !out_path) throw std::invalid_argument("null path");
-    BulkInputs B;
-    load_bulk_inputs(bulk_txt, B, ctx->particle == 1 ? 0 : 1);
-    std::vector<std::vector<cd>> records;
-    bulk_solve(ctx, B, records, stats);
+    const int inegpos = ctx->particle == 1 ? 0 : 1;
+    std::vector<BulkInputs> B(1);
+    load_bulk_inputs(bulk_txt, B[0], inegpos, 0);
+    B.resize(B[0].ndom);
+    for (int d = 1; d < B[0].ndom; ++d) load_bulk_inputs(bulk_txt, B[d], inegpos, d);
+    std::vector<std::vector<std::vector<cd>>> records(B.size());
+    double total[4] = {0, 0, 0, 0};
+    for (size_t d = 0; d < B.size(); ++d) {  // one blkref per domain (bulkio.f90:150-214)
+      double st[4] = {0, 0, 0, 0};
+      bulk_solve(ctx, B[d], records[d], st);
+      total[0] += st[0];
+      total[1] = std::max(total[1], st[1]);
+      total[2] = std::max(total[2], st[2]);
+      total[3] += st[3];
+    }
+    if (stats)
+      for (int k = 0; k < 4; ++k) stats[k] = total[k];
     write_bulkp(out_path, B, records);
   });
 }
@@ -1923,6 +2145,11 @@ int trhepd_surf_run(trhepd_context* ctx, const char* bulkp, const char* surf, do
     if (!valid_precision(precision)) throw std::invalid_argument("unknown precision form");
     SurfaceInputs S;
     load_surface_inputs(bulkp, surf, dz2, int_method, S);
+    if (S.ndom > 1) {
+      surf_run_domains(ctx, bulkp, surf, dz2, int_method, precision, S, out_path, f2, max_f2,
+                       dims);
+      return;
+    }
     structure_factors(ctx, S);
     trhepd_pot_state pot = pot_view(S);
     int nang = S.naz * S.ng;

@@ -27,3 +27,32 @@ def read_rocking_curves(path) -> tuple[np.ndarray, np.ndarray, dict]:
     vals = np.array([_fortran_float(t) for t in toks[3 + 2 * nb:]])
     arr = vals.reshape(-1, nb + 1)
     return arr[:, 0], arr[:, 1:], {"naz": naz, "ng": ng, "nb": nb, "beams": ihik}
+
+
+def read_domain_curves(path) -> tuple[list, dict]:
+    """Return ([(angles, f2[nrows, nb_d]) per domain], header) of a multi-domain .md
+    file (surfio.f90:276-287 header, then each domain's srfref rows)."""
+    lines = [ln for ln in open(path).read().split("\n") if not ln.startswith("#")]
+    toks = " ".join(lines).replace(",", " ").split()
+    naz, ng, ndom, nh, nk = (int(t) for t in toks[:5])
+    gam = float(toks[5])
+    p = 6
+    nbd, rdom, wdom = [], [], []
+    for _ in range(ndom):
+        nbd.append(int(toks[p]))
+        rdom.append(float(toks[p + 1]))
+        wdom.append(_fortran_float(toks[p + 2]))
+        p += 3
+    beams = []
+    for nb in nbd:
+        beams.append(np.array([int(t) for t in toks[p:p + 2 * nb]]).reshape(nb, 2))
+        p += 2 * nb
+    vals = np.array([_fortran_float(t) for t in toks[p:]])
+    rows = naz * ng
+    out, q = [], 0
+    for nb in nbd:
+        arr = vals[q:q + rows * (nb + 1)].reshape(rows, nb + 1)
+        out.append((arr[:, 0], arr[:, 1:]))
+        q += rows * (nb + 1)
+    return out, {"naz": naz, "ng": ng, "ndom": ndom, "nh": nh, "nk": nk, "gam_deg": gam,
+                 "nbd": nbd, "rdom_deg": rdom, "wdom": wdom, "beams": beams}
