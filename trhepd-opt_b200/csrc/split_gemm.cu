@@ -801,14 +801,26 @@ __host__ __device__ constexpr uint32_t instr_desc_i8(int nt) {
          | ((uint32_t)(nt >> 3) << 17)  // N
          | ((uint32_t)(BM >> 4) << 24); // M
 }
+// A-operand collector use of one MMA: the MMAs of one A slice (pairs (s, t) for
+// t = 0..S-1-s) run back to back, so the first fills the collector buffer from
+// shared memory, the middle ones use it and the last releases it; an A slice with
+// a single MMA reads shared memory as usual.  Each reuse saves one A tile read
+// (128 x 32 bytes) from shared memory, whose bandwidth bounds this kernel.
+enum CollectorOp { kCollNone = 0, kCollFill = 1, kCollUse = 2, kCollLast = 3 };
+template <int kOp>
 __device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
                                           uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-      : "memory");
+#define TRHEPD_MMA_I8(Q)                                                                   \
+  asm volatile("{\n\t.reg .pred p;\n\t"                                                  \
+               "setp.ne.b32 p, %4, 0;\n\t"                                                \
+               "tcgen05.mma.cta_group::1.kind::i8" Q " [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem), \
+               "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)                          \
+               : "memory")
+  if constexpr (kOp == kCollFill) TRHEPD_MMA_I8(".collector::a::fill");
+  else if constexpr (kOp == kCollUse) TRHEPD_MMA_I8(".collector::a::use");
+  else if constexpr (kOp == kCollLast) TRHEPD_MMA_I8(".collector::a::lastuse");
+  else TRHEPD_MMA_I8("");
+#undef TRHEPD_MMA_I8
 }
 
 // Balanced base-256 digits of X = rint(x * scale), scale = 2^(7 - e + 8(S-1)),
@@ -933,6 +945,11 @@ __device__ __forceinline__ void tile_counter_done(int* counter, unsigned ctas) {
     __threadfence();
   }
 }
+
+#ifndef TRHEPD_COLLECT_A
+#define TRHEPD_COLLECT_A 1
+#endif
+constexpr bool kCollectA = TRHEPD_COLLECT_A != 0;  // A-slice reuse through the MMA collector
 
 // Persistent INT8 stage product: one CTA per SM (or fewer) takes tiles from a
 // per-launch counter; warp 0 claims them and issues TMA, warp 1 the MMAs of every slice pair (s, t) with s + t < S into
@@ -1096,7 +1113,11 @@ __global__ void __launch_bounds__(P_THREADS, 1)
                   const int L = s + t;
                   const uint64_t ad = sw64_desc(sa + s * i8::A_SLICE_BYTES + kk * 32);
                   const uint64_t bd = sw64_desc(sb + t * BSL + kk * 32);
-                  tc_mma_i8(tmem + L * NTS, ad, bd, idesc, started[L] ? 1u : 0u);
+                  const uint32_t acc = started[L] ? 1u : 0u;
+                  if (!kCollectA || S - s == 1) tc_mma_i8<kCollNone>(tmem + L * NTS, ad, bd, idesc, acc);
+                  else if (t == 0) tc_mma_i8<kCollFill>(tmem + L * NTS, ad, bd, idesc, acc);
+                  else if (t == S - s - 1) tc_mma_i8<kCollLast>(tmem + L * NTS, ad, bd, idesc, acc);
+                  else tc_mma_i8<kCollUse>(tmem + L * NTS, ad, bd, idesc, acc);
                   started[L] = true;
                 }
               }
