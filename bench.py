@@ -282,12 +282,13 @@ def serve_leg(device: int, seconds: float, load: float, precision: int, seed: in
     return out
 
 
-def uneven_leg(ctx, precision: int, per_n: int = 8, seed: int = 0) -> dict:
+def uneven_leg(ctx, precision: int, per_n: int = 64, seed: int = 0) -> dict:
     """Candidate-structure batch of uneven beam counts: per_n jittered candidates
     (sigma 0.1 A) of a base structure for each N in {23, 47, 95, 191}, 61 angles,
     15 A in 0.02 A slices, all solved by one trhepd_batch_solve (the N <= 64 ones
-    in shared fused launches); two batch solves warm up, the next two are
-    timed (device time from the library's events)."""
+    in shared fused launches); two batch solves warm up, the next one is timed
+    (device time from the library's events).  per_n = 64 is the 256-structure
+    candidate batch."""
     tmp = Path(tempfile.mkdtemp(prefix="trhepd_uneven_"))
     probs, nang = [], 0
     for n in (23, 47, 95, 191):
@@ -305,7 +306,7 @@ def uneven_leg(ctx, precision: int, per_n: int = 8, seed: int = 0) -> dict:
     for _ in range(2):  # buffers sized, graphs of the larger problems captured
         surface.solve_batch(ctx, rps, precision)
     ms = []
-    for _ in range(2):
+    for _ in range(1):
         surface.solve_batch(ctx, rps, precision)
         ms.append(ctx.last_stats()["device_ms"])
     st = ctx.last_stats()
@@ -363,7 +364,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven candidate batch")
     ap.add_argument("--no-bulk", action="store_true", help="skip the bulk boundary solve leg")
-    ap.add_argument("--uneven-per-n", type=int, default=8,
+    ap.add_argument("--uneven-per-n", type=int, default=64,
                     help="candidates per beam count in the uneven batch (64: 256 structures)")
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-load", type=float, default=0.5,
@@ -563,9 +564,21 @@ def main():
     fp64 = None
     f2_64 = None
     if split and not args.no_fp64:
-        st, f2_64 = compare(native.FP64)
+        # the warm-up solve is profiled (per-launch events of the FP64 stage kernel),
+        # the second one is timed without events
+        ctx.set_option(native.OPT_PROFILE, 1)
+        st64p = solve_ms(native.FP64)
+        ctx.set_option(native.OPT_PROFILE, 0)
+        st = solve_ms(native.FP64)
+        _, f2_64 = rp.fetch()
         fp64 = {"value": nang / (st["device_ms"] / 1e3), "ms_per_step": st["device_ms"],
-                "split_speedup": (st["device_ms"] / ms_per_step)}
+                "split_speedup": (st["device_ms"] / ms_per_step),
+                "roofline": fp64_roofline(st64p, nang, n, f64_peak, peaks,
+                                          NCU_TRAFFIC.get((args.workload, "fp64", 0))),
+                "breakdown": {"solve_ms": st64p["device_ms"],
+                              "stage_products_ms": st64p["stage_kernel_ms"],
+                              "renormalisations_ms": st64p["renorm_ms"],
+                              "renormalisations": st64p["renormalisations"]}}
         fp64.update({"split_" + k: v for k, v in errors(f2_main, f2_64).items()})
     bf16 = None
     if prec == native.SPLIT_INT8 and not args.no_bf16:
@@ -657,6 +670,34 @@ def main():
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def fp64_roofline(stp: dict, nang: int, n: int, f64_peak, peaks: dict, traffic) -> dict:
+    """Roofline of k_stage_gemm_f64 from one profiled FP64 solve: FP64 tensor work
+    8*nang*N^3 per launch (complex N^3 per angle) against cuBLAS DGEMM measured in
+    the run, and the algorithmic HBM bytes (Q, P read; P, Q' written) against
+    MEASURED_PEAKS.json hbm_gbs."""
+    nprod = max(stp["stage_products"], 1)
+    ms = stp["tensor_kernel_ms"] / nprod
+    flop = 8.0 * nang * n ** 3
+    achieved = flop / (ms * 1e-3) / 1e12
+    peak = f64_peak["sustained"] if f64_peak else None
+    hbm_bytes = 4 * 16.0 * nang * n * n
+    hbm_peak = peaks.get("hbm_gbs") or 6650.0
+    hbm_ms = hbm_bytes / (hbm_peak * 1e9) * 1e3
+    flop_ms = flop / (peak * 1e12) * 1e3 if peak else 0.0
+    return {"bound": "tensor" if flop_ms >= hbm_ms else "hbm", "achieved": achieved,
+            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+            "traffic": traffic * nang / 16.0 if traffic else None,
+            "kernel": "k_stage_gemm_f64 (FP64 DMMA mma.sync.m16n8k4)",
+            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run, sustained over a 3 s loop",
+            "avg_launch_ms": ms,
+            "hbm": {"algorithmic_bytes_per_launch": hbm_bytes, "peak_gbs": hbm_peak,
+                    "achieved_gbs": hbm_bytes / (ms * 1e-3) / 1e9, "frac": hbm_ms / ms,
+                    "time_at_peak_ms": hbm_ms},
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                              "on the 16-angle profiling case, scaled by angles "
+                              "(profiles/k_stage_gemm_f64_dense521s.md)" if traffic else None}
 
 
 def surface_slices(workdir: Path, s) -> int:

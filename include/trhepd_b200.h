@@ -135,7 +135,7 @@ int trhepd_plane_group_images(int nsg, int ma, int mb, int na, int nb, double x,
 
 /*
  * Stage potential tables of an integrator: v, vi complex (nv, ncol) with
- * ncol = ns for int_method 4, 6*ns+1 for 5, 11*ns+1 for 6 and 2*ns+1 for 7.
+ * ncol = ns for int_method 4, 6*ns+1 for 5, 11*ns+1 for 6 and 2*ns+1 for 7 and 8.
  * Replaces hp_int_init4/6 (sim-trhepd-rheed/src/surf_prkn.f90:174-197),
  * m2_int_init (surf_magnus.f90:4-20), rk4_int_init (surf_rk.f90:4-25) and
  * comp_scpot (surfio.f90:29-41).
@@ -144,7 +144,7 @@ int trhepd_potential_table(trhepd_context* ctx, const trhepd_pot_state* pot, int
                            int ns, double dz, double* v, double* vi, int* ncol);
 
 /*
- * Same tables as trhepd_potential_table (every int_method 1-7), for callers that
+ * Same tables as trhepd_potential_table (every int_method 1-8), for callers that
  * cannot allocate device memory (a host that hands the whole GPU to its own memory
  * pool at start-up, or a service whose device memory is planned once): no
  * cudaMalloc/cudaFree, no context.  Its device scratch (input copies and the table)
@@ -156,7 +156,7 @@ int trhepd_potential_table(trhepd_context* ctx, const trhepd_pot_state* pot, int
  * the last call's contents; nothing in it has to start at zero, since each call
  * writes what it reads), so calls whose GPU work overlaps race.  Returns
  * TRHEPD_ENOMEM when the inputs and the table need more than the 32 MiB, and
- * TRHEPD_EINVAL for an int_method outside 1-7.
+ * TRHEPD_EINVAL for an int_method outside 1-8.
  * This entry point has no counterpart in the reference.
  */
 int trhepd_potential_table_noalloc(const trhepd_pot_state* pot, int int_method, int ns,
@@ -166,7 +166,8 @@ int trhepd_potential_table_noalloc(const trhepd_pot_state* pot, int int_method, 
  * Surface solve of every (azimuth, glancing angle) of one domain in one batch.
  * Replaces srfref (sim-trhepd-rheed/src/surflf.f90:7-171) including its
  * integrator call (lf_int_spa surf_magnus.f90:46-110, hp_int4 / hp_int6
- * surf_prkn.f90:123-141, rk4_int surf_rk.f90:27-91: int_method 4-7) and the intensity
+ * surf_prkn.f90:123-141, rk4_int surf_rk.f90:27-91, rk4_intgs surf_rk.f90:93-156:
+ * int_method 4-8; the Magnus integrators 1-3 as well) and the intensity
  * formula (surflf.f90:142-151).  Arguments keep srfref's names and meaning;
  * t1_records holds the bulk reflection records srfref reads from unit 1
  * (surflf.f90:65-72): nrep1*nrep2 angles, each ngr blocks of nbg(l)^2 complex

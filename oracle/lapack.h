@@ -48,4 +48,14 @@ inline void ztrsm(char side, char uplo, char ta, char diag, int m, int n, cplx a
                   const cplx* a, int lda, cplx* b, int ldb) {
   scipy_ztrsm_(&side, &uplo, &ta, &diag, &m, &n, &alpha, a, &lda, b, &ldb, 1, 1, 1, 1);
 }
+// C = alpha*op(A)^H op(A) + beta*C (Hermitian rank-k update), column-major
+inline void zherk(char uplo, char tr, int n, int k, double alpha, const cplx* a, int lda,
+                  double beta, cplx* c, int ldc) {
+  scipy_zherk_(&uplo, &tr, &n, &k, &alpha, a, &lda, &beta, c, &ldc, 1, 1);
+}
+inline int zpotrf(char uplo, int n, cplx* a, int lda) {
+  int info = 0;
+  scipy_zpotrf_(&uplo, &n, a, &lda, &info, 1);
+  return info;
+}
 }  // namespace oracle

@@ -1208,6 +1208,183 @@ static void rk4_int(double dz, int ns, int nb, int nv, CMat& f, const cplx* g, c
     for (int i = 0; i < nb; ++i) f(i, j) = std::conj(t1(j, nb + i));
 }
 
+// ---------------------------------------------------------------- int_method 8
+// invstrans: [q; p] = S^{-1} [I; f], S^{-1} = 2 [G^{-1}, G^{-1}; i I, -i I] up to the
+// factor the reference drops (matcomp.f90:89-115)
+static void invstrans(int n, CMat& q, CMat& p, const CMat& f, const cplx* g) {
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      const cplx ig = 1.0 / g[i];
+      if (i == j) {
+        q(i, j) = ig + ig * f(i, j);
+        p(i, j) = cplx(0, -1) + cplx(0, 1) * f(i, j);
+      } else {
+        q(i, j) = ig * f(i, j);
+        p(i, j) = cplx(0, 1) * f(i, j);
+      }
+    }
+}
+
+// strans + matAdivB2: [q; p] <- S [q; p], then p <- p q^{-1} as (q^T \ p^T)^T
+// (matcomp.f90:117-137, 5-20)
+static void strans(int n, CMat& q, CMat& p, const cplx* g, std::vector<int>& piv) {
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      const cplx x = q(i, j), y = p(i, j);
+      q(i, j) = g[i] * x + cplx(0, 1) * y;
+      p(i, j) = g[i] * x - cplx(0, 1) * y;
+    }
+  CMat t1(n, 2 * n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      t1(i, j) = q(j, i);
+      t1(i, n + j) = p(j, i);
+    }
+  matAbdivB(n, t1.data(), n, piv);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) p(i, j) = t1(j, n + i);
+}
+
+// vvi2matf: the stage matrix acting on q from the left (matcomp.f90:281-306); it is
+// the conjugate transpose of vvi2mate's
+static void vvi2matf(int n, int nv, const cplx* v, const cplx* vi, const int* iv, const cplx* g,
+                     CMat& t) {
+  std::vector<cplx> v0(nv), v1(nv);
+  for (int k = 0; k < nv; ++k) {
+    v0[k] = -(v[k] + vi[k]);
+    v1[k] = std::conj(vi[k] - v[k]);
+  }
+  for (int j = 0; j < n; ++j) {
+    for (int i = 0; i < j; ++i) t(i, j) = v1[iv[(size_t)i * n + j] - 1];
+    t(j, j) = v0[0] - g[j] * g[j];
+    for (int i = j + 1; i < n; ++i) t(i, j) = v0[iv[(size_t)j * n + i] - 1];
+  }
+}
+
+// bcgs / cqr: CholeskyQR of T = [q; p] (2n x n): C = T^H T (zherk, upper), C = R^H R
+// (zpotrf), T <- T R^{-1} (ztrsm) (matgs.f90:5-35)
+static void bcgs(int n, CMat& q, CMat& p) {
+  const int m = 2 * n;
+  std::vector<cplx> t((size_t)m * n), c((size_t)n * n, cplx(0, 0));
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      t[(size_t)j * m + i] = q(i, j);
+      t[(size_t)j * m + n + i] = p(i, j);
+    }
+  zherk('U', 'C', n, m, 1.0, t.data(), m, 0.0, c.data(), n);
+  zpotrf('U', n, c.data(), n);
+  ztrsm('R', 'U', 'N', 'N', m, n, cplx(1, 0), c.data(), n, t.data(), m);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      q(i, j) = t[(size_t)j * m + i];
+      p(i, j) = t[(size_t)j * m + n + i];
+    }
+}
+
+// power_step / power_est: power iteration on [q; p]^H [q; p] with the vector x kept
+// between calls; s < 0 initialises x; at most s steps, stopping when the vector
+// moves by < 1e-2 or the estimate grows by < 1e-2 of itself (matcomp.f90:530-594;
+// the reference also prints every step, which has no effect on the result)
+static void power_step(int n, const CMat& q, const CMat& p, std::vector<cplx>& x, double& d,
+                       double& dp) {
+  std::vector<cplx> y(2 * (size_t)n), z(n);
+  for (int i = 0; i < n; ++i) {
+    cplx a(0, 0), b(0, 0);
+    for (int j = 0; j < n; ++j) {
+      a += q(i, j) * x[j];
+      b += p(i, j) * x[j];
+    }
+    y[i] = a;
+    y[n + i] = b;
+  }
+  for (int j = 0; j < n; ++j) {
+    cplx a(0, 0);
+    for (int i = 0; i < n; ++i) a += std::conj(q(i, j)) * y[i];
+    for (int i = 0; i < n; ++i) a += std::conj(p(i, j)) * y[n + i];
+    z[j] = a;
+  }
+  cplx cr(0, 0);
+  double dn = 0.0;
+  for (int i = 0; i < n; ++i) {
+    dn = dn + z[i].real() * z[i].real() + z[i].imag() * z[i].imag();
+    cr = cr + std::conj(x[i]) * z[i];
+  }
+  d = std::abs(cr);
+  dn = 1.0 / std::sqrt(dn);
+  dp = 0.0;
+  for (int i = 0; i < n; ++i) {
+    z[i] = z[i] * dn;
+    const cplx c = z[i] - x[i];
+    dp = dp + c.real() * c.real() + c.imag() * c.imag();
+    x[i] = z[i];
+  }
+  dp = std::sqrt(dp);
+}
+
+static double power_est(int n, const CMat& q, const CMat& p, std::vector<cplx>& x, int s) {
+  if (s < 0) {
+    x.assign(n, cplx(1.0, 1.0) / std::sqrt(2.0 * n));
+    return -1.0;
+  }
+  double d0 = -1.0, d = 0.0, dp = 0.0;
+  for (int i = 1; i <= s; ++i) {
+    power_step(n, q, p, x, d, dp);
+    if (dp < 1e-2 || d - d0 < 1e-2 * d) break;
+    d0 = d;
+  }
+  return d;
+}
+
+// rk4_intgs: classical RK4 on [q; p] with CholeskyQR re-orthogonalisation when the
+// power estimate of ||[q; p]||^2 exceeds 1e2 (surf_rk.f90:93-156)
+static void rk4_intgs(double dz, int ns, int nb, int nv, CMat& f, const cplx* g, const int* iv,
+                      const cplx* v, const cplx* vi, IntStats& st) {
+  CMat q(nb, nb), p(nb, nb), q2(nb, nb), m0(nb, nb), m1(nb, nb), m2(nb, nb);
+  CMat r1(nb, nb), s1(nb, nb), r2(nb, nb), s2(nb, nb), r3(nb, nb), s3(nb, nb), r4(nb, nb),
+      s4(nb, nb);
+  std::vector<cplx> x;
+  std::vector<int> piv;
+  const size_t nn = (size_t)nb * nb;
+  invstrans(nb, q, p, f, g);
+  bcgs(nb, q, p);
+  power_est(nb, q, p, x, -100);
+  vvi2matf(nb, nv, v, vi, iv, g, m2);
+  for (int l = 1; l <= ns; ++l) {
+    m0.a = m2.a;
+    vvi2matf(nb, nv, v + (size_t)(2 * l - 1) * nv, vi + (size_t)(2 * l - 1) * nv, iv, g, m1);
+    vvi2matf(nb, nv, v + (size_t)(2 * l) * nv, vi + (size_t)(2 * l) * nv, iv, g, m2);
+    r1.a = p.a;
+    zgemm('N', 'N', nb, nb, nb, 1.0, m0.data(), nb, q.data(), nb, 0.0, s1.data(), nb);
+    for (size_t e = 0; e < nn; ++e) {
+      q2.a[e] = q.a[e] + 0.5 * dz * r1.a[e];
+      r2.a[e] = p.a[e] + 0.5 * dz * s1.a[e];
+    }
+    zgemm('N', 'N', nb, nb, nb, 1.0, m1.data(), nb, q2.data(), nb, 0.0, s2.data(), nb);
+    for (size_t e = 0; e < nn; ++e) {
+      q2.a[e] = q.a[e] + 0.5 * dz * r2.a[e];
+      r3.a[e] = p.a[e] + 0.5 * dz * s2.a[e];
+    }
+    zgemm('N', 'N', nb, nb, nb, 1.0, m1.data(), nb, q2.data(), nb, 0.0, s3.data(), nb);
+    for (size_t e = 0; e < nn; ++e) {
+      q2.a[e] = q.a[e] + dz * r3.a[e];
+      r4.a[e] = p.a[e] + dz * s3.a[e];
+    }
+    zgemm('N', 'N', nb, nb, nb, 1.0, m2.data(), nb, q2.data(), nb, 0.0, s4.data(), nb);
+    for (size_t e = 0; e < nn; ++e) {
+      q.a[e] = q.a[e] + (dz / 6) * (r1.a[e] + 2.0 * r2.a[e] + 2.0 * r3.a[e] + r4.a[e]);
+      p.a[e] = p.a[e] + (dz / 6) * (s1.a[e] + 2.0 * s2.a[e] + 2.0 * s3.a[e] + s4.a[e]);
+    }
+    st.gemms += 4;
+    const double d = power_est(nb, q, p, x, nb);
+    if (d > 1e2) {
+      bcgs(nb, q, p);
+      st.renorm++;
+    }
+  }
+  strans(nb, q, p, g, piv);
+  f.a = p.a;
+}
+
 // ---------------------------------------------------------------- surface model
 // mod_scpot3 + surfio state (sim-trhepd-rheed/src/surfio.f90:18-58, 60-381)
 struct SurfModel {
@@ -1518,6 +1695,7 @@ static int build_potential(const SurfModel& S, const SurfModel::Domain& D, int m
       break;
     }
     case 7:
+    case 8:  // rk4_int_init serves both (surflf.f90:36-37)
       for (int l = 1; l <= ns; ++l) {
         double iz = dz * (l - 1);
         depth.push_back(iz);
@@ -1526,7 +1704,7 @@ static int build_potential(const SurfModel& S, const SurfModel::Domain& D, int m
       depth.push_back(dz * ns);
       break;
     default:
-      throw std::runtime_error("int_method must be 1..7");
+      throw std::runtime_error("int_method must be 1..8");
   }
   int ncol = (int)depth.size();
   v.assign((size_t)nv * ncol, cplx(0, 0));
@@ -1589,6 +1767,9 @@ static void solve_one(const SurfModel& S, const SurfModel::Domain& D, int nb, co
       break;
     case 7:
       rk4_int(S.dzs, S.ns, nb, nv, f, gma.data(), iv, v, vi, st);
+      break;
+    case 8:
+      rk4_intgs(S.dzs, S.ns, nb, nv, f, gma.data(), iv, v, vi, st);
       break;
   }
   int nb0 = 0;
@@ -2189,6 +2370,7 @@ int oracle_surface_solve(void* hh, int first, int count, double* f2, double* ang
   int nb = S.nbd[0];
   int total = a.nrep1 * a.nrep2;
   if (first < 0 || count < 0 || first + count > total) return -1;
+  scipy_openblas_set_num_threads(1);  // one angle per OpenMP thread, serial BLAS inside
 #pragma omp parallel for schedule(dynamic)
   for (int t = first; t < first + count; ++t) {
     int irep1 = t / a.nrep2, irep2 = t % a.nrep2;

@@ -14,7 +14,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OUT = HERE / "_lib" / "libtrhepd_b200.so"
 SOURCES = ["kernels_f64.cu", "split_gemm.cu", "bulk.cu", "magnus.cu", "small.cu", "solver.cu",
-           "curves.cu", "noalloc.cu",
+           "curves.cu", "noalloc.cu", "cholqr.cu",
            "host_model.cpp", "bulk_model.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -29,6 +29,7 @@ struct Integrator {
   Family family = kRkn;
   int s = 6;                   // RKN stages per slice
   const double* bab = nullptr; // RKN coefficients (b1, a1, b2, a2, ...)
+  bool gs = false;             // RK4 with CholeskyQR re-orthogonalisation (int_method 8)
 };
 
 inline Integrator integrator_for(int method) {
@@ -40,10 +41,11 @@ inline Integrator integrator_for(int method) {
     case 5: return {5, kRkn, 6, kRkn46};
     case 6: return {6, kRkn, 11, kRkn611};
     case 7: return {7, kRk4, 2, nullptr};
+    case 8: return {8, kRk4, 2, nullptr, true};  // rk4_intgs: rk4_int_init's table
     default:
       throw std::invalid_argument(
-          "int_method must be 1-3 (Magnus 2/4/6), 4 (leapfrog), 5 (RKN-4), 6 (RKN-6) or 7 (RK4)"
-          " on the GPU path");
+          "int_method must be 1-3 (Magnus 2/4/6), 4 (leapfrog), 5 (RKN-4), 6 (RKN-6), 7 (RK4) or"
+          " 8 (RK4 with CholeskyQR)");
   }
 }
 

@@ -86,11 +86,22 @@ void launch_cond_est(const cd* Q, int nang, int n, int ld, int force, int* flag,
 constexpr int kMaxBeams = 832;
 
 // K8: Q^{-1} P by blocked Gauss-Jordan with partial pivoting, per flagged angle.
-// scratch: gj_scratch_bytes(nang, n) bytes.  fused: complex multiply-adds as four
-// FMAs (faster, different rounding; the split forms' renormalisations).
+// scratch: gj_scratch_bytes(nang, n) bytes.  arith: the rounding of the complex
+// multiply-adds:
+//   kGjProductFirst  products formed first, then added (the reference's rounding),
+//                    shared-memory panel and one thread per trailing column (the
+//                    boundary transforms and the bulk solve),
+//   kGjFused         four fused multiply-adds per complex product in the
+//                    row-per-thread panel, the trailing update on the FP64 tensor
+//                    path (the split forms' renormalisations),
+//   kGjFp64Mma       the row-per-thread panel with products formed first, the
+//                    trailing update on the FP64 tensor path (the FP64 form's
+//                    renormalisations).
+// Beyond 640 beams every form takes the shared-memory kernels.
+enum GjArith { kGjProductFirst = 0, kGjFused = 1, kGjFp64Mma = 2 };
 size_t gj_scratch_bytes(int nang, int n);
 void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld, void* scratch,
-                         unsigned* status, cudaStream_t st, bool fused = false);
+                         unsigned* status, cudaStream_t st, int arith = kGjProductFirst);
 
 // RK4 stage combination (rk4_int, surf_rk.f90:27-91); see kernels_f64.cu.
 void launch_rk4_combine(cd* Q, cd* P, cd* Qt, cd* Pt, cd* KP, cd* SQ, cd* SP, int j, double w,

@@ -636,6 +636,111 @@ __global__ void k_gj_panel(const cd* __restrict__ Q, const int* __restrict__ fla
   }
 }
 
+// Panel step for n <= kPanelRowsMax rows, one row per thread: Gauss-Jordan
+// elimination of the panel columns in place, with the pivot rule of k_gj_panel.
+// Column step jj pivots, swaps rows col and p, scales the pivot row by r = 1/d and
+// eliminates the column from every other row i with the multiplier g = f_i r
+// (f_i the row's entry in column jj): x_k <- x_k - g u_k for the other columns,
+// and the freed slot jj takes -g.  After w steps the panel holds E with
+// E [B1; B_other] = [I; 0] over the pivot columns: its pivot rows are B1^{-1}, its
+// other rows -B_other B1^{-1}.  The trailing update is then, after the same row
+// swaps, C1' = E_pivot C1 for the pivot rows and C' = C + E_i C1 for the others.
+// One barrier per column: each warp publishes its best candidate row, and the
+// owner of row col publishes that row, before it.
+constexpr int kPanelRowsMax = 640;
+template <bool kF, int kMaxT>
+__global__ void __launch_bounds__(kMaxT, 1)
+    k_gj_panel_rows(const cd* __restrict__ Q, const int* __restrict__ flag, int n, int ld, int c0,
+                    int w, int* __restrict__ piv, cd* __restrict__ E, unsigned* status) {
+  static_assert(kWMax == 16, "one 16-column panel per thread row");
+  const int a = blockIdx.x;
+  if (flag && !flag[a]) return;
+  constexpr int kMaxWarps = kMaxT / 32;
+  __shared__ double cand_v[2][kMaxWarps];
+  __shared__ int cand_i[2][kMaxWarps];
+  __shared__ cd cand_row[2][kMaxWarps][kWMax];
+  __shared__ cd crow[2][kWMax];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  const unsigned full = 0xffffffffu;
+  cd x[kWMax];
+  {
+    const cd* A = Q + (size_t)a * n * ld + (size_t)min(tid, n - 1) * ld + c0;
+#pragma unroll
+    for (int k = 0; k < kWMax; ++k) x[k] = (tid < n && k < w) ? A[k] : cd{0.0, 0.0};
+  }
+  // a runtime loop over the columns (an unrolled one overflows the instruction
+  // cache); column jj of the row is picked by a select over the 16 registers
+  for (int jj = 0; jj < w; ++jj) {
+    const int col = c0 + jj, buf = jj & 1;
+    // ---- this warp's candidate: max |re|+|im| over rows >= col, lowest row on ties
+    cd xj = x[0];
+#pragma unroll
+    for (int k = 1; k < kWMax; ++k)
+      if (k == jj) xj = x[k];
+    const bool live = tid >= col && tid < n;
+    double best = live ? cabs1(xj) : -1.0;
+    int bi = live ? tid : n;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(full, best, o);
+      const int oi = __shfl_xor_sync(full, bi, o);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    if (tid == bi) {
+#pragma unroll
+      for (int k = 0; k < kWMax; ++k) cand_row[buf][warp][k] = x[k];
+    }
+    if (lane == 0) {
+      cand_v[buf][warp] = best;
+      cand_i[buf][warp] = bi;
+    }
+    if (tid == col) {
+#pragma unroll
+      for (int k = 0; k < kWMax; ++k) crow[buf][k] = x[k];
+    }
+    __syncthreads();
+    // ---- the block's pivot among the warp candidates
+    best = (lane < nw) ? cand_v[buf][lane] : -1.0;
+    bi = (lane < nw) ? cand_i[buf][lane] : n;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(full, best, o);
+      const int oi = __shfl_xor_sync(full, bi, o);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    const int p = __shfl_sync(full, bi, 0), pw = p >> 5;  // row p is thread p's
+    if (tid == 0) piv[a * kWMax + jj] = p;
+    const cd* u = cand_row[buf][pw];  // the pivot row (old row p)
+    const cd d = u[jj];  // shared memory: a dynamic index is fine
+    if (d.x == 0.0 && d.y == 0.0 && tid == 0) atomicOr(status, kStatusZeroPivot);
+    const cd r = cdiv(cd{1.0, 0.0}, d);
+    if (tid == col) {
+#pragma unroll
+      for (int k = 0; k < kWMax; ++k) x[k] = (k == jj) ? r : u[k] * r;
+    } else {
+      if (tid == p) {  // row p now holds the old row col
+#pragma unroll
+        for (int k = 0; k < kWMax; ++k) x[k] = crow[buf][k];
+        xj = crow[buf][jj];
+      }
+      const cd g = xj * r;
+#pragma unroll
+      for (int k = 0; k < kWMax; ++k) x[k] = (k == jj) ? -g : gj_sub<kF>(x[k], g, u[k]);
+    }
+  }
+  if (tid < n) {
+    cd* e = E + ((size_t)a * n + tid) * kWMax;
+#pragma unroll
+    for (int k = 0; k < kWMax; ++k) e[k] = x[k];
+  }
+}
+
 // Each CTA owns kUpdCols of the remaining columns of one angle.
 // One thread per column of the trailing matrix (Q columns right of the panel,
 // then every P column), 128 columns per block: the column's pivot-row values C1
@@ -737,28 +842,236 @@ __global__ void __launch_bounds__(kUpdCols, 4) k_gj_update(cd* __restrict__ Q, c
   }
 }
 
+// Trailing update from the panel's E on the FP64 tensor path (fused rounding).
+// C' = C + E C1 for every row (C = 0 for the pivot rows, whose E rows are B1^{-1})
+// is a complex GEMM with K = 16.  The CTA owns kMmaCols trailing columns of one
+// angle; after a common setup its four warps work independently on 16-row strips
+// (warp w: strips w, w+4, ...).  Per strip: m16n8k4 FP64 MMAs, four real MMAs per
+// complex product, accumulators initialised from C; the warp's E rows come
+// through its own two cp.async buffers and the next strip's C values are loaded
+// into registers while the current strip's MMAs run.
+// Row swaps: thread 0 replays the panel's swap sequence on the (at most 2 kW)
+// touched row positions, so every position knows which original row its value
+// comes from; C1 (the pivot rows after the swaps) and the values that end in
+// touched rows below the panel are read into shared memory before any row is
+// written, and a strip reads a touched row from that stash.
+constexpr int kMmaCols = 32;        // complex columns per CTA (4 n8 tiles)
+constexpr int kStrip = 16;          // rows per warp strip
+constexpr int kEStr = kWMax + 4;    // complex entries per E row in shared memory
+constexpr int kC1Str = kMmaCols + 2;
+struct MmaUpdSmem {
+  cd E[4][2][kStrip][kEStr];
+  cd C1[kWMax][kC1Str];
+  cd stash[kWMax][kMmaCols];
+  short rslot[kMaxBeams];
+  int tpos[2 * kWMax], tsrc[2 * kWMax];
+  int ntouched;
+};
+__global__ void __launch_bounds__(128, 3)
+    k_gj_update_mma(cd* __restrict__ Q, cd* __restrict__ P, const int* __restrict__ flag, int n,
+                    int ld, int c0, int w, const int* __restrict__ pivs,
+                    const cd* __restrict__ E) {
+  constexpr int kW = kWMax, kNi = kMmaCols / 8;
+  const int a = blockIdx.y;
+  if (flag && !flag[a]) return;
+  extern __shared__ __align__(16) unsigned char mma_dyn[];
+  MmaUpdSmem& sm = *reinterpret_cast<MmaUpdSmem*>(mma_dyn);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int qrest = n - (c0 + w), total = qrest + n;
+  const int vc0 = blockIdx.x * kMmaCols;
+  cd* Qa = Q + (size_t)a * n * ld;
+  cd* Pa = P + (size_t)a * n * ld;
+  // row 0 of trailing column vc (vc < total)
+  auto colp = [&](int vc) -> cd* { return vc < qrest ? Qa + (c0 + w + vc) : Pa + (vc - qrest); };
+  const cd* Ea = E + (size_t)a * n * kW;
+  for (int i = tid; i < n; i += 128) sm.rslot[i] = -1;
+  __syncthreads();
+  if (tid == 0) {
+    int nt = w;
+    for (int q = 0; q < w; ++q) sm.tpos[q] = sm.tsrc[q] = c0 + q;
+    for (int jj = 0; jj < w; ++jj) {
+      const int r1 = pivs[a * kW + jj];
+      int i1 = -1;
+      for (int q = 0; q < nt; ++q)
+        if (sm.tpos[q] == r1) i1 = q;
+      if (i1 < 0) {
+        i1 = nt++;
+        sm.tpos[i1] = sm.tsrc[i1] = r1;
+      }
+      const int s = sm.tsrc[jj];
+      sm.tsrc[jj] = sm.tsrc[i1];
+      sm.tsrc[i1] = s;
+    }
+    for (int q = w; q < nt; ++q) sm.rslot[sm.tpos[q]] = (short)(q - w);
+    sm.ntouched = nt;
+  }
+  __syncthreads();
+  {
+    const int nt = sm.ntouched;
+#pragma unroll
+    for (int it = 0; it < 2 * kW * kMmaCols / 128; ++it) {
+      const int e = tid + it * 128, q = e / kMmaCols, c = e % kMmaCols, vc = vc0 + c;
+      if (q < kW) {
+        sm.C1[q][c] =
+            (q < w && vc < total) ? colp(vc)[(size_t)sm.tsrc[q] * ld] : cd{0.0, 0.0};
+      } else {  // stash slot s: touched entry w + s (rows below the panel)
+        const int sl = q - kW, te = w + sl;
+        if (te < nt) sm.stash[sl][c] = vc < total ? colp(vc)[(size_t)sm.tsrc[te] * ld] : cd{0.0, 0.0};
+      }
+    }
+  }
+  __syncthreads();
+  // this thread's 8 columns are vc0 + ni * 8 + 2t + j; addresses formed on use
+  const int vt = vc0 + 2 * t;
+  auto fetch_e = [&](int strip, int b) {
+#pragma unroll
+    for (int q = 0; q < kStrip * kW / 32; ++q) {
+      const int e = lane + q * 32, r = e / kW, k = e % kW, row = strip * kStrip + r;
+      const cd* src = Ea + (size_t)min(row, n - 1) * kW + k;
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sm.E[warp][b][r][k]);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+                   "r"(row < n ? 16 : 0)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // C values of a strip in accumulator order (0 in the pivot rows, stash values in
+  // touched rows)
+  auto load_c = [&](int strip, double (&cr)[kNi][4], double (&ci)[kNi][4]) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = strip * kStrip + g + 8 * h;
+      const bool live = r < n && !(r >= c0 && r < c0 + w);
+      const int sl = live ? sm.rslot[r] : -1;
+#pragma unroll
+      for (int ni = 0; ni < kNi; ++ni)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int vc = vt + ni * 8 + j;
+          cd v = cd{0.0, 0.0};
+          if (live && vc < total)
+            v = sl >= 0 ? sm.stash[sl][ni * 8 + 2 * t + j] : colp(vc)[(size_t)r * ld];
+          cr[ni][2 * h + j] = v.x;
+          ci[ni][2 * h + j] = v.y;
+        }
+    }
+  };
+  const int nstrips = ceil_div(n, kStrip);
+  double cr[kNi][4], ci[kNi][4];
+  if (warp < nstrips) {
+    fetch_e(warp, 0);
+    load_c(warp, cr, ci);
+  }
+  int b = 0;
+  for (int strip = warp; strip < nstrips; strip += 4, b ^= 1) {
+    const int nxt = strip + 4;
+    double nr[kNi][4], nim[kNi][4];
+    if (nxt < nstrips) {
+      fetch_e(nxt, b ^ 1);
+      load_c(nxt, nr, nim);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncwarp();
+#pragma unroll
+    for (int kk = 0; kk < kW / 4; ++kk) {
+      const cd a0 = sm.E[warp][b][g][kk * 4 + t];
+      const cd a1 = sm.E[warp][b][g + 8][kk * 4 + t];
+#pragma unroll
+      for (int ni = 0; ni < kNi; ++ni) {
+        const cd bf = sm.C1[kk * 4 + t][ni * 8 + g];
+        double* R = cr[ni];
+        double* I = ci[ni];
+        dmma(R[0], R[1], R[2], R[3], a0.x, a1.x, bf.x);
+        dmma(R[0], R[1], R[2], R[3], -a0.y, -a1.y, bf.y);
+        dmma(I[0], I[1], I[2], I[3], a0.x, a1.x, bf.y);
+        dmma(I[0], I[1], I[2], I[3], a0.y, a1.y, bf.x);
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = strip * kStrip + g + 8 * h;
+      if (r < n) {
+#pragma unroll
+        for (int ni = 0; ni < kNi; ++ni)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const int vc = vt + ni * 8 + j;
+            if (vc < total) colp(vc)[(size_t)r * ld] = cd{cr[ni][2 * h + j], ci[ni][2 * h + j]};
+          }
+      }
+    }
+    __syncwarp();  // the next fetch reuses this strip's buffer
+    if (nxt < nstrips) {
+#pragma unroll
+      for (int ni = 0; ni < kNi; ++ni)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          cr[ni][e] = nr[ni][e];
+          ci[ni][e] = nim[ni][e];
+        }
+    }
+  }
+}
+
+// The original path: the shared-memory panel (W1, L2 by triangular inverses) and
+// the one-thread-per-column update, for the product-first arithmetic (the boundary
+// transforms, the bulk solve) and for more than kPanelRowsMax rows.
 template <int kW, bool kF>
-static void gauss_jordan_panels(cd* Q, cd* P, const int* flag, int nang, int n, int ld,
-                                const GJScratch& sc, unsigned* status, cudaStream_t st) {
-  const size_t smem = (size_t)n * kW * sizeof(cd);
+static void gauss_jordan_smem(cd* Q, cd* P, const int* flag, int nang, int n, int ld,
+                              const GJScratch& sc, unsigned* status, cudaStream_t st) {
   static SmemOptIn attr;
+  const size_t smem = (size_t)n * kW * sizeof(cd);
   attr.ensure((const void*)k_gj_panel<kW, kF>, smem);
   for (int c0 = 0; c0 < n; c0 += kW) {
-    int w = (n - c0 < kW) ? n - c0 : kW;
+    const int w = (n - c0 < kW) ? n - c0 : kW;
     k_gj_panel<kW, kF><<<nang, 256, smem, st>>>(Q, flag, n, ld, c0, w, sc, status);
-    int total = (n - (c0 + w)) + n;
+    const int total = (n - (c0 + w)) + n;
     dim3 grid(ceil_div(total, kUpdCols), nang);
     k_gj_update<kW, kF><<<grid, kUpdCols, 0, st>>>(Q, P, flag, n, ld, c0, w, sc);
   }
 }
 
+// The renormalisations: the row-per-thread panel writing E (fused or product-first
+// complex arithmetic) and the trailing update on the FP64 tensor path; n <= 640.
+template <bool kF>
+static void gauss_jordan_rows(cd* Q, cd* P, const int* flag, int nang, int n, int ld,
+                              const GJScratch& sc, unsigned* status, cudaStream_t st) {
+  static SmemOptIn attr;
+  attr.ensure((const void*)k_gj_update_mma, sizeof(MmaUpdSmem));
+  const int threads = round_up(n, 32);
+  for (int c0 = 0; c0 < n; c0 += kWMax) {
+    const int w = (n - c0 < kWMax) ? n - c0 : kWMax;
+    if (threads <= 256)
+      k_gj_panel_rows<kF, 256><<<nang, threads, 0, st>>>(Q, flag, n, ld, c0, w, sc.piv, sc.L2,
+                                                         status);
+    else if (threads <= 544)
+      k_gj_panel_rows<kF, 544><<<nang, threads, 0, st>>>(Q, flag, n, ld, c0, w, sc.piv, sc.L2,
+                                                         status);
+    else
+      k_gj_panel_rows<kF, kPanelRowsMax><<<nang, threads, 0, st>>>(Q, flag, n, ld, c0, w, sc.piv,
+                                                                   sc.L2, status);
+    const int total = (n - (c0 + w)) + n;
+    dim3 grid(ceil_div(total, kMmaCols), nang);
+    k_gj_update_mma<<<grid, 128, sizeof(MmaUpdSmem), st>>>(Q, P, flag, n, ld, c0, w, sc.piv,
+                                                            sc.L2);
+  }
+}
+
 void launch_gauss_jordan(cd* Q, cd* P, const int* flag, int nang, int n, int ld, void* scratch,
-                         unsigned* status, cudaStream_t st, bool fused) {
+                         unsigned* status, cudaStream_t st, int arith) {
   GJScratch sc = gj_carve(scratch, nang, n);
-  if (fused)
-    gauss_jordan_panels<kWMax, true>(Q, P, flag, nang, n, ld, sc, status, st);
-  else
-    gauss_jordan_panels<kWMax, false>(Q, P, flag, nang, n, ld, sc, status, st);
+  const bool rows = n <= kPanelRowsMax;
+  if (arith == kGjFused) {
+    if (rows) gauss_jordan_rows<true>(Q, P, flag, nang, n, ld, sc, status, st);
+    else gauss_jordan_smem<kWMax, true>(Q, P, flag, nang, n, ld, sc, status, st);
+  } else if (arith == kGjFp64Mma && rows) {
+    gauss_jordan_rows<false>(Q, P, flag, nang, n, ld, sc, status, st);
+  } else {
+    gauss_jordan_smem<kWMax, false>(Q, P, flag, nang, n, ld, sc, status, st);
+  }
 }
 
 // ============================================================ RK4 stage combination

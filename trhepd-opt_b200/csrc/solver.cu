@@ -25,6 +25,7 @@
 #include "integrators.h"
 #include "kernels.h"
 #include "small.h"
+#include "cholqr.h"
 #include "split_gemm.h"
 
 using namespace trhepd;
@@ -222,6 +223,8 @@ struct RunState {
   bool capturing = false;    // launches go into a CUDA graph: no events on the stream
   long prof_entries = 0;     // event quadruples recorded in profile mode
   long renorm_entries = 0;   // event pairs around renormalisations (profile mode)
+  cd* gsx = nullptr;         // int_method 8: power-estimate vectors (nang x n)
+  void* gss = nullptr;       // int_method 8: CholeskyQR scratch
   int nprob = 1;             // stacked problems (see trhepd_problem::nprob)
   const TableEntry* const* tables = nullptr;
   StackedRows sr{};          // rows and stage-matrix stride per stacked problem
@@ -473,6 +476,16 @@ void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_m
   CK(cudaMemsetAsync(R.Q, 0, R.sbytes, st));
   CK(cudaMemsetAsync(R.Qn, 0, R.sbytes, st));
   CK(cudaMemsetAsync(R.P, 0, R.sbytes, st));
+  if (Pb.I.gs) {
+    // rk4_intgs (surf_rk.f90:106-109): invstrans, CholeskyQR of every angle, the
+    // power-estimate vector initialised
+    R.gsx = (cd*)C->mg[1].ensure((size_t)nang * n * sizeof(cd));
+    R.gss = C->mg[0].ensure(cholqr_scratch_bytes(nang, n, ld));
+    launch_invstrans_build(Pb.F.as<cd>(), R.Q, R.P, R.gam, nang, n, ld, st);
+    launch_power_est(R.Q, R.P, R.gsx, R.flags, R.dval, nang, n, ld, -1, st);
+    R.launches += 2 + launch_cholqr(R.Q, R.P, R.flags, nang, n, ld, R.gss, R.status, st);
+    return;
+  }
   // invstransh: Q = I + F^H, P = I - F^H; P <- Q^{-1} P; P <- i P conj(G); Q = I
   launch_invstransh_build(Pb.F.as<cd>(), R.Q, R.P, nang, n, ld, st);
   launch_gauss_jordan(R.Q, R.P, nullptr, nang, n, ld, R.gjs, R.status, st);
@@ -482,6 +495,22 @@ void begin_run(trhepd_context* C, trhepd_problem& Pb, int precision, int nprod_m
   if (C->renorm_policy == 1) {
     double kap = Pb.kappa_max + 1.0;
     R.interval = std::max(1, (int)std::floor(C->renorm_tau / (kap * Pb.dz)));
+  }
+}
+
+// rk4_intgs after each slice (surf_rk.f90:147-152): the power estimate of
+// ||[q; p]||^2 (at most nb steps), then CholeskyQR of the angles above 1e2.
+void reorthogonalise(trhepd_context* C, RunState& R) {
+  cudaEvent_t* ev = (C->profile && 2 * (R.renorm_entries + 1) <= (long)C->rnpool.size())
+                        ? &C->rnpool[2 * R.renorm_entries]
+                        : nullptr;
+  if (ev) CK(cudaEventRecord(ev[0], R.st));
+  launch_power_est(R.Q, R.P, R.gsx, R.flags, R.dval, R.nang, R.n, R.ld, R.n, R.st);
+  R.launches += 1 + launch_cholqr(R.Q, R.P, R.flags, R.nang, R.n, R.ld, R.gss, R.status, R.st);
+  ++R.renorms;  // upper bound; per-angle decisions stay on the device
+  if (ev) {
+    CK(cudaEventRecord(ev[1], R.st));
+    ++R.renorm_entries;
   }
 }
 
@@ -538,13 +567,15 @@ void renormalise(trhepd_context* C, RunState& R, int l, bool every_slice) {
 void renormalise_launch(trhepd_context* C, RunState& R, bool last, int l, bool every_slice) {
   if (C->renorm_policy == 0 && !every_slice) {
     launch_cond_est(R.Q, R.nang, R.n, R.ld, last ? 1 : 0, R.flags, R.dval, R.st);
-    launch_gauss_jordan(R.Q, R.P, R.flags, R.nang, R.n, R.ld, R.gjs, R.status, R.st, R.split);
+    launch_gauss_jordan(R.Q, R.P, R.flags, R.nang, R.n, R.ld, R.gjs, R.status, R.st,
+                        R.split ? kGjFused : kGjFp64Mma);
     launch_set_identity(R.Q, R.flags, R.nang, R.n, R.ld, R.st);
     R.launches += 2 + R.gj_per;
     R.gj_launches += R.gj_per;
     if (!last) ++R.renorms;  // upper bound; per-angle decisions stay on the device
   } else if (last || every_slice || (l % R.interval) == 0) {
-    launch_gauss_jordan(R.Q, R.P, nullptr, R.nang, R.n, R.ld, R.gjs, R.status, R.st, R.split);
+    launch_gauss_jordan(R.Q, R.P, nullptr, R.nang, R.n, R.ld, R.gjs, R.status, R.st,
+                        R.split ? kGjFused : kGjFp64Mma);
     launch_set_identity(R.Q, nullptr, R.nang, R.n, R.ld, R.st);
     R.launches += 1 + R.gj_per;
     R.gj_launches += R.gj_per;
@@ -556,7 +587,10 @@ void renormalise_launch(trhepd_context* C, RunState& R, bool last, int l, bool e
 void finish_device(trhepd_context* C, trhepd_problem& Pb, RunState& R) {
   cudaStream_t st = R.st;
   const int n = R.n, nang = R.nang, ld = R.ld;
-  launch_stransh_build(R.Q, R.P, R.gam, nang, n, ld, st);
+  if (Pb.I.gs)
+    launch_strans_build(R.Q, R.P, R.gam, nang, n, ld, st);  // strans + matAdivB2
+  else
+    launch_stransh_build(R.Q, R.P, R.gam, nang, n, ld, st);
   launch_gauss_jordan(R.Q, R.P, nullptr, nang, n, ld, R.gjs, R.status, st);
   launch_check_finite(R.P, (size_t)nang * n * ld, R.status, st);
   launch_intensities(R.P, R.gam, Pb.wnsga2.as<double>(), nang, n, ld, Pb.nb0,
@@ -733,7 +767,10 @@ void run_rk4(trhepd_context* C, trhepd_problem& Pb, int precision, RunState& R) 
                          R.ld, R.st);
       R.launches += 1;
     }
-    renormalise(C, R, l, false);
+    if (Pb.I.gs)
+      reorthogonalise(C, R);
+    else
+      renormalise(C, R, l, false);
   }
   finish_device(C, Pb, R);
 }
