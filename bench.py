@@ -65,9 +65,14 @@ from trhepd_opt_b200 import build as tbuild  # noqa: E402
 from trhepd_opt_b200 import bulkfile, generator, native, surface  # noqa: E402
 
 METRIC = "angle-solves/s at N=521, split-precision vs FP64 on 1 B200; p50/p99 latency"
-# DRAM bytes (read + write) per launch of the tensor-core stage kernel from one ncu
-# capture (profiles/), keyed by (workload, form); absent entries report null.
-NCU_TRAFFIC: dict = {}
+# DRAM bytes (read + write) per launch of the stage kernels from one ncu capture of
+# the 16-angle profiling case (dense521s, same N and generator), keyed by (workload,
+# form, digit slices); the bench scales them by angles / 16.  Summaries and commands:
+# profiles/k_split_gemm_i8_dense521s.md, profiles/k_stage_gemm_f64_dense521s.md.
+NCU_TRAFFIC: dict = {
+    ("dense521", "int8", 5): (202.690816 + 95.043584) * 1e6,  # k_split_gemm_i8<5>
+    ("dense521", "fp64", 0): (145.711360 + 85.679872) * 1e6,  # k_stage_gemm_f64
+}
 WORKLOADS = {
     "dense521": ("dense521: N=521 beams, 61 glancing angles 0.5-6.5 deg, 20 A region in 0.01 A "
                  "slices (sp4 RKN), synthetic 2x2 Si/Ge surface over 4-atom bulk, seed 3",
@@ -533,8 +538,9 @@ def main():
                               "(profiles/k_split_gemm_i8_dense521s.md)" if traffic else None,
             "note": "ops per launch = slice pairs x 8*nangles*N^3 (complex N^3 as a real "
                     "(nangles*N) x 2N x 2N product per slice pair); stage_product_ms adds "
-                    "the slicing and exponent kernels of the same stage; the kernel is "
-                    "bound by shared-memory operand bandwidth (see frac_of_mma_issue_rate)"}
+                    "the slicing and exponent kernels of the same stage; ncu of the kernel: "
+                    "tensor pipe active 43 %, issue stalls led by long-scoreboard (the "
+                    "epilogue's FP64 state loads) and barrier (the accumulator hand-off)"}
     # where the device time of one solve goes (the profiled solve; events between
     # launches make it slightly longer than an unprofiled one)
     breakdown = {"solve_ms": stp["device_ms"], "stage_products_ms": stp["stage_kernel_ms"],
@@ -664,8 +670,10 @@ def main():
                     "max_rel_err_all_spots": fp64["split_max_rel_err_all_spots"],
                     "fp64_value": fp64["value"], "split_value": value,
                     "renormalisation": "growth bound ln(1e3) for both forms; Gauss-Jordan "
-                                       "with fused complex multiply-adds (split) and with "
-                                       "products formed first (FP64, reference rounding)"}}
+                                       "panels of 16 columns (row-per-thread panel kernel) "
+                                       "with the trailing update on the FP64 tensor path in "
+                                       "both forms; panel arithmetic with fused complex "
+                                       "multiply-adds (split) or products formed first (FP64)"}}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()

@@ -887,24 +887,29 @@ __global__ void __launch_bounds__(128, 3)
   const cd* Ea = E + (size_t)a * n * kW;
   for (int i = tid; i < n; i += 128) sm.rslot[i] = -1;
   __syncthreads();
-  if (tid == 0) {
-    int nt = w;
-    for (int q = 0; q < w; ++q) sm.tpos[q] = sm.tsrc[q] = c0 + q;
+  if (warp == 0) {
+    // lane q holds touched entry q (position, source row): entries 0..w-1 are the
+    // pivot block, later ones the pivot rows below it in order of first use
+    int pos = lane < w ? c0 + lane : -1, src = pos, nt = w;
+    const int myp = lane < w ? pivs[a * kW + lane] : 0;
     for (int jj = 0; jj < w; ++jj) {
-      const int r1 = pivs[a * kW + jj];
-      int i1 = -1;
-      for (int q = 0; q < nt; ++q)
-        if (sm.tpos[q] == r1) i1 = q;
-      if (i1 < 0) {
+      const int r1 = __shfl_sync(0xffffffffu, myp, jj);
+      const unsigned hit = __ballot_sync(0xffffffffu, pos == r1);
+      int i1;
+      if (hit) {
+        i1 = __ffs(hit) - 1;
+      } else {
         i1 = nt++;
-        sm.tpos[i1] = sm.tsrc[i1] = r1;
+        if (lane == i1) pos = src = r1;
       }
-      const int s = sm.tsrc[jj];
-      sm.tsrc[jj] = sm.tsrc[i1];
-      sm.tsrc[i1] = s;
+      const int sj = __shfl_sync(0xffffffffu, src, jj), si = __shfl_sync(0xffffffffu, src, i1);
+      if (lane == jj) src = si;
+      if (lane == i1) src = sj;
     }
-    for (int q = w; q < nt; ++q) sm.rslot[sm.tpos[q]] = (short)(q - w);
-    sm.ntouched = nt;
+    sm.tpos[lane] = pos;
+    sm.tsrc[lane] = src;
+    if (lane >= w && lane < nt) sm.rslot[pos] = (short)(lane - w);
+    if (lane == 0) sm.ntouched = nt;
   }
   __syncthreads();
   {
