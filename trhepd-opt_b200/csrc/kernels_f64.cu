@@ -473,17 +473,19 @@ constexpr int kWMax = 16;      // panel width the scratch is sized for
 constexpr int kUpdCols = 128;  // trailing columns per update block
 
 struct GJScratch {
-  int* piv;   // nang x kW
+  int* piv;   // nang x 2 kW
   cd* W1;     // nang x kW x kW
-  cd* L2;     // nang x n x kW
+  cd* L2;     // nang x n x 2 kW (the shared-memory path uses nang x n x kW of it)
 };
 
+// Pivots and multipliers: 2 kW per angle (the row-per-thread path keeps the pivots
+// and E of two panels; the shared-memory path uses the first kW of each).
 size_t gj_scratch_bytes(int nang, int n) {
-  size_t b = (size_t)nang * kWMax * sizeof(int);
+  size_t b = (size_t)nang * 2 * kWMax * sizeof(int);
   b = (b + 255) & ~size_t(255);
   b += (size_t)nang * kWMax * kWMax * sizeof(cd);
   b = (b + 255) & ~size_t(255);
-  b += (size_t)nang * n * kWMax * sizeof(cd);
+  b += (size_t)nang * n * 2 * kWMax * sizeof(cd);
   return b + 256;
 }
 
@@ -491,7 +493,7 @@ static GJScratch gj_carve(void* scratch, int nang, int n) {
   GJScratch s;
   char* p = reinterpret_cast<char*>(scratch);
   s.piv = reinterpret_cast<int*>(p);
-  size_t b = (size_t)nang * kWMax * sizeof(int);
+  size_t b = (size_t)nang * 2 * kWMax * sizeof(int);
   b = (b + 255) & ~size_t(255);
   s.W1 = reinterpret_cast<cd*>(p + b);
   b += (size_t)nang * kWMax * kWMax * sizeof(cd);
@@ -651,7 +653,8 @@ constexpr int kPanelRowsMax = 640;
 template <bool kF, int kMaxT>
 __global__ void __launch_bounds__(kMaxT, 1)
     k_gj_panel_rows(const cd* __restrict__ Q, const int* __restrict__ flag, int n, int ld, int c0,
-                    int w, int* __restrict__ piv, cd* __restrict__ E, unsigned* status) {
+                    int w, int* __restrict__ piv, int pstride, cd* __restrict__ E, int estride,
+                    unsigned* status) {
   static_assert(kWMax == 16, "one 16-column panel per thread row");
   const int a = blockIdx.x;
   if (flag && !flag[a]) return;
@@ -715,11 +718,12 @@ __global__ void __launch_bounds__(kMaxT, 1)
       }
     }
     const int p = __shfl_sync(full, bi, 0), pw = p >> 5;  // row p is thread p's
-    if (tid == 0) piv[a * kWMax + jj] = p;
+    if (tid == 0) piv[a * pstride + jj] = p;
     const cd* u = cand_row[buf][pw];  // the pivot row (old row p)
     const cd d = u[jj];  // shared memory: a dynamic index is fine
     if (d.x == 0.0 && d.y == 0.0 && tid == 0) atomicOr(status, kStatusZeroPivot);
-    const cd r = cdiv(cd{1.0, 0.0}, d);
+    const double dinv = 1.0 / (d.x * d.x + d.y * d.y);  // 1/d = conj(d) / |d|^2
+    const cd r = cd{d.x * dinv, -d.y * dinv};
     if (tid == col) {
 #pragma unroll
       for (int k = 0; k < kWMax; ++k) x[k] = (k == jj) ? r : u[k] * r;
@@ -735,7 +739,7 @@ __global__ void __launch_bounds__(kMaxT, 1)
     }
   }
   if (tid < n) {
-    cd* e = E + ((size_t)a * n + tid) * kWMax;
+    cd* e = E + ((size_t)a * n + tid) * estride;
 #pragma unroll
     for (int k = 0; k < kWMax; ++k) e[k] = x[k];
   }
@@ -842,73 +846,121 @@ __global__ void __launch_bounds__(kUpdCols, 4) k_gj_update(cd* __restrict__ Q, c
   }
 }
 
-// Trailing update from the panel's E on the FP64 tensor path (fused rounding).
-// C' = C + E C1 for every row (C = 0 for the pivot rows, whose E rows are B1^{-1})
-// is a complex GEMM with K = 16.  The CTA owns kMmaCols trailing columns of one
-// angle; after a common setup its four warps work independently on 16-row strips
-// (warp w: strips w, w+4, ...).  Per strip: m16n8k4 FP64 MMAs, four real MMAs per
-// complex product, accumulators initialised from C; the warp's E rows come
-// through its own two cp.async buffers and the next strip's C values are loaded
-// into registers while the current strip's MMAs run.
-// Row swaps: thread 0 replays the panel's swap sequence on the (at most 2 kW)
-// touched row positions, so every position knows which original row its value
-// comes from; C1 (the pivot rows after the swaps) and the values that end in
-// touched rows below the panel are read into shared memory before any row is
-// written, and a strip reads a touched row from that stash.
+// Trailing update from a Gauss-Jordan step's E on the FP64 tensor path (fused
+// rounding).  For the kW pivot rows c0..c0+w-1 (w <= kW) the step is, after its
+// row swaps, C' = C + E C1 for every row (C = 0 for the pivot rows, whose E rows
+// are B1^{-1}): a complex GEMM with K = kW over the trailing columns.  The columns
+// come in two segments (Q right of the panel and P; or the 16 columns of another
+// step's E), each with its own base, row stride and angle stride.  The CTA owns
+// kMmaCols columns of one angle; after a common setup its four warps work
+// independently on 16-row strips (warp w: strips w, w+4, ...).  Per strip: m16n8k4
+// FP64 MMAs, four real MMAs per complex product, accumulators initialised from C;
+// the warp's E rows come through its own two cp.async buffers and the next strip's
+// C values are loaded into registers while the current strip's MMAs run.
+// Row swaps: warp 0 replays the step's swap sequence on the (at most 2 kW) touched
+// row positions, so every position knows which original row its value comes from;
+// C1 (the pivot rows after the swaps) and the values that end in touched rows
+// below the pivot block are read into shared memory before any row is written,
+// and a strip reads a touched row from that stash.
 constexpr int kMmaCols = 32;        // complex columns per CTA (4 n8 tiles)
 constexpr int kStrip = 16;          // rows per warp strip
-constexpr int kEStr = kWMax + 4;    // complex entries per E row in shared memory
 constexpr int kC1Str = kMmaCols + 2;
+template <int kW>
 struct MmaUpdSmem {
+  static constexpr int kEStr = kW + 4;  // complex entries per E row in shared memory
   cd E[4][2][kStrip][kEStr];
-  cd C1[kWMax][kC1Str];
-  cd stash[kWMax][kMmaCols];
+  cd C1[kW][kC1Str];
+  cd stash[kW][kMmaCols];
   short rslot[kMaxBeams];
-  int tpos[2 * kWMax], tsrc[2 * kWMax];
+  int tpos[2 * kW], tsrc[2 * kW];
   int ntouched;
 };
-__global__ void __launch_bounds__(128, 3)
-    k_gj_update_mma(cd* __restrict__ Q, cd* __restrict__ P, const int* __restrict__ flag, int n,
-                    int ld, int c0, int w, const int* __restrict__ pivs,
-                    const cd* __restrict__ E) {
-  constexpr int kW = kWMax, kNi = kMmaCols / 8;
-  const int a = blockIdx.y;
-  if (flag && !flag[a]) return;
-  extern __shared__ __align__(16) unsigned char mma_dyn[];
-  MmaUpdSmem& sm = *reinterpret_cast<MmaUpdSmem*>(mma_dyn);
+
+// Trailing columns of an update: segment 0 (n0 columns) then segment 1.  Element
+// (r, vc) of angle a is p + a * as + r * ld + vc (vc counted within its segment).
+struct GjCols {
+  cd* p0;
+  long long as0;
+  int ld0, n0;
+  cd* p1;
+  long long as1;
+  int ld1, n1;
+};
+
+// One work item: angle a, trailing columns vc0 .. vc0 + kMmaCols - 1.
+template <int kW>
+__device__ __forceinline__ void gj_update_mma_item(MmaUpdSmem<kW>& sm, const GjCols& cols, int n,
+                                                   int c0, int w, const int* __restrict__ pivs,
+                                                   int pstride, const cd* __restrict__ E,
+                                                   int estride, int a, int vc0) {
+  constexpr int kNi = kMmaCols / 8, kSlots = (2 * kW + 31) / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int qrest = n - (c0 + w), total = qrest + n;
-  const int vc0 = blockIdx.x * kMmaCols;
-  cd* Qa = Q + (size_t)a * n * ld;
-  cd* Pa = P + (size_t)a * n * ld;
-  // row 0 of trailing column vc (vc < total)
-  auto colp = [&](int vc) -> cd* { return vc < qrest ? Qa + (c0 + w + vc) : Pa + (vc - qrest); };
-  const cd* Ea = E + (size_t)a * n * kW;
+  const int total = cols.n0 + cols.n1;
+  cd* const b0 = cols.p0 + (size_t)a * cols.as0;
+  cd* const b1 = cols.p1 + (size_t)a * cols.as1;
+  // element (r, vc) of this angle's trailing columns (vc < total)
+  auto at = [&](int r, int vc) -> cd* {
+    return vc < cols.n0 ? b0 + (size_t)r * cols.ld0 + vc
+                        : b1 + (size_t)r * cols.ld1 + (vc - cols.n0);
+  };
+  const cd* Ea = E + (size_t)a * n * estride;
+  const int* pa = pivs + (size_t)a * pstride;
   for (int i = tid; i < n; i += 128) sm.rslot[i] = -1;
   __syncthreads();
   if (warp == 0) {
-    // lane q holds touched entry q (position, source row): entries 0..w-1 are the
-    // pivot block, later ones the pivot rows below it in order of first use
-    int pos = lane < w ? c0 + lane : -1, src = pos, nt = w;
-    const int myp = lane < w ? pivs[a * kW + lane] : 0;
-    for (int jj = 0; jj < w; ++jj) {
-      const int r1 = __shfl_sync(0xffffffffu, myp, jj);
-      const unsigned hit = __ballot_sync(0xffffffffu, pos == r1);
-      int i1;
-      if (hit) {
-        i1 = __ffs(hit) - 1;
-      } else {
-        i1 = nt++;
-        if (lane == i1) pos = src = r1;
-      }
-      const int sj = __shfl_sync(0xffffffffu, src, jj), si = __shfl_sync(0xffffffffu, src, i1);
-      if (lane == jj) src = si;
-      if (lane == i1) src = sj;
+    // entry q (lane q & 31, slot q >> 5) holds a touched position and the row its
+    // value comes from: entries 0..w-1 are the pivot block, later ones the pivot
+    // rows below it in order of first use
+    int pos[kSlots], src[kSlots], myp[kSlots];
+#pragma unroll
+    for (int e = 0; e < kSlots; ++e) {
+      const int q = lane + 32 * e;
+      pos[e] = q < w ? c0 + q : -1;
+      src[e] = pos[e];
+      myp[e] = q < w ? pa[q] : 0;
     }
-    sm.tpos[lane] = pos;
-    sm.tsrc[lane] = src;
-    if (lane >= w && lane < nt) sm.rslot[pos] = (short)(lane - w);
+    int nt = w;
+    for (int jj = 0; jj < w; ++jj) {
+      int r1 = 0;
+#pragma unroll
+      for (int e = 0; e < kSlots; ++e)
+        if ((jj >> 5) == e) r1 = __shfl_sync(0xffffffffu, myp[e], jj & 31);
+      int i1 = -1;
+#pragma unroll
+      for (int e = kSlots - 1; e >= 0; --e) {
+        const unsigned hit = __ballot_sync(0xffffffffu, pos[e] == r1);
+        if (hit) i1 = 32 * e + __ffs(hit) - 1;
+      }
+      if (i1 < 0) {
+        i1 = nt++;
+#pragma unroll
+        for (int e = 0; e < kSlots; ++e)
+          if (lane + 32 * e == i1) pos[e] = src[e] = r1;
+      }
+      int sj = 0, si = 0;
+#pragma unroll
+      for (int e = 0; e < kSlots; ++e) {
+        const int vj = __shfl_sync(0xffffffffu, src[e], jj & 31);
+        const int vi = __shfl_sync(0xffffffffu, src[e], i1 & 31);
+        if ((jj >> 5) == e) sj = vj;
+        if ((i1 >> 5) == e) si = vi;
+      }
+#pragma unroll
+      for (int e = 0; e < kSlots; ++e) {
+        if (lane + 32 * e == jj) src[e] = si;
+        if (lane + 32 * e == i1) src[e] = sj;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < kSlots; ++e) {
+      const int q = lane + 32 * e;
+      if (q < 2 * kW) {
+        sm.tpos[q] = pos[e];
+        sm.tsrc[q] = src[e];
+      }
+      if (q >= w && q < nt) sm.rslot[pos[e]] = (short)(q - w);
+    }
     if (lane == 0) sm.ntouched = nt;
   }
   __syncthreads();
@@ -918,11 +970,10 @@ __global__ void __launch_bounds__(128, 3)
     for (int it = 0; it < 2 * kW * kMmaCols / 128; ++it) {
       const int e = tid + it * 128, q = e / kMmaCols, c = e % kMmaCols, vc = vc0 + c;
       if (q < kW) {
-        sm.C1[q][c] =
-            (q < w && vc < total) ? colp(vc)[(size_t)sm.tsrc[q] * ld] : cd{0.0, 0.0};
-      } else {  // stash slot s: touched entry w + s (rows below the panel)
+        sm.C1[q][c] = (q < w && vc < total) ? *at(sm.tsrc[q], vc) : cd{0.0, 0.0};
+      } else {  // stash slot sl: touched entry w + sl (rows below the pivot block)
         const int sl = q - kW, te = w + sl;
-        if (te < nt) sm.stash[sl][c] = vc < total ? colp(vc)[(size_t)sm.tsrc[te] * ld] : cd{0.0, 0.0};
+        if (te < nt) sm.stash[sl][c] = vc < total ? *at(sm.tsrc[te], vc) : cd{0.0, 0.0};
       }
     }
   }
@@ -933,7 +984,7 @@ __global__ void __launch_bounds__(128, 3)
 #pragma unroll
     for (int q = 0; q < kStrip * kW / 32; ++q) {
       const int e = lane + q * 32, r = e / kW, k = e % kW, row = strip * kStrip + r;
-      const cd* src = Ea + (size_t)min(row, n - 1) * kW + k;
+      const cd* src = Ea + (size_t)min(row, n - 1) * estride + k;
       const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sm.E[warp][b][r][k]);
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
                    "r"(row < n ? 16 : 0)
@@ -955,8 +1006,7 @@ __global__ void __launch_bounds__(128, 3)
         for (int j = 0; j < 2; ++j) {
           const int vc = vt + ni * 8 + j;
           cd v = cd{0.0, 0.0};
-          if (live && vc < total)
-            v = sl >= 0 ? sm.stash[sl][ni * 8 + 2 * t + j] : colp(vc)[(size_t)r * ld];
+          if (live && vc < total) v = sl >= 0 ? sm.stash[sl][ni * 8 + 2 * t + j] : *at(r, vc);
           cr[ni][2 * h + j] = v.x;
           ci[ni][2 * h + j] = v.y;
         }
@@ -1004,7 +1054,7 @@ __global__ void __launch_bounds__(128, 3)
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
             const int vc = vt + ni * 8 + j;
-            if (vc < total) colp(vc)[(size_t)r * ld] = cd{cr[ni][2 * h + j], ci[ni][2 * h + j]};
+            if (vc < total) *at(r, vc) = cd{cr[ni][2 * h + j], ci[ni][2 * h + j]};
           }
       }
     }
@@ -1018,6 +1068,25 @@ __global__ void __launch_bounds__(128, 3)
           ci[ni][e] = nim[ni][e];
         }
     }
+  }
+}
+
+// Grid-stride over the (angle, column tile) items, so the last wave of a launch is
+// not left partly empty.
+template <int kW>
+__global__ void __launch_bounds__(128, 2)
+    k_gj_update_mma(GjCols cols, const int* __restrict__ flag, int n, int c0, int w,
+                    const int* __restrict__ pivs, int pstride, const cd* __restrict__ E,
+                    int estride, int nang) {
+  extern __shared__ __align__(16) unsigned char mma_dyn[];
+  MmaUpdSmem<kW>& sm = *reinterpret_cast<MmaUpdSmem<kW>*>(mma_dyn);
+  const int tiles = ceil_div(cols.n0 + cols.n1, kMmaCols);
+  for (int item = blockIdx.x; item < tiles * nang; item += gridDim.x) {
+    const int a = item / tiles;
+    if (flag && !flag[a]) continue;
+    gj_update_mma_item<kW>(sm, cols, n, c0, w, pivs, pstride, E, estride, a,
+                           (item - a * tiles) * kMmaCols);
+    __syncthreads();  // the next item reuses the shared memory
   }
 }
 
@@ -1039,29 +1108,82 @@ static void gauss_jordan_smem(cd* Q, cd* P, const int* flag, int nang, int n, in
   }
 }
 
-// The renormalisations: the row-per-thread panel writing E (fused or product-first
-// complex arithmetic) and the trailing update on the FP64 tensor path; n <= 640.
+static int gj_sm_count() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms > 0 ? sms : 148;
+}
+
+// The renormalisations, n <= 640: the row-per-thread panel (fused or product-first
+// complex arithmetic) and the trailing update on the FP64 tensor path.  The split
+// forms take 32 pivot columns per trailing update.  For columns c0..c0+31: the panel on the first 16
+// (E_a), a rank-16 update of the next 16 columns only, the panel on those (E_b),
+// the second step applied to E_a's 16 columns (so that [E_a | E_b] is the E of a
+// 32-column Gauss-Jordan step: the in-place elimination of the second half would
+// have updated the first half's slots), then one rank-32 update of every other
+// trailing column with the 32 row swaps in order.  The last panel of fewer than
+// 17 columns takes one rank-16 step.  E and the pivots live in the scratch's
+// 32-column blocks (row stride 32).
 template <bool kF>
 static void gauss_jordan_rows(cd* Q, cd* P, const int* flag, int nang, int n, int ld,
                               const GJScratch& sc, unsigned* status, cudaStream_t st) {
-  static SmemOptIn attr;
-  attr.ensure((const void*)k_gj_update_mma, sizeof(MmaUpdSmem));
-  const int threads = round_up(n, 32);
-  for (int c0 = 0; c0 < n; c0 += kWMax) {
-    const int w = (n - c0 < kWMax) ? n - c0 : kWMax;
+  static SmemOptIn attr16, attr32;
+  attr16.ensure((const void*)k_gj_update_mma<16>, sizeof(MmaUpdSmem<16>));
+  attr32.ensure((const void*)k_gj_update_mma<32>, sizeof(MmaUpdSmem<32>));
+  const int threads = round_up(n, 32), sms = gj_sm_count();
+  constexpr int kP = 2 * kWMax;  // pivots and E columns per angle in the scratch
+  const long long qa = (long long)n * ld, ea = (long long)n * kP;
+  auto panel = [&](int c, int w, int poff) {
+    int* pv = sc.piv + poff;
+    cd* E = sc.L2 + poff;
     if (threads <= 256)
-      k_gj_panel_rows<kF, 256><<<nang, threads, 0, st>>>(Q, flag, n, ld, c0, w, sc.piv, sc.L2,
+      k_gj_panel_rows<kF, 256><<<nang, threads, 0, st>>>(Q, flag, n, ld, c, w, pv, kP, E, kP,
                                                          status);
     else if (threads <= 544)
-      k_gj_panel_rows<kF, 544><<<nang, threads, 0, st>>>(Q, flag, n, ld, c0, w, sc.piv, sc.L2,
+      k_gj_panel_rows<kF, 544><<<nang, threads, 0, st>>>(Q, flag, n, ld, c, w, pv, kP, E, kP,
                                                          status);
     else
-      k_gj_panel_rows<kF, kPanelRowsMax><<<nang, threads, 0, st>>>(Q, flag, n, ld, c0, w, sc.piv,
-                                                                   sc.L2, status);
-    const int total = (n - (c0 + w)) + n;
-    dim3 grid(ceil_div(total, kMmaCols), nang);
-    k_gj_update_mma<<<grid, 128, sizeof(MmaUpdSmem), st>>>(Q, P, flag, n, ld, c0, w, sc.piv,
-                                                            sc.L2);
+      k_gj_panel_rows<kF, kPanelRowsMax><<<nang, threads, 0, st>>>(Q, flag, n, ld, c, w, pv, kP,
+                                                                   E, kP, status);
+  };
+  auto update16 = [&](const GjCols& cols, int c, int w, int poff) {
+    const int items = ceil_div(cols.n0 + cols.n1, kMmaCols) * nang;
+    if (items == 0) return;
+    k_gj_update_mma<16><<<std::min(items, 2 * sms), 128, sizeof(MmaUpdSmem<16>), st>>>(
+        cols, flag, n, c, w, sc.piv + poff, kP, sc.L2 + poff, kP, nang);
+  };
+  if (!kF) {
+    // the FP64 form: rank-16 steps throughout (its parity against the reference's
+    // test521 sp6 0.68 output, 2e-9, holds with this blocking and not with the
+    // rank-32 one, 2.5e-9)
+    for (int c0 = 0; c0 < n; c0 += kWMax) {
+      const int w = std::min(kWMax, n - c0);
+      panel(c0, w, 0);
+      update16(GjCols{Q + c0 + w, qa, ld, n - c0 - w, P, qa, ld, n}, c0, w, 0);
+    }
+    return;
+  }
+  for (int c0 = 0; c0 < n;) {
+    const int rem = n - c0;
+    if (rem <= kWMax) {  // one rank-16 step: Q right of the panel (none) and P
+      panel(c0, rem, 0);
+      update16(GjCols{Q + c0 + rem, qa, ld, 0, P, qa, ld, n}, c0, rem, 0);
+      break;
+    }
+    const int wb = std::min(kWMax, rem - kWMax), w = kWMax + wb;
+    panel(c0, kWMax, 0);
+    // step a on the next panel's columns only
+    update16(GjCols{Q + c0 + kWMax, qa, ld, wb, P, qa, ld, 0}, c0, kWMax, 0);
+    panel(c0 + kWMax, wb, kWMax);
+    // step b on E_a's 16 columns
+    update16(GjCols{sc.L2, ea, kP, kWMax, P, qa, ld, 0}, c0 + kWMax, wb, kWMax);
+    // both steps on every other trailing column
+    const GjCols rest{Q + c0 + w, qa, ld, n - c0 - w, P, qa, ld, n};
+    const int items = ceil_div(rest.n0 + rest.n1, kMmaCols) * nang;
+    k_gj_update_mma<32><<<std::min(items, 2 * sms), 128, sizeof(MmaUpdSmem<32>), st>>>(
+        rest, flag, n, c0, w, sc.piv, kP, sc.L2, kP, nang);
+    c0 += w;
   }
 }
 
