@@ -668,6 +668,7 @@ def main():
                 "split_vs_fp64": None if not fp64 else {
                     "speedup": fp64["split_speedup"],
                     "max_rel_err_all_spots": fp64["split_max_rel_err_all_spots"],
+                    "every_spot_within_1e-6": bool(fp64["split_max_rel_err_all_spots"] <= 1e-6),
                     "fp64_value": fp64["value"], "split_value": value,
                     "renormalisation": "growth bound ln(1e3) for both forms; Gauss-Jordan "
                                        "panels of 16 columns (row-per-thread panel kernel) "
