@@ -1074,7 +1074,7 @@ __device__ __forceinline__ void gj_update_mma_item(MmaUpdSmem<kW>& sm, const GjC
 // Grid-stride over the (angle, column tile) items, so the last wave of a launch is
 // not left partly empty.
 template <int kW>
-__global__ void __launch_bounds__(128, 2)
+__global__ void __launch_bounds__(128, kW == 16 ? 3 : 2)
     k_gj_update_mma(GjCols cols, const int* __restrict__ flag, int n, int c0, int w,
                     const int* __restrict__ pivs, int pstride, const cd* __restrict__ E,
                     int estride, int nang) {
@@ -1150,7 +1150,7 @@ static void gauss_jordan_rows(cd* Q, cd* P, const int* flag, int nang, int n, in
   auto update16 = [&](const GjCols& cols, int c, int w, int poff) {
     const int items = ceil_div(cols.n0 + cols.n1, kMmaCols) * nang;
     if (items == 0) return;
-    k_gj_update_mma<16><<<std::min(items, 2 * sms), 128, sizeof(MmaUpdSmem<16>), st>>>(
+    k_gj_update_mma<16><<<std::min(items, 3 * sms), 128, sizeof(MmaUpdSmem<16>), st>>>(
         cols, flag, n, c, w, sc.piv + poff, kP, sc.L2 + poff, kP, nang);
   };
   if (!kF) {

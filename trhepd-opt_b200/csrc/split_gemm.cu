@@ -862,34 +862,40 @@ __device__ __forceinline__ uint16_t pack2(int a, int b) {
 
 // One warp per stacked row: exponent of the off-diagonal row maximum, then the S
 // digit slices of the row, (Re, Im) interleaved; each lane writes two complex k.
-template <int S>
-__global__ void k_slice_rows_i8(const cd* __restrict__ Q, int rows, int n, int ld, int kr,
-                                uint32_t* __restrict__ A, int* __restrict__ erow) {
+template <int S, int NPL>
+__global__ void __launch_bounds__(256) k_slice_rows_i8(const cd* __restrict__ Q, int rows, int n,
+                                                       int ld, int kc, uint16_t* __restrict__ A,
+                                                       int* __restrict__ erow) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= rows) return;
   const int r = warp, i = r % n;
   const cd* q = Q + (size_t)r * ld;
+  // one pass over the row: lane holds complex k = lane + 32 j (k < kc, zero past n
+  // and on the diagonal), the row maximum, then the digits from registers
+  cd v[NPL];
   double m = 0.0;
-  for (int k = lane; k < n; k += 32)
-    if (k != i) m = fmax(m, fmax(fabs(q[k].x), fabs(q[k].y)));
+#pragma unroll
+  for (int j = 0; j < NPL; ++j) {
+    const int k = lane + 32 * j;
+    v[j] = (k < n && k != i) ? q[k] : cd{0.0, 0.0};
+    m = fmax(m, fmax(fabs(v[j].x), fabs(v[j].y)));
+  }
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   int e = 0;
   if (m > 0.0) frexp(m * kDigitHeadroom, &e);
   if (lane == 0) erow[r] = e;
   const double sc = digit_scale(e, S);
-  const int kw = kr / 4;      // 32-bit words per slice row (two complex k each)
-  for (int w = lane; w < kw; w += 32) {
-    const int k0 = 2 * w, k1 = 2 * w + 1;
-    const cd v0 = (k0 < n && k0 != i) ? q[k0] : cd{0.0, 0.0};
-    const cd v1 = (k1 < n && k1 != i) ? q[k1] : cd{0.0, 0.0};
-    int a[S], b[S], c[S], d[S];
-    digits_i8<S>(v0.x, sc, a);
-    digits_i8<S>(v0.y, sc, b);
-    digits_i8<S>(v1.x, sc, c);
-    digits_i8<S>(v1.y, sc, d);
 #pragma unroll
-    for (int s = 0; s < S; ++s) A[((size_t)s * rows + r) * kw + w] = pack4(a[s], b[s], c[s], d[s]);
+  for (int j = 0; j < NPL; ++j) {
+    const int k = lane + 32 * j;
+    if (k < kc) {
+      int a[S], b[S];
+      digits_i8<S>(v[j].x, sc, a);
+      digits_i8<S>(v[j].y, sc, b);
+#pragma unroll
+      for (int s = 0; s < S; ++s) A[((size_t)s * rows + r) * kc + k] = pack2(a[s], b[s]);
+    }
   }
 }
 
@@ -1367,6 +1373,20 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 
 }  // namespace split
 
+// Row slicing with the row held in registers: complex entries per lane NPL >=
+// ceil(kc / 32), the smallest instantiated (kc <= 832).
+template <int S>
+static void slice_rows_i8(const cd* Q, int rows, int n, int ld, int kc, uint16_t* A, int* erow,
+                          cudaStream_t st) {
+  const int blocks = ceil_div(rows, 8), npl = ceil_div(kc, 32);
+  if (npl <= 2) split::k_slice_rows_i8<S, 2><<<blocks, 256, 0, st>>>(Q, rows, n, ld, kc, A, erow);
+  else if (npl <= 4) split::k_slice_rows_i8<S, 4><<<blocks, 256, 0, st>>>(Q, rows, n, ld, kc, A, erow);
+  else if (npl <= 8) split::k_slice_rows_i8<S, 8><<<blocks, 256, 0, st>>>(Q, rows, n, ld, kc, A, erow);
+  else if (npl <= 12) split::k_slice_rows_i8<S, 12><<<blocks, 256, 0, st>>>(Q, rows, n, ld, kc, A, erow);
+  else if (npl <= 17) split::k_slice_rows_i8<S, 17><<<blocks, 256, 0, st>>>(Q, rows, n, ld, kc, A, erow);
+  else split::k_slice_rows_i8<S, 26><<<blocks, 256, 0, st>>>(Q, rows, n, ld, kc, A, erow);
+}
+
 // ============================================================ host side
 namespace {
 
@@ -1522,10 +1542,9 @@ void run_split_i8(const SplitWorkspace& w, const cd* Q, cd* P, cd* Qo, const cd*
   const int kr = 2 * c.kc;
   if (kr > 16384) throw std::invalid_argument("INT8 split form: k beyond the exact INT32 range");
   uint16_t* B = reinterpret_cast<uint16_t*>(c.B);
-  uint32_t* A = reinterpret_cast<uint32_t*>(c.A);
   split::k_slice_cols_i8<S><<<dim3(n, nprob), 128, 0, st>>>(V, n, ld, c.kc, c.nrows, c.fcol, B,
                                                             sr.vstride, c.npad);
-  split::k_slice_rows_i8<S><<<ceil_div(c.rows, 8), 256, 0, st>>>(Q, c.rows, n, ld, kr, A, c.erow);
+  slice_rows_i8<S>(Q, c.rows, n, ld, c.kc, reinterpret_cast<uint16_t*>(c.A), c.erow, st);
   CUtensorMap ta = make_map(c.A, kr, c.rows, S, 1);
   CUtensorMap tb = make_map(c.B, kr, c.nrows, S * nprob, 1, NTS);
   split::EpiArgs ep{Q, P, Qo, V, D, c.erow, c.fcol, w.status, c.rows, n, ld, c.kc, S, cb, ca};
