@@ -243,10 +243,25 @@ def cpu_sample(workdir: Path, s, plan: dict) -> tuple[float, int]:
     return t, L
 
 
-def cpu_baseline(workdir: Path, s, nangles: int, max_seconds: float = 25.0) -> dict:
-    plan = cpu_sample_plan(workdir, s, nangles, max_seconds)
-    t, L = cpu_sample(workdir, s, plan)
-    return {"seconds": t, "angles": plan["angles"], "slices": L, "cores": plan["cores"]}
+def cpu_model() -> str:
+    """The host CPU's model name (Linux /proc/cpuinfo), else the platform's."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def cpu_baseline(workdir: Path, s, nangles: int, reps: int = 5, seconds: float = 6.0) -> dict:
+    """The median of `reps` timed samples of about `seconds` each."""
+    plan = cpu_sample_plan(workdir, s, nangles, seconds)
+    runs = [cpu_sample(workdir, s, plan) for _ in range(reps)]
+    times = sorted(t for t, _ in runs)
+    return {"seconds": times[len(times) // 2], "samples_s": times, "angles": plan["angles"],
+            "slices": runs[0][1], "cores": plan["cores"]}
 
 
 def serve_leg(device: int, seconds: float, load: float, precision: int, seed: int = 0) -> dict:
@@ -411,6 +426,7 @@ def main():
                     "config": {"workload": desc},
                     "cpu_baseline": {"value": value, "unit": "angle-solves/s",
                                      "cores": plan["cores"], "kind": "port",
+                                     "cpu_model": cpu_model(), "nproc": os.cpu_count(),
                                      "sample": f"per step {plan['angles']} angles x first {L} "
                                                f"of {S_ns} slices on {plan['cores']} threads, "
                                                "scaled by slice count"},
@@ -614,8 +630,10 @@ def main():
         ns = rp.ns
         cpu_value = b["angles"] / (b["seconds"] * ns / b["slices"])
         cpu = {"value": cpu_value, "unit": "angle-solves/s", "cores": b["cores"], "kind": "port",
-               "sample": f"{b['angles']} angles x first {b['slices']} of {ns} slices on "
-                         f"{b['cores']} threads, scaled by slice count"}
+               "sample": f"median of {len(b['samples_s'])} samples of {b['angles']} angles x "
+                         f"first {b['slices']} of {ns} slices on {b['cores']} threads, scaled "
+                         "by slice count",
+               "samples_s": b["samples_s"], "cpu_model": cpu_model(), "nproc": os.cpu_count()}
 
     rp.close()
     sp.close()
