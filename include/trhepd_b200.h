@@ -75,7 +75,9 @@ enum trhepd_option {
   TRHEPD_OPT_MAX_CTAS = 11      /* 0 (default): the stage-product kernels use every SM; k > 0:
                                    the persistent split kernels run at most k CTAs and the FP64
                                    stage kernel at most 2k blocks, leaving the other SMs to
-                                   kernels of other contexts (streams) on the same GPU */
+                                   kernels of other contexts (streams) on the same GPU; -1: the
+                                   split kernels run one CTA per tile, so higher-priority work of
+                                   other contexts starts between tiles */
 };
 
 typedef struct trhepd_context trhepd_context;

@@ -138,8 +138,9 @@ def test_split_other_integrators(ctx, tmp_path, method, precision):
 
 def test_cta_cap_gives_identical_results(ctx, tmp_path):
     """TRHEPD_OPT_MAX_CTAS caps the stage kernels' grids (a serving slot leaving SMs
-    to others): every tile is computed by the same code whichever CTA takes it, so
-    the results are bit-identical to the uncapped solve."""
+    to others) or runs the split kernels one CTA per tile (-1): every tile is
+    computed by the same code whichever CTA takes it, so the results are
+    bit-identical to the uncapped solve."""
     from trhepd_opt_b200 import generator, native
     sp, rp = _resident(ctx, tmp_path, generator.dense(200, n_angles=13, region=2.0))
     ctx.set_option(native.OPT_SPLIT_SLICES, 5)
@@ -147,11 +148,12 @@ def test_cta_cap_gives_identical_results(ctx, tmp_path):
     for prec in (native.SPLIT_INT8, native.SPLIT_BF16, native.FP64):
         rp.solve(prec)
         _, ref = rp.fetch()
-        ctx.set_option(native.OPT_MAX_CTAS, 16)
-        try:
-            rp.solve(prec)
-            _, got = rp.fetch()
-        finally:
-            ctx.set_option(native.OPT_MAX_CTAS, 0)
-        assert np.array_equal(got, ref), prec
+        for cap in (16, -1):  # at most 16 CTAs; one CTA per tile
+            ctx.set_option(native.OPT_MAX_CTAS, cap)
+            try:
+                rp.solve(prec)
+                _, got = rp.fetch()
+            finally:
+                ctx.set_option(native.OPT_MAX_CTAS, 0)
+            assert np.array_equal(got, ref), (prec, cap)
     ctx.set_option(native.OPT_FUSED_MAX_N, 64)

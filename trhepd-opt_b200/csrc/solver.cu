@@ -99,7 +99,7 @@ struct trhepd_context {
   int fused_max_n = kFusedMaxBeams;  // FP64 RKN solves with n <= this run fused (0: never)
   int validate = 0;              // 1: split solves also run the FP64 form (per-curve errors)
   int particle = 0;              // trhepd_bulk_run: 0 positrons, 1 electrons
-  int max_ctas = 0;              // persistent split kernels: CTA cap (0: one per SM)
+  int max_ctas = 0;              // persistent split kernels: CTA cap (0: one per SM, -1: one per tile)
   double stats[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<double> curve_err; // 3 per angle of the last validated solve (curves.h)
   std::vector<cudaEvent_t> evpool;
@@ -1867,7 +1867,8 @@ int trhepd_set_option(trhepd_context* c, int option, double value) {
       c->validate = value != 0.0;
       return TRHEPD_OK;
     case TRHEPD_OPT_MAX_CTAS:
-      if (value < 0 || value > 1 << 20) return fail(c, TRHEPD_EINVAL, "CTA cap must be >= 0");
+      if (value < -1 || value > 1 << 20 || value != (double)(int)value)
+        return fail(c, TRHEPD_EINVAL, "CTA cap must be an integer >= -1");
       c->max_ctas = (int)value;
       return TRHEPD_OK;
     case TRHEPD_OPT_PARTICLE:

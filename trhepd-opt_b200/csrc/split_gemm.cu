@@ -1476,8 +1476,12 @@ int sm_count() {
 
 // CTAs of a persistent kernel: one per SM, or fewer when the context caps them (a
 // serving slot leaving SMs to concurrent requests of other slots).
+// CTAs of a persistent split kernel: one per SM, at most max_ctas (> 0), or one
+// per tile (max_ctas = -1: each CTA takes about one tile and exits, so the block
+// scheduler can start higher-priority work of other streams between tiles).
 int persistent_grid(const SplitWorkspace& w) {
   const int sms = sm_count();
+  if (w.max_ctas < 0) return 1 << 30;
   return w.max_ctas > 0 ? std::min(sms, w.max_ctas) : sms;
 }
 

@@ -83,12 +83,13 @@ def poisson_stream(rate: float, duration: float, seed: int = 0, mix=None,
 
 FUSED_MAX_N = 64
 # slot layout: (smallest N, largest N, stream priority 0 lowest .. 1 highest, SM cap
-# of the stage-product kernels, 0 = every SM).  A large solve's stage kernels hold
-# their SMs for a whole launch (persistent split kernels) or a block's lifetime
-# (FP64), so a small request's kernels would queue for SMs behind every launch; the
-# large-N slot is capped at 48 of the 148 SMs and the other slots always find SMs
-# free.  Their own kernels are not capped: the split kernels' CTAs take tiles from a
-# shared counter, so the CTAs that start at once do the work.
+# of the stage-product kernels, 0 = every SM, -1 = one CTA per tile).  A large
+# solve's stage kernels hold their SMs for a whole launch (persistent split kernels)
+# or a block's lifetime (FP64), so a small request's kernels would queue for SMs
+# behind every launch; the large-N slot is capped at 48 of the 148 SMs and the
+# other slots always find SMs free.  Their own kernels are not capped: the split
+# kernels' CTAs take tiles from a shared counter, so the CTAs that start at once do
+# the work.  (One CTA per tile in the middle slot left the measured p99 unchanged.)
 DEFAULT_SLOTS = ((0, 95, 1.0, 0), (0, 95, 1.0, 0), (96, 191, 0.5, 0), (192, 1 << 30, 0.0, 48))
 
 
