@@ -461,14 +461,22 @@ void launch_cond_est(const cd* Q, int nang, int n, int ld, int force, int* flag,
 
 // ============================================================ K8 blocked Gauss-Jordan
 // [Q | P] -> [I | Q^{-1} P] with partial pivoting (pivot = max |re|+|im| among the
-// rows not yet used, lowest index on ties, as zgetrf's izamax).  Panels of kW = 16
-// columns (24-column panels, which fit shared memory up to n = 530, measured
-// slower at n = 521: the panel kernel's serial column steps outweigh the saved
-// passes over the trailing matrix): the panel kernel factors rows c0.. of the panel (LU with row swaps) and
-// forms W1 = B1^{-1} and the elimination multipliers L2 = B2 B1^{-1} for every
-// other row; the update kernel applies the swaps and
-//   C1 <- W1 C1,   C2 <- C2 - L2 C1
-// to all remaining columns (Q columns right of the panel and every P column).
+// rows not yet used, lowest index on ties, as zgetrf's izamax), in panels of
+// kW = 16 columns.  Two implementations (launch_gauss_jordan picks by arithmetic
+// and size):
+// * shared memory (products-first arithmetic, and beyond 640 rows): the panel
+//   kernel factors rows c0.. of the n x 16 panel in shared memory (LU with row
+//   swaps) and forms W1 = B1^{-1} and the elimination multipliers L2 = B2 B1^{-1}
+//   for every other row; the update kernel applies the swaps and
+//     C1 <- W1 C1,   C2 <- C2 - L2 C1
+//   to all remaining columns (Q columns right of the panel and every P column),
+//   one thread per column.  (24-column panels, which fit shared memory up to
+//   n = 530, measured slower at n = 521: the serial column steps outweigh the
+//   saved passes over the trailing matrix.)
+// * row per thread (the renormalisations, n <= 640): k_gj_panel_rows eliminates
+//   the panel in place with each row in one thread's registers and writes E; the
+//   trailing update C' = C + E C1 runs on the FP64 tensor path
+//   (k_gj_update_mma), rank 32 in the split forms.
 constexpr int kWMax = 16;      // panel width the scratch is sized for
 constexpr int kUpdCols = 128;  // trailing columns per update block
 
