@@ -366,6 +366,33 @@ def bulk_leg(ctx, cpu: bool) -> dict:
     return out
 
 
+def rk4_leg(ctx) -> dict:
+    """int_method 7 (RK4, Gauss-Jordan renormalisation on the Gershgorin test) and
+    int_method 8 (RK4, CholeskyQR when the power estimate exceeds 1e2) on the
+    reference's test47 structure (N = 47, 0.22 A slices), plain FP64 through
+    trhepd_surf_run: device time of the second solve of each, and how far the two
+    results are apart (the re-orthogonalisation changes rounding only)."""
+    out = {}
+    try:
+        d = ROOT / "tests" / "golden" / "test47"
+        ctx.set_option(native.OPT_RENORM_POLICY, 0)
+        f2s = {}
+        for m in (7, 8):
+            ctx.surf_run(d / "bulkP.b", d / "surf.txt", 0.22, m, native.FP64)
+            f2, dims = ctx.surf_run(d / "bulkP.b", d / "surf.txt", 0.22, m, native.FP64)
+            ms = ctx.last_stats()["device_ms"]
+            f2s[m] = f2
+            out[f"int_method_{m}"] = {"device_ms": ms, "angles": dims["nangles"],
+                                      "angle_solves_per_s": dims["nangles"] / (ms / 1e3)}
+        rowmax = np.maximum(np.abs(f2s[7]).max(axis=1, keepdims=True), 1e-300)
+        out["max_diff_vs_rowmax"] = float((np.abs(f2s[8] - f2s[7]) / rowmax).max())
+    except Exception as e:  # a failed leg is reported, the bench line still prints
+        out["error"] = f"{type(e).__name__}: {e}"
+    finally:
+        ctx.set_option(native.OPT_RENORM_POLICY, 1)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -384,6 +411,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven candidate batch")
     ap.add_argument("--no-bulk", action="store_true", help="skip the bulk boundary solve leg")
+    ap.add_argument("--no-rk4", action="store_true", help="skip the int_method 7/8 leg")
     ap.add_argument("--uneven-per-n", type=int, default=64,
                     help="candidates per beam count in the uneven batch (64: 256 structures)")
     ap.add_argument("--serve-seconds", type=float, default=60.0)
@@ -643,6 +671,9 @@ def main():
     bulk = None
     if rank == 0 and ws == 1 and not args.no_bulk:
         bulk = bulk_leg(ctx, cpu=not args.no_cpu_baseline)
+    rk4 = None
+    if rank == 0 and ws == 1 and not args.no_rk4:
+        rk4 = rk4_leg(ctx)
     ctx.close()
 
     serve = None
@@ -680,6 +711,7 @@ def main():
                 "cpu_baseline": cpu,
                 "gpu_launches": launches, "clocks": clk, "wall_seconds_timed": t_wall,
                 "serving": serve, "uneven_batch": uneven, "bulk_boundary": bulk,
+                "rk4_methods": rk4,
                 "breakdown": breakdown,
                 "bf16_split": bf16, "fp64": fp64,
                 # last, so that a truncated view of the line still shows them
